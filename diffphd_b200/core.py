@@ -1,0 +1,317 @@
+"""Python facade over libdiffphd_b200.so, mirroring the reference's SWIG `HexDeformable` / `TetDeformable`
+(cpp/core/src/py_diff_pd_core.i:60-68; method names from cpp/core/include/fem/deformable.h) so that code
+written against `py_diff_pd` (e.g. python/py_diff_pd/env/env_base.py:163-427) runs unchanged on the B200
+path.  Vectors may be lists, numpy arrays or the `StdRealVector` / `StdIntVector` helpers; outputs are
+written into the mutable containers passed in, as SWIG's by-reference std::vector outputs are.
+
+The computation always runs in the CUDA library; there is no CPU fallback.  Errors raised by the library
+(the reference's CheckError) surface as RuntimeError with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libdiffphd_b200.so"
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib = None
+
+
+class StdRealVector(list):
+    """Stand-in for the reference's SWIG StdRealVector (a resizable list of floats)."""
+
+    def __init__(self, n=0):
+        super().__init__([0.0] * int(n) if isinstance(n, (int, np.integer)) else list(n))
+
+
+class StdIntVector(list):
+    def __init__(self, n=0):
+        super().__init__([0] * int(n) if isinstance(n, (int, np.integer)) else list(n))
+
+
+def load_library():
+    """Load the in-tree CUDA library; fails loudly when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"diffphd_b200 CUDA library missing at {LIB_PATH}; build it with "
+                           "`python -m diffphd_b200.build` (there is no CPU fallback)")
+    L = C.CDLL(str(LIB_PATH))
+    L.dphd_last_error.restype = C.c_char_p
+    L.dphd_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    L.dphd_destroy.argtypes = [C.c_void_p]
+    L.dphd_init_from_bin.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_char_p, C.c_double, C.c_double]
+    L.dphd_init_from_arrays.argtypes = [C.c_void_p, _dp, C.c_int, _ip, C.c_int, C.c_double, C.c_char_p, C.c_double,
+                                        C.c_double]
+    L.dphd_set_dirichlet.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    L.dphd_add_pd_energy.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_int, _ip, C.c_int]
+    L.dphd_add_state_force.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_int]
+    L.dphd_set_frictional_boundary.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_int, _ip, C.c_int]
+    for f in ("dphd_dofs", "dphd_act_dofs", "dphd_num_pd_element_energies", "dphd_num_state_force_parameters",
+              "dphd_num_pd_params", "dphd_num_frames", "dphd_last_backward_iters"):
+        getattr(L, f).argtypes = [C.c_void_p]
+    L.dphd_s_memory_bytes.argtypes = [C.c_void_p]
+    L.dphd_s_memory_bytes.restype = C.c_longlong
+    L.dphd_s_nnz.argtypes = [C.c_void_p]
+    L.dphd_s_nnz.restype = C.c_longlong
+    L.dphd_frame_stats.argtypes = [C.c_void_p, _ip, _ip]
+    L.dphd_reset_frame_stats.argtypes = [C.c_void_p]
+    kv = [C.POINTER(C.c_char_p), _dp, C.c_int]
+    L.dphd_forward.argtypes = [C.c_void_p, C.c_char_p, _dp, _dp, _dp, _dp, C.c_double] + kv + [_dp, _dp, _ip, _ip]
+    bw = [C.c_void_p, C.c_char_p, _dp, _dp, _dp, _dp, C.c_double, _dp, _dp, _ip, C.c_int, _dp, _dp] + kv + \
+         [_dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.dphd_backward.argtypes = bw
+    L.dphd_backward_ex.argtypes = bw + [_dp]
+    L.dphd_forward_device.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + kv + \
+                                     [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.dphd_debug_ainv.argtypes = [C.c_void_p, C.c_double, _dp, _dp, C.c_int]
+    L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+    L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Names declared in include/diffphd_b200.h (for the ABI completeness test)."""
+    import re
+    hdr = (_PKG.parent / "include" / "diffphd_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(dphd_[a-z_0-9]+)\s*\(", hdr)))
+
+
+def _arr(x, n=None):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())
+    if n is not None and a.size != n:
+        raise RuntimeError(f"Inconsistent vector size: expected {n}, got {a.size}")
+    return a
+
+
+def _iarr(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int32).ravel())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def _opts(options):
+    options = dict(options or {})
+    keys = [str(k) for k in options]
+    karr = (C.c_char_p * max(1, len(keys)))(*[k.encode() for k in keys])
+    vals = np.array([float(options[k]) for k in keys] or [0.0], dtype=np.float64)
+    return karr, vals, len(keys)
+
+
+def _write_out(dst, src):
+    """Copy into a by-reference output: numpy array in place, list-likes resized."""
+    if isinstance(dst, np.ndarray):
+        dst.reshape(-1)[:] = src
+    elif isinstance(dst, list):
+        dst[:] = list(src)
+    elif dst is not None:
+        raise TypeError("output containers must be numpy arrays or lists")
+
+
+class Deformable:
+    vertex_dim = 3
+    element_dim = 8
+
+    def __init__(self):
+        L = load_library()
+        h = C.c_void_p()
+        self._check(L.dphd_create(3, self.element_dim, C.byref(h)))
+        self._h = h
+        self._L = L
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and getattr(self, "_L", None) is not None:
+            self._L.dphd_destroy(h)
+            self._h = None
+
+    @staticmethod
+    def _check(rc):
+        if rc != 0:
+            raise RuntimeError(load_library().dphd_last_error().decode())
+
+    # ---- builder --------------------------------------------------------------------------------
+    def Initialize(self, mesh_or_vertices, *args):
+        """Initialize(bin_file, density, material_type, E, nu) or
+        Initialize(vertices (n,3), elements (m,k), density, material_type, E, nu)."""
+        if isinstance(mesh_or_vertices, (str, os.PathLike)):
+            density, material, E, nu = args
+            self._check(self._L.dphd_init_from_bin(self._h, str(mesh_or_vertices).encode(), float(density),
+                                                   material.encode(), float(E), float(nu)))
+        else:
+            elements, density, material, E, nu = args
+            v = _arr(mesh_or_vertices)
+            e = _iarr(elements)
+            self._check(self._L.dphd_init_from_arrays(self._h, _ptr(v), v.size // 3, _iptr(e),
+                                                      e.size // self.element_dim, float(density), material.encode(),
+                                                      float(E), float(nu)))
+
+    def SetDirichletBoundaryCondition(self, dof, val):
+        self._check(self._L.dphd_set_dirichlet(self._h, int(dof), float(val)))
+
+    def AddPdEnergy(self, energy_type, params, indices):
+        p = _arr(params)
+        i = _iarr(indices)
+        self._check(self._L.dphd_add_pd_energy(self._h, energy_type.encode(), _ptr(p), p.size, _iptr(i), i.size))
+
+    def AddStateForce(self, force_type, params):
+        p = _arr(params)
+        self._check(self._L.dphd_add_state_force(self._h, force_type.encode(), _ptr(p), p.size))
+
+    def SetFrictionalBoundary(self, boundary_type, params, indices):
+        p = _arr(params)
+        i = _iarr(indices)
+        self._check(self._L.dphd_set_frictional_boundary(self._h, boundary_type.encode(), _ptr(p), p.size,
+                                                         _iptr(i), i.size))
+
+    # ---- accessors ------------------------------------------------------------------------------
+    def dofs(self):
+        return self._L.dphd_dofs(self._h)
+
+    def act_dofs(self):
+        return self._L.dphd_act_dofs(self._h)
+
+    def NumOfPdElementEnergies(self):
+        return self._L.dphd_num_pd_element_energies(self._h)
+
+    def NumOfPdMuscleEnergies(self):
+        return 0
+
+    def NumOfStateForceParameters(self):
+        return self._L.dphd_num_state_force_parameters(self._h)
+
+    def NumOfPdParams(self):
+        return self._L.dphd_num_pd_params(self._h)
+
+    # ---- step ------------------------------------------------------------------------------------
+    def PyForward(self, method, q, v, a, f_ext, dt, options, q_next, v_next, active_contact_idx):
+        n = self.dofs()
+        qa, va, fa = _arr(q, n), _arr(v, n), _arr(f_ext, n)
+        aa = _arr(a) if a is not None and len(a) else np.zeros(1)
+        qn, vn = np.zeros(n), np.zeros(n)
+        act = np.zeros(max(1, n // 3), dtype=np.int32)
+        na = C.c_int(act.size)
+        k, vals, no = _opts(options)
+        self._check(self._L.dphd_forward(self._h, method.encode(), _ptr(qa), _ptr(va), _ptr(aa), _ptr(fa),
+                                         float(dt), k, _ptr(vals), no, _ptr(qn), _ptr(vn), _iptr(act),
+                                         C.byref(na)))
+        _write_out(q_next, qn)
+        _write_out(v_next, vn)
+        if active_contact_idx is not None:
+            _write_out(active_contact_idx, act[:na.value].tolist() if isinstance(active_contact_idx, list)
+                       else act[:na.value])
+        return qn, vn
+
+    def PyBackward(self, method, q, v, a, f_ext, dt, q_next, v_next, active_contact_idx, dl_dq_next, dl_dv_next,
+                   options, dl_dq, dl_dv, dl_da, dl_df_ext, dl_dmat_w, dl_dact_w, dl_dstate_p):
+        out = self.backward(method, q, v, a, f_ext, dt, q_next, v_next, active_contact_idx, dl_dq_next,
+                            dl_dv_next, options)
+        for dst, key in ((dl_dq, "dl_dq"), (dl_dv, "dl_dv"), (dl_da, "dl_da"), (dl_df_ext, "dl_df_ext"),
+                         (dl_dmat_w, "dl_dmat_w"), (dl_dact_w, "dl_dact_w"), (dl_dstate_p, "dl_dstate_p")):
+            _write_out(dst, out[key])
+        return out
+
+    def backward(self, method, q, v, a, f_ext, dt, q_next, v_next, active_contact_idx, dl_dq_next, dl_dv_next,
+                 options):
+        """PyBackward returning a dict, with the extension `dl_dparams` (per AddPdEnergy parameter arrays)."""
+        n = self.dofs()
+        arrs = [_arr(x, n) for x in (q, v, f_ext, q_next, v_next, dl_dq_next, dl_dv_next)]
+        qa, va, fa, qna, vna, g1, g2 = arrs
+        aa = _arr(a) if a is not None and len(a) else np.zeros(1)
+        act = _iarr(active_contact_idx if active_contact_idx is not None else [])
+        actp = act if act.size else np.zeros(1, np.int32)
+        dq, dv, df = np.zeros(n), np.zeros(n), np.zeros(n)
+        ne = self.NumOfPdElementEnergies()
+        ns = self.NumOfStateForceParameters()
+        npar = self.NumOfPdParams()
+        dmat, dstate, dpar = np.zeros(max(ne, 1)), np.zeros(max(ns, 1)), np.zeros(max(npar, 1))
+        da, dact = np.zeros(1), np.zeros(1)
+        k, vals, no = _opts(options)
+        self._check(self._L.dphd_backward_ex(self._h, method.encode(), _ptr(qa), _ptr(va), _ptr(aa), _ptr(fa),
+                                             float(dt), _ptr(qna), _ptr(vna), _iptr(actp), int(act.size), _ptr(g1),
+                                             _ptr(g2), k, _ptr(vals), no, _ptr(dq), _ptr(dv), _ptr(da), _ptr(df),
+                                             _ptr(dmat), _ptr(dact), _ptr(dstate), _ptr(dpar)))
+        return {"dl_dq": dq, "dl_dv": dv, "dl_da": np.zeros(self.act_dofs()), "dl_df_ext": df,
+                "dl_dmat_w": dmat[:ne], "dl_dact_w": np.zeros(0), "dl_dstate_p": dstate[:ns],
+                "dl_dparams": dpar[:npar], "iters": self._L.dphd_last_backward_iters(self._h)}
+
+    def forward_device(self, method, q, v, f_ext, dt, options, q_next, v_next, stream=0):
+        """Device-pointer step on torch CUDA tensors (float64, contiguous, 3n); `stream` is a raw cudaStream_t."""
+        k, vals, no = _opts(options)
+        self._check(self._L.dphd_forward_device(self._h, method.encode(), C.c_void_p(q.data_ptr()),
+                                                C.c_void_p(v.data_ptr()), C.c_void_p(f_ext.data_ptr()), float(dt),
+                                                k, _ptr(vals), no, C.c_void_p(q_next.data_ptr()),
+                                                C.c_void_p(v_next.data_ptr()), C.c_void_p(int(stream))))
+
+    # ---- statistics ------------------------------------------------------------------------------
+    def frame_stats(self):
+        nf = self._L.dphd_num_frames(self._h)
+        it = np.zeros(max(nf, 1), np.int32)
+        cv = np.zeros(max(nf, 1), np.int32)
+        self._check(self._L.dphd_frame_stats(self._h, _iptr(it), _iptr(cv)))
+        return it[:nf].copy(), cv[:nf].copy()
+
+    def reset_frame_stats(self):
+        self._check(self._L.dphd_reset_frame_stats(self._h))
+
+    def s_memory_bytes(self):
+        return int(self._L.dphd_s_memory_bytes(self._h))
+
+    def s_nnz(self):
+        return int(self._L.dphd_s_nnz(self._h))
+
+    # ---- diagnostics -----------------------------------------------------------------------------
+    def debug_ainv(self, b, dt, fp32=False):
+        b = _arr(b, self.dofs())
+        x = np.zeros_like(b)
+        self._check(self._L.dphd_debug_ainv(self._h, float(dt), _ptr(b), _ptr(x), int(bool(fp32))))
+        return x
+
+    def debug_host_sts(self, b, dt):
+        b = _arr(b, self.dofs())
+        x = np.zeros_like(b)
+        self._check(self._L.dphd_debug_host_sts(self._h, float(dt), _ptr(b), _ptr(x)))
+        return x
+
+    def debug_local_step(self, q, dt):
+        q = _arr(q, self.dofs())
+        r = np.zeros_like(q)
+        self._check(self._L.dphd_debug_local_step(self._h, float(dt), _ptr(q), _ptr(r)))
+        return r
+
+
+class HexDeformable(Deformable):
+    element_dim = 8
+
+
+class TetDeformable(Deformable):
+    element_dim = 4
+
+
+def from_scene(scene):
+    """Build a Hex/TetDeformable from a diffphd_b200.scenes.Scene with the reference builder calls."""
+    cls = HexDeformable if scene.elems.shape[1] == 8 else TetDeformable
+    d = cls()
+    d.Initialize(scene.verts, scene.elems, scene.density, "none", 0.0, 0.0)
+    for dof, val in zip(scene.dirichlet_dofs, scene.dirichlet_vals):
+        d.SetDirichletBoundaryCondition(int(dof), float(val))
+    for kind, params, idx in scene.energies:
+        d.AddPdEnergy(kind, params, idx)
+    if scene.gravity is not None:
+        d.AddStateForce("gravity", scene.gravity)
+    if scene.plane is not None:
+        d.SetFrictionalBoundary("planar", scene.plane[0], scene.plane[1])
+    return d

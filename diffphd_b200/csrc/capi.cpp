@@ -1,0 +1,285 @@
+// extern "C" boundary: status codes + thread-local last-error message, no exceptions across the ABI
+// (the reference maps CheckError's ExceptionWithCallStack to a Python RuntimeError through SWIG,
+// cpp/core/src/py_diff_pd_core.i:17-27; here the Python layer raises RuntimeError from the message).
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/diffphd_b200.h"
+#include "engine.h"
+
+using dphd::Engine;
+using dphd::Error;
+
+struct dphd_deformable {
+    Engine* eng;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        g_last_error.clear();
+        f();
+        return 0;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return 1;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "out of host memory";
+        return 3;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return 2;
+    }
+}
+
+std::map<std::string, double> to_map(const char** keys, const double* vals, int n) {
+    std::map<std::string, double> m;
+    for (int i = 0; i < n; ++i) {
+        DPHD_CHECK(keys && keys[i], "null option key");
+        m[keys[i]] = vals[i];
+    }
+    return m;
+}
+
+void check_method(const char* method) {
+    DPHD_CHECK(method != nullptr, "null method");
+    const std::string s(method);
+    DPHD_CHECK(s == "pd_eigen_alg_phd" || s == "pd_eigen_pcg_proj_gpu",
+               "Unsupported method on this path: " + s + " (expected pd_eigen_alg_phd)");
+}
+
+Engine& E(dphd_deformable* h) {
+    DPHD_CHECK(h && h->eng, "null deformable handle");
+    return *h->eng;
+}
+const Engine& E(const dphd_deformable* h) {
+    DPHD_CHECK(h && h->eng, "null deformable handle");
+    return *h->eng;
+}
+
+// .bin reader (cpp/core/src/mesh/mesh.cpp:4-31, file_helper.cpp:169-184)
+void read_bin(const char* path, int k_expect, std::vector<double>& verts, std::vector<int>& elems, int& n, int& m) {
+    std::ifstream f(path, std::ios::binary);
+    DPHD_CHECK(f.good(), std::string("Cannot open mesh file: ") + path);
+    int vdim = 0, edim = 0, r = 0, c = 0;
+    f.read((char*)&vdim, 4);
+    f.read((char*)&edim, 4);
+    DPHD_CHECK(f.good() && vdim == 3 && edim == k_expect, std::string("Corrupted mesh file: ") + path);
+    f.read((char*)&r, 4);
+    f.read((char*)&c, 4);
+    DPHD_CHECK(f.good() && r == 3 && c > 0, "Inconsistent mesh matrix size.");
+    std::vector<double> vt((size_t)r * c);
+    f.read((char*)vt.data(), vt.size() * 8);
+    n = c;
+    verts.resize((size_t)3 * n);
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) verts[3 * i + d] = vt[(size_t)d * n + i];
+    int r2 = 0, c2 = 0;
+    f.read((char*)&r2, 4);
+    f.read((char*)&c2, 4);
+    DPHD_CHECK(f.good() && r2 == k_expect && c2 > 0, "Inconsistent mesh matrix size.");
+    std::vector<int> et((size_t)r2 * c2);
+    f.read((char*)et.data(), et.size() * 4);
+    DPHD_CHECK(f.good(), std::string("Truncated mesh file: ") + path);
+    m = c2;
+    elems.resize((size_t)k_expect * m);
+    for (int e = 0; e < m; ++e)
+        for (int a = 0; a < k_expect; ++a) elems[(size_t)e * k_expect + a] = et[(size_t)a * m + e];
+}
+}  // namespace
+
+extern "C" {
+
+const char* dphd_last_error(void) { return g_last_error.c_str(); }
+
+int dphd_create(int vertex_dim, int element_dim, dphd_deformable** out) {
+    return guard([&] {
+        DPHD_CHECK(out, "null output handle");
+        *out = nullptr;
+        auto* h = new dphd_deformable{nullptr};
+        try {
+            h->eng = new Engine(vertex_dim, element_dim);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int dphd_destroy(dphd_deformable* h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->eng;
+        delete h;
+    });
+}
+
+int dphd_init_from_bin(dphd_deformable* h, const char* bin_file, double density, const char* material_type,
+                       double E_, double nu) {
+    return guard([&] {
+        Engine& e = E(h);
+        std::vector<double> v;
+        std::vector<int> el;
+        int n = 0, m = 0;
+        read_bin(bin_file, e.M.k, v, el, n, m);
+        e.init_from_arrays(v.data(), n, el.data(), m, density, material_type ? material_type : "", E_, nu);
+    });
+}
+
+int dphd_init_from_arrays(dphd_deformable* h, const double* verts, int n, const int* elems, int m, double density,
+                          const char* material_type, double E_, double nu) {
+    return guard([&] {
+        DPHD_CHECK(verts && elems, "null mesh arrays");
+        E(h).init_from_arrays(verts, n, elems, m, density, material_type ? material_type : "", E_, nu);
+    });
+}
+
+int dphd_set_dirichlet(dphd_deformable* h, int dof, double val) {
+    return guard([&] { E(h).set_dirichlet(dof, val); });
+}
+
+int dphd_add_pd_energy(dphd_deformable* h, const char* type, const double* params, int np, const int* idx,
+                       int nidx) {
+    return guard([&] {
+        DPHD_CHECK(type && (params || np == 0) && (idx || nidx == 0), "null argument");
+        E(h).add_pd_energy(type, params, np, idx, nidx);
+    });
+}
+
+int dphd_add_state_force(dphd_deformable* h, const char* type, const double* params, int np) {
+    return guard([&] {
+        DPHD_CHECK(type && (params || np == 0), "null argument");
+        E(h).add_state_force(type, params, np);
+    });
+}
+
+int dphd_set_frictional_boundary(dphd_deformable* h, const char* type, const double* params, int np,
+                                 const int* idx, int nidx) {
+    return guard([&] {
+        DPHD_CHECK(type && (params || np == 0) && (idx || nidx == 0), "null argument");
+        E(h).set_frictional_boundary(type, params, np, idx, nidx);
+    });
+}
+
+int dphd_dofs(const dphd_deformable* h) { return h && h->eng ? h->eng->dofs() : -1; }
+int dphd_act_dofs(const dphd_deformable* h) { return h && h->eng ? 0 : -1; }
+int dphd_num_pd_element_energies(const dphd_deformable* h) { return h && h->eng ? h->eng->num_pd_energies() : -1; }
+int dphd_num_state_force_parameters(const dphd_deformable* h) {
+    return h && h->eng ? h->eng->num_state_params() : -1;
+}
+int dphd_num_pd_params(const dphd_deformable* h) { return h && h->eng ? h->eng->num_pd_params() : -1; }
+
+int dphd_forward(dphd_deformable* h, const char* method, const double* q, const double* v, const double* a,
+                 const double* f_ext, double dt, const char** keys, const double* vals, int nopts, double* q_next,
+                 double* v_next, int* active_idx, int* n_active) {
+    (void)a;
+    return guard([&] {
+        check_method(method);
+        DPHD_CHECK(q && v && f_ext && q_next && v_next, "null vector argument");
+        DPHD_CHECK(dt > 0, "dt must be positive");
+        const dphd::Options o = dphd::Options::parse(to_map(keys, vals, nopts));
+        std::vector<int> act;
+        E(h).forward(q, v, f_ext, dt, o, q_next, v_next, act);
+        if (n_active) {
+            DPHD_CHECK((int)act.size() <= *n_active || !active_idx, "active_idx capacity too small");
+            for (size_t i = 0; i < act.size() && active_idx; ++i) active_idx[i] = act[i];
+            *n_active = (int)act.size();
+        }
+    });
+}
+
+static int backward_impl(dphd_deformable* h, const char* method, const double* q, const double* v, const double* f,
+                         double dt, const double* qn, const double* vn, const double* gq, const double* gv,
+                         const char** keys, const double* vals, int nopts, double* dq, double* dv, double* df,
+                         double* dmat, double* dstate, double* dparams) {
+    return guard([&] {
+        check_method(method);
+        DPHD_CHECK(q && v && f && qn && vn && gq && gv && dq && dv && df, "null vector argument");
+        DPHD_CHECK(dt > 0, "dt must be positive");
+        Engine& e = E(h);
+        const dphd::Options o = dphd::Options::parse(to_map(keys, vals, nopts));
+        std::vector<double> mat(std::max(1, e.num_pd_energies())), st(3), par(std::max(1, e.num_pd_params()));
+        e.backward(q, v, f, dt, qn, vn, gq, gv, o, dq, dv, df, mat.data(), par.data(), st.data());
+        if (dmat)
+            for (int i = 0; i < e.num_pd_energies(); ++i) dmat[i] = mat[i];
+        if (dstate)
+            for (int i = 0; i < e.num_state_params(); ++i) dstate[i] = st[i];
+        if (dparams)
+            for (int i = 0; i < e.num_pd_params(); ++i) dparams[i] = par[i];
+    });
+}
+
+int dphd_backward(dphd_deformable* h, const char* method, const double* q, const double* v, const double* a,
+                  const double* f_ext, double dt, const double* q_next, const double* v_next, const int* active_idx,
+                  int n_active, const double* dl_dq_next, const double* dl_dv_next, const char** keys,
+                  const double* vals, int nopts, double* dl_dq, double* dl_dv, double* dl_da, double* dl_df_ext,
+                  double* dl_dmat_w, double* dl_dact_w, double* dl_dstate_p) {
+    (void)a; (void)active_idx; (void)n_active; (void)dl_da; (void)dl_dact_w;
+    return backward_impl(h, method, q, v, f_ext, dt, q_next, v_next, dl_dq_next, dl_dv_next, keys, vals, nopts,
+                         dl_dq, dl_dv, dl_df_ext, dl_dmat_w, dl_dstate_p, nullptr);
+}
+
+int dphd_backward_ex(dphd_deformable* h, const char* method, const double* q, const double* v, const double* a,
+                     const double* f_ext, double dt, const double* q_next, const double* v_next,
+                     const int* active_idx, int n_active, const double* dl_dq_next, const double* dl_dv_next,
+                     const char** keys, const double* vals, int nopts, double* dl_dq, double* dl_dv, double* dl_da,
+                     double* dl_df_ext, double* dl_dmat_w, double* dl_dact_w, double* dl_dstate_p,
+                     double* dl_dparams) {
+    (void)a; (void)active_idx; (void)n_active; (void)dl_da; (void)dl_dact_w;
+    return backward_impl(h, method, q, v, f_ext, dt, q_next, v_next, dl_dq_next, dl_dv_next, keys, vals, nopts,
+                         dl_dq, dl_dv, dl_df_ext, dl_dmat_w, dl_dstate_p, dl_dparams);
+}
+
+int dphd_forward_device(dphd_deformable* h, const char* method, const double* d_q, const double* d_v,
+                        const double* d_f, double dt, const char** keys, const double* vals, int nopts,
+                        double* d_qn, double* d_vn, void* stream) {
+    return guard([&] {
+        check_method(method);
+        DPHD_CHECK(d_q && d_v && d_f && d_qn && d_vn, "null device pointer");
+        DPHD_CHECK(dt > 0, "dt must be positive");
+        const dphd::Options o = dphd::Options::parse(to_map(keys, vals, nopts));
+        E(h).forward_device(d_q, d_v, d_f, dt, o, d_qn, d_vn, (cudaStream_t)stream);
+    });
+}
+
+int dphd_num_frames(const dphd_deformable* h) {
+    return h && h->eng ? (int)h->eng->stats.frame_iters.size() : -1;
+}
+int dphd_frame_stats(const dphd_deformable* h, int* it, int* cv) {
+    return guard([&] {
+        const Engine& e = E(h);
+        for (size_t i = 0; i < e.stats.frame_iters.size(); ++i) {
+            if (it) it[i] = e.stats.frame_iters[i];
+            if (cv) cv[i] = e.stats.frame_converged[i];
+        }
+    });
+}
+int dphd_reset_frame_stats(dphd_deformable* h) {
+    return guard([&] {
+        E(h).stats.frame_iters.clear();
+        E(h).stats.frame_converged.clear();
+    });
+}
+int dphd_last_backward_iters(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.last_bwd_iters : -1; }
+long long dphd_s_memory_bytes(const dphd_deformable* h) { return h && h->eng ? h->eng->s_memory_bytes() : -1; }
+long long dphd_s_nnz(const dphd_deformable* h) { return h && h->eng ? h->eng->s_nnz() : -1; }
+
+int dphd_debug_ainv(dphd_deformable* h, double dt, const double* b, double* x, int fp32) {
+    return guard([&] { E(h).apply_ainv(dt, b, x, fp32 != 0); });
+}
+int dphd_debug_host_sts(dphd_deformable* h, double dt, const double* b, double* x) {
+    return guard([&] { E(h).host_sts_apply(dt, b, x); });
+}
+int dphd_debug_local_step(dphd_deformable* h, double dt, const double* q, double* rhs) {
+    return guard([&] { E(h).local_step(dt, q, rhs); });
+}
+
+}  // extern "C"

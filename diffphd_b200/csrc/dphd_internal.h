@@ -1,0 +1,85 @@
+// Internal data structures of the B200 projective-dynamics step (not part of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace dphd {
+
+struct Error : std::runtime_error {
+    explicit Error(const std::string& s) : std::runtime_error(s) {}
+};
+#define DPHD_CHECK(cond, msg)                  \
+    do {                                       \
+        if (!(cond)) throw ::dphd::Error(msg); \
+    } while (0)
+
+enum EnergyType { kCorotated = 0, kVolume = 1, kNeoHookean = 2 };
+
+// One AddPdEnergy call (cpp/core/src/fem/deformable_pd_energy.cpp:43-153).
+struct PdEnergy {
+    int type = kCorotated;
+    std::vector<double> params;      // exactly as passed
+    std::vector<double> w_elem;      // per-element stiffness; empty when homogeneous
+    double w_mean = 0;               // stiffness(): mean of w_elem, or the scalar
+    double mu = 0, la = 0;           // Neo-Hookean means used by the proximal map
+    std::vector<uint8_t> in_set;     // element membership
+    bool all_elements = true;
+    double elem_w(int e) const { return w_elem.empty() ? w_mean : w_elem[e]; }
+};
+
+// Host model: the Deformable<3,k> state the AlgPhd path reads.
+struct HostModel {
+    int n = 0, m = 0, k = 0, s = 0;  // nodes, elements, nodes per element, samples per element
+    bool hex = true;
+    std::vector<double> X;           // 3n rest positions (node-major xyz)
+    std::vector<int> E;              // m*k connectivity
+    double density = 0, vol = 0;     // density, average element volume
+    std::vector<double> grad;        // hex: 8 samples x 8 nodes x 3; tet: m x 4 x 3
+    std::map<int, double> dirichlet;
+    std::vector<PdEnergy> energies;
+    bool has_gravity = false;
+    double gravity[3] = {0, 0, 0};
+    bool has_plane = false;
+    double plane_n[3] = {0, 0, 1}, plane_off = 0;
+    std::vector<int> contact_nodes;  // sorted unique
+    double mass() const { return density * vol; }
+    const double* g(int e, int smp) const { return &grad[((size_t)(hex ? 0 : e) * s + smp) * k * 3]; }
+};
+
+// Sparse-inverse factor S = D^-1/2 L^-1 P of the node-level PD matrix (A = P^T L D L^T P, shared by the
+// three axes because Dirichlet constraints fix whole nodes).  P is a nested-dissection ordering followed
+// by an elimination-tree postorder, so row i of L^-1 is dense on [lo_i, i] (its etree descendants form a
+// contiguous range): S is stored as one contiguous segment per row, column indices implicit.
+struct SFactor {
+    int n = 0;
+    std::vector<int> perm;           // perm[j] = node at permuted position j
+    std::vector<int> iperm;          // iperm[node] = position
+    std::vector<int> lo;             // first column of row i (= i - subtree_size + 1)
+    std::vector<int> parent;         // etree parent (permuted indices), -1 at roots
+    std::vector<double> Dinv_sqrt;
+    // values: row i occupies vals[row_ptr[i] .. row_ptr[i+1]) for columns lo[i]..i
+    std::vector<int64_t> row_ptr;
+    std::vector<double> vals;
+    int64_t nnz() const { return row_ptr.empty() ? 0 : row_ptr.back(); }
+    int64_t nnz_L = 0;
+    int max_depth = 0;
+};
+
+// Node-level PD matrix in CSR (original node order): A = diag(m/h^2 or 1) + sum_e w_e vol/s sum_s G_s G_s^T.
+struct NodeMatrix {
+    int n = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+};
+
+void init_samples(HostModel& M);
+double element_volume(const HostModel& M, int e);
+NodeMatrix assemble_A(const HostModel& M, double dt);
+std::vector<int> nested_dissection(const HostModel& M, const NodeMatrix& A);
+void build_sfactor(const NodeMatrix& A, const std::vector<int>& order, SFactor& S, int threads);
+
+}  // namespace dphd

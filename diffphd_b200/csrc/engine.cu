@@ -1,0 +1,687 @@
+// Forward and adjoint drivers of the B200 projective-dynamics step.
+//
+// Forward (ForwardProjectiveDynamicsAlgPhd, cpp/core/src/fem/deformable_projective_dynamics_forward_gpu.cpp:387-1594,
+// contact-free branch): q_tilde, then PD iterations  pd = local_step(q); q_raw = A^-1 (m/h^2 q_tilde + pd)
+// with Dirichlet rows zeroed; Dirichlet reset; Type-II Anderson acceleration; dual gate
+// |dq| <= rtol |q_prev| + atol and |d pd| <= rtol |pd_prev| + atol for iter > 0.  Every iteration is six
+// kernels on one stream; the stop decision is taken on the device and polled every `poll_chunk` iterations.
+//
+// Adjoint (BackwardProjectiveDynamicsAlgPhd, deformable_projective_dynamics_backward_gpu.cpp:648-917): the
+// backbone fixed point mu <- A^-1 (g_bar + K_pd mu) with the same acceleration, then the downstream routing
+// to dl/dq, dl/dv, dl/df_ext and the gravity parameters, and per-element parameter gradients.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <set>
+
+#include "engine.h"
+
+namespace dphd {
+
+#define CUDA_OK(x)                                                                                    \
+    do {                                                                                              \
+        cudaError_t e__ = (x);                                                                        \
+        if (e__ != cudaSuccess) throw Error(std::string("CUDA error: ") + cudaGetErrorString(e__) +   \
+                                            " at " + __FILE__ + ":" + std::to_string(__LINE__));      \
+    } while (0)
+
+void DeviceBuffer::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+void DeviceBuffer::alloc(size_t b) {
+    if (b == bytes && p) return;
+    release();
+    if (b == 0) return;
+    CUDA_OK(cudaMalloc(&p, b));
+    bytes = b;
+}
+void DeviceBuffer::copy_in(const void* src, size_t b) { CUDA_OK(cudaMemcpy(p, src, b, cudaMemcpyHostToDevice)); }
+
+Options Options::parse(const std::map<std::string, double>& m) {
+    Options o;
+    for (const char* req : {"max_pd_iter", "abs_tol", "rel_tol", "verbose", "thread_ct"})
+        DPHD_CHECK(m.count(req), std::string("Missing option ") + req + ".");
+    o.max_pd_iter = (int)m.at("max_pd_iter");
+    o.abs_tol = m.at("abs_tol");
+    o.rel_tol = m.at("rel_tol");
+    o.verbose = (int)m.at("verbose");
+    o.thread_ct = (int)m.at("thread_ct");
+    auto get = [&](const char* k, double def) { return m.count(k) ? m.at(k) : def; };
+    o.aa_window = (int)get("aa_window", 5);
+    o.friction_mu = get("friction_mu", 0);
+    o.restitution = get("restitution", 0);
+    o.contact_slop = get("friction_contact_slop", 1e-8);
+    o.bwd_clip = get("alg_phd_bwd_clip_norm", 1e6);
+    o.bwd_mean_stiffness = (int)get("bwd_mean_stiffness", 0);
+    o.bwd_cascade_cap = (int)get("bwd_cascade_cap", 1);
+    o.bwd_eigen_filter = (int)get("bwd_eigen_filter", 0);
+    o.fp32_bulk = (int)get("fp32_bulk", 0);
+    o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
+    DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
+               "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
+    DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
+    return o;
+}
+
+Engine::Engine(int vertex_dim, int element_dim) {
+    DPHD_CHECK(vertex_dim == 3, "Only 3D deformables (vertex_dim = 3) are supported on this path.");
+    DPHD_CHECK(element_dim == 8 || element_dim == 4, "element_dim must be 8 (hex) or 4 (tet).");
+    M.k = element_dim;
+    M.hex = element_dim == 8;
+    M.s = M.hex ? 8 : 1;
+}
+
+Engine::~Engine() {
+    if (h_ctrl_) cudaFreeHost(h_ctrl_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::init_from_arrays(const double* verts, int n, const int* elems, int m, double density,
+                              const std::string& material, double E, double nu) {
+    (void)E;
+    (void)nu;
+    DPHD_CHECK(material == "none",
+               "Only material 'none' (elasticity from AddPdEnergy) is supported on the AlgPhd path; got '" +
+                   material + "'.");
+    DPHD_CHECK(n > 0 && m > 0, "Empty mesh.");
+    M.n = n;
+    M.m = m;
+    M.X.assign(verts, verts + 3 * (size_t)n);
+    M.E.assign(elems, elems + (size_t)m * M.k);
+    for (int v : M.E) DPHD_CHECK(v >= 0 && v < n, "Element references a vertex out of range.");
+    M.density = density;
+    double sum = 0;
+    for (int e = 0; e < m; ++e) sum += element_volume(M, e);
+    M.vol = sum / m;
+    init_samples(M);
+    built_ = false;
+}
+
+void Engine::set_dirichlet(int dof, double val) {
+    DPHD_CHECK(dof >= 0 && dof < dofs(), "Dirichlet dof out of range.");
+    if (!M.dirichlet.count(dof)) built_ = false;
+    M.dirichlet[dof] = val;
+    device_ready_ = false;
+}
+
+void Engine::add_pd_energy(const std::string& type, const double* params, int np, const int* idx, int nidx) {
+    DPHD_CHECK(M.n > 0, "Initialize the mesh before adding energies.");
+    DPHD_CHECK((int)M.energies.size() < kMaxEnergies, "At most 4 PD element energies are supported.");
+    PdEnergy en;
+    if (type == "corotated") en.type = kCorotated;
+    else if (type == "volume") en.type = kVolume;
+    else if (type == "pd_neohookean") en.type = kNeoHookean;
+    else throw Error("Unsupported PD energy: " + type);
+    en.params.assign(params, params + np);
+    if (en.type != kNeoHookean) {
+        DPHD_CHECK(np == 1 || np == M.m, "Inconsistent param size: expected 1 (homogeneous) or element_num=" +
+                                             std::to_string(M.m) + " (per-element), got " + std::to_string(np));
+        if (np == 1) {
+            en.w_mean = params[0];
+        } else {
+            en.w_elem.assign(params, params + np);
+            en.w_mean = std::accumulate(en.w_elem.begin(), en.w_elem.end(), 0.0) / np;
+        }
+    } else {
+        DPHD_CHECK(np == 2 || np == 2 * M.m, "pd_neohookean expects params = [mu, lambda] or per-element "
+                                             "[mu_1, la_1, ..., mu_n, la_n] of length 2*element_num=" +
+                                                 std::to_string(2 * M.m) + ", got " + std::to_string(np));
+        if (np == 2) {
+            en.mu = params[0];
+            en.la = params[1];
+            en.w_mean = 2 * params[0];
+        } else {
+            double sm = 0, sl = 0;
+            en.w_elem.resize(M.m);
+            for (int e = 0; e < M.m; ++e) {
+                sm += params[2 * e];
+                sl += params[2 * e + 1];
+                en.w_elem[e] = 2 * params[2 * e];
+            }
+            en.mu = sm / M.m;
+            en.la = sl / M.m;
+            en.w_mean = std::accumulate(en.w_elem.begin(), en.w_elem.end(), 0.0) / M.m;
+        }
+    }
+    en.all_elements = (nidx == 0);
+    en.in_set.assign(M.m, en.all_elements ? 1 : 0);
+    for (int i = 0; i < nidx; ++i) {
+        DPHD_CHECK(idx[i] >= 0 && idx[i] < M.m, "Element index out of bound.");
+        en.in_set[idx[i]] = 1;
+    }
+    M.energies.push_back(en);
+    built_ = false;
+}
+
+void Engine::add_state_force(const std::string& type, const double* params, int np) {
+    DPHD_CHECK(type == "gravity", "Unsupported state force on this path: " + type);
+    DPHD_CHECK(np == 3, "Inconsistent params for GravitionalStateForce.");
+    DPHD_CHECK(!M.has_gravity, "Gravity was already added.");
+    M.has_gravity = true;
+    for (int d = 0; d < 3; ++d) M.gravity[d] = params[d];
+}
+
+void Engine::set_frictional_boundary(const std::string& type, const double* params, int np, const int* idx,
+                                     int nidx) {
+    DPHD_CHECK(type == "planar", "Unsupported frictional boundary on this path: " + type);
+    DPHD_CHECK(np == 4, "Incompatible parameter number.");
+    const double nn = std::sqrt(params[0] * params[0] + params[1] * params[1] + params[2] * params[2]);
+    DPHD_CHECK(nn > 2.220446049250313e-16, "Singular normal.");
+    for (int d = 0; d < 3; ++d) M.plane_n[d] = params[d] / nn;
+    M.plane_off = params[3] / nn;
+    std::set<int> u(idx, idx + nidx);
+    DPHD_CHECK((int)u.size() == nidx, "Duplicated vertex elements.");
+    for (int v : u) DPHD_CHECK(v >= 0 && v < M.n, "Frictional boundary vertex out of range.");
+    M.contact_nodes.assign(u.begin(), u.end());
+    M.has_plane = true;
+}
+
+int Engine::num_pd_params() const {
+    int t = 0;
+    for (const auto& e : M.energies) t += (int)e.params.size();
+    return t;
+}
+
+long long Engine::s_memory_bytes() const {
+    return (long long)d_vals64.bytes + (long long)d_vals32.bytes + (long long)d_row_off.bytes + d_row_a.bytes +
+           d_row_len.bytes + d_tile_ptr.bytes + d_tile_rows.bytes;
+}
+
+void Engine::ensure_built(double dt, int threads) {
+    DPHD_CHECK(M.n > 0, "Deformable is not initialized.");
+    DPHD_CHECK(!M.energies.empty(), "No PD energy was added.");
+    if (built_ && built_dt_ == dt) {
+        if (!device_ready_) build_device(threads);
+        return;
+    }
+    // One node-level factor serves all three axes only when Dirichlet constraints fix whole nodes.
+    std::map<int, int> per_node;
+    for (const auto& kv : M.dirichlet) per_node[kv.first / 3]++;
+    for (const auto& kv : per_node)
+        DPHD_CHECK(kv.second == 3, "Dirichlet constraints must fix all three DoFs of a node on this path (node " +
+                                       std::to_string(kv.first) + ").");
+    A = assemble_A(M, dt);
+    const std::vector<int> order = nested_dissection(M, A);
+    S = SFactor();
+    build_sfactor(A, order, S, threads);
+    built_ = true;
+    built_dt_ = dt;
+    device_ready_ = false;
+    build_device(threads);
+}
+
+void Engine::build_device(int threads) {
+    (void)threads;
+    if (!stream_) CUDA_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    if (!h_ctrl_) CUDA_OK(cudaMallocHost(&h_ctrl_, sizeof(Ctrl)));
+    const int n = M.n, m = M.m, k = M.k;
+    const int n3 = 3 * n;
+    npad_ = ((n + kTileCols - 1) / kTileCols) * kTileCols;
+    ntiles_ = npad_ / kTileCols;
+    // S rows, padded to 16-byte (4-value) aligned segments
+    std::vector<int> ra(n), rl(n);
+    std::vector<int64_t> ro(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        ra[i] = S.lo[i] & ~3;
+        rl[i] = ((i + 1 - ra[i]) + 3) & ~3;
+        ro[i + 1] = ro[i] + rl[i];
+    }
+    std::vector<double> v64(ro[n], 0.0);
+    for (int i = 0; i < n; ++i) {
+        const double* src = &S.vals[S.row_ptr[i]];
+        std::copy(src, src + (i - S.lo[i] + 1), &v64[ro[i] + (S.lo[i] - ra[i])]);
+    }
+    std::vector<float> v32(v64.begin(), v64.end());
+    // column tiles of S^T: rows whose padded segment meets the tile, ascending
+    std::vector<int> tcnt(ntiles_ + 1, 0);
+    for (int i = 0; i < n; ++i)
+        for (int t = ra[i] / kTileCols; t <= (ra[i] + rl[i] - 1) / kTileCols; ++t) tcnt[t + 1]++;
+    for (int t = 0; t < ntiles_; ++t) tcnt[t + 1] += tcnt[t];
+    std::vector<int> trows(tcnt[ntiles_]), tpos(tcnt.begin(), tcnt.end() - 1);
+    for (int i = 0; i < n; ++i)
+        for (int t = ra[i] / kTileCols; t <= (ra[i] + rl[i] - 1) / kTileCols; ++t) trows[tpos[t]++] = i;
+    d_row_a.upload(ra);
+    d_row_len.upload(rl);
+    d_row_off.upload(ro);
+    d_vals64.upload(v64);
+    d_vals32.upload(v32);
+    d_tile_ptr.upload(tcnt);
+    d_tile_rows.upload(trows);
+    d_perm.upload(S.perm);
+    d_iperm.upload(S.iperm);
+    // mesh, samples, constraints
+    dE.upload(M.E);
+    dX.upload(M.X);
+    dgrad.upload(M.grad);
+    std::vector<unsigned char> fn(n, 0), fd(n3, 0), ed(m, 0);
+    std::vector<double> fv(n3, 0.0), qb(n3, 0.0);
+    for (const auto& kv : M.dirichlet) {
+        fn[kv.first / 3] = 1;
+        fd[kv.first] = 1;
+        fv[kv.first] = kv.second;
+        qb[kv.first] = kv.second;
+    }
+    for (int e = 0; e < m; ++e)
+        for (int a = 0; a < k; ++a)
+            if (fn[M.E[(size_t)e * k + a]]) ed[e] = 1;
+    d_fixed_node.upload(fn);
+    d_fixed_dof.upload(fd);
+    d_fixed_val.upload(fv);
+    d_qb.upload(qb);
+    d_elem_dir.upload(ed);
+    // node <- (element, corner) incidence, ascending element order (deterministic gather)
+    std::vector<int> np(n + 1, 0);
+    for (int v : M.E) np[v + 1]++;
+    for (int i = 0; i < n; ++i) np[i + 1] += np[i];
+    std::vector<int> inc(np[n]), ip(np.begin(), np.end() - 1);
+    for (int e = 0; e < m; ++e)
+        for (int a = 0; a < k; ++a) inc[ip[M.E[(size_t)e * k + a]]++] = e * k + a;
+    d_node_ptr.upload(np);
+    d_node_inc.upload(inc);
+    // energies
+    for (int i = 0; i < kMaxEnergies; ++i) {
+        d_w[i].release();
+        d_w32[i].release();
+        d_mask[i].release();
+    }
+    for (size_t i = 0; i < M.energies.size(); ++i) {
+        const PdEnergy& en = M.energies[i];
+        if (!en.w_elem.empty()) {
+            d_w[i].upload(en.w_elem);
+            std::vector<float> w32(en.w_elem.begin(), en.w_elem.end());
+            d_w32[i].upload(w32);
+        }
+        if (!en.all_elements) d_mask[i].upload(en.in_set);
+    }
+    // work buffers
+    const size_t ld = (size_t)n3;
+    for (DeviceBuffer* b : {&d_q, &d_v, &d_f, &d_qt, &d_x, &d_xraw, &d_prev_pd, &d_lg, &d_lx, &d_qn, &d_vn, &d_gbar})
+        b->alloc(ld * sizeof(double));
+    d_dG.alloc(ld * kMaxWindow * sizeof(double));
+    d_dX.alloc(ld * kMaxWindow * sizeof(double));
+    d_part_gate.alloc(kRedBlocks * 2 * sizeof(double));
+    d_part_aa.alloc(kRedBlocks * 64 * sizeof(double));
+    d_part_upd.alloc(kRedBlocks * 3 * sizeof(double));
+    d_gravf.alloc(3 * sizeof(double));
+    d_elem_out64.alloc((size_t)m * k * 3 * sizeof(double));
+    d_elem_out32.alloc((size_t)m * k * 3 * sizeof(float));
+    d_vperm64.alloc((size_t)npad_ * 3 * sizeof(double));
+    d_vperm32.alloc((size_t)npad_ * 3 * sizeof(float));
+    d_y64.alloc((size_t)npad_ * 3 * sizeof(double));
+    d_y32.alloc((size_t)npad_ * 3 * sizeof(float));
+    CUDA_OK(cudaMemset(d_vperm64.p, 0, d_vperm64.bytes));
+    CUDA_OK(cudaMemset(d_vperm32.p, 0, d_vperm32.bytes));
+    CUDA_OK(cudaMemset(d_y64.p, 0, d_y64.bytes));
+    CUDA_OK(cudaMemset(d_y32.p, 0, d_y32.bytes));
+    d_ctrl.alloc(sizeof(Ctrl));
+    CUDA_OK(cudaMemset(d_ctrl.p, 0, sizeof(Ctrl)));
+    double gf[3] = {0, 0, 0};
+    if (M.has_gravity)
+        for (int d = 0; d < 3; ++d) gf[d] = M.mass() * M.gravity[d];
+    d_gravf.copy_in(gf, sizeof(gf));
+    device_ready_ = true;
+}
+
+EnergyPack Engine::energy_pack() const {
+    EnergyPack ep{};
+    ep.count = (int)M.energies.size();
+    for (int i = 0; i < ep.count; ++i) {
+        const PdEnergy& en = M.energies[i];
+        ElemEnergyDev& d = ep.en[i];
+        d.type = en.type;
+        d.per_element = en.w_elem.empty() ? 0 : 1;
+        d.w_mean = en.w_mean;
+        d.mu = en.mu;
+        d.la = en.la;
+        d.w = d_w[i].as<double>();
+        d.w32 = d_w32[i].as<float>();
+        d.mask = d_mask[i].as<unsigned char>();
+    }
+    return ep;
+}
+
+void Engine::launch_ainv(bool fp32, cudaStream_t st) {
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    if (fp32) {
+        launch_spmv_S<float>(M.n, d_row_off.as<int64_t>(), d_row_a.as<int>(), d_row_len.as<int>(),
+                             d_vals32.as<float>(), d_vperm32.as<float>(), npad_, d_y32.as<float>(), c, st);
+        launch_spmv_ST<float>(M.n, ntiles_, d_tile_ptr.as<int>(), d_tile_rows.as<int>(), d_row_off.as<int64_t>(),
+                              d_row_a.as<int>(), d_row_len.as<int>(), d_vals32.as<float>(), d_y32.as<float>(), npad_,
+                              d_perm.as<int>(), d_xraw.as<double>(), c, st);
+    } else {
+        launch_spmv_S<double>(M.n, d_row_off.as<int64_t>(), d_row_a.as<int>(), d_row_len.as<int>(),
+                              d_vals64.as<double>(), d_vperm64.as<double>(), npad_, d_y64.as<double>(), c, st);
+        launch_spmv_ST<double>(M.n, ntiles_, d_tile_ptr.as<int>(), d_tile_rows.as<int>(), d_row_off.as<int64_t>(),
+                               d_row_a.as<int>(), d_row_len.as<int>(), d_vals64.as<double>(), d_y64.as<double>(),
+                               npad_, d_perm.as<int>(), d_xraw.as<double>(), c, st);
+    }
+}
+
+static void init_ctrl(Ctrl* h, int mode, const Options& o, int max_iter, double clip) {
+    std::memset(h, 0, sizeof(Ctrl));
+    h->max_iter = max_iter;
+    h->window = o.aa_window;
+    h->mode = mode;
+    h->rel_tol = o.rel_tol;
+    h->abs_tol = o.abs_tol;
+    h->clip = clip;
+}
+
+void Engine::check_status(const char* where) {
+    if (h_ctrl_->status & kStatusSingularF) throw Error("Singular F.");
+    (void)where;
+}
+
+void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st) {
+    const int n = M.n, n3 = 3 * n;
+    const double inv_h2m = M.mass() / (h * h);
+    const double vol_over_s = M.vol / M.s;
+    const EnergyPack ep = energy_pack();
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    CUDA_OK(cudaMemcpyAsync(d_x.p, dq_in, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(cudaMemsetAsync(d_prev_pd.p, 0, n3 * sizeof(double), st));
+    init_ctrl(h_ctrl_, 0, o, o.max_pd_iter, 0.0);
+    CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    const bool f32 = o.fp32_bulk != 0;
+    int launched = 0;
+    int chunk = std::min(o.poll_chunk, 4);
+    while (launched < o.max_pd_iter) {
+        const int todo = std::min(chunk, o.max_pd_iter - launched);
+        for (int it = 0; it < todo; ++it) {
+            if (f32) {
+                launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                       d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                                       d_elem_out32.as<float>(), c, st);
+                launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out32.as<float>(),
+                                         d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(),
+                                         d_iperm.as<int>(), d_vperm32.as<float>(), npad_, nullptr,
+                                         d_prev_pd.as<double>(), d_part_gate.as<double>(), c, st);
+            } else {
+                launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                        d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                                        d_elem_out64.as<double>(), c, st);
+                launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
+                                          d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(),
+                                          d_iperm.as<int>(), d_vperm64.as<double>(), npad_, nullptr,
+                                          d_prev_pd.as<double>(), d_part_gate.as<double>(), c, st);
+            }
+            launch_ainv(f32, st);
+            launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
+                             d_lx.as<double>(), n3, d_part_aa.as<double>(), c, st);
+            launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3,
+                             d_part_upd.as<double>(), d_part_gate.as<double>(), kRedBlocks, c, st);
+        }
+        CUDA_OK(cudaGetLastError());
+        launched += todo;
+        CUDA_OK(cudaMemcpyAsync(h_ctrl_, c, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        if (h_ctrl_->done) break;
+        chunk = std::min(chunk * 2, std::max(o.poll_chunk, 4));
+    }
+    check_status("forward");
+    stats.frame_iters.push_back(h_ctrl_->iter);
+    stats.frame_converged.push_back(h_ctrl_->converged);
+    if (!h_ctrl_->converged && o.verbose >= 0)
+        std::fprintf(stderr, "frame: %zu alg_phd: PD loop did not converge.\n", stats.frame_iters.size());
+}
+
+void Engine::forward_device(const double* dq, const double* dv, const double* df, double dt, const Options& o,
+                            double* dqn, double* dvn, cudaStream_t st) {
+    DPHD_CHECK(!M.has_plane || M.contact_nodes.empty(),
+               "Frictional contact is not available in this build of the device step.");
+    ensure_built(dt, o.thread_ct);
+    const int n3 = dofs();
+    const double h2m = dt * dt / M.mass();
+    launch_qtilde(n3, dq, dv, df, dt, h2m, d_gravf.as<double>(), d_qt.as<double>(), st);
+    run_forward_loop(dq, dt, o, st);
+    CUDA_OK(cudaMemcpyAsync(dqn, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    launch_velocity(n3, d_x.as<double>(), dq, 1.0 / dt, dvn, st);
+    CUDA_OK(cudaGetLastError());
+}
+
+void Engine::forward(const double* q, const double* v, const double* f_ext, double dt, const Options& o,
+                     double* q_next, double* v_next, std::vector<int>& active) {
+    ensure_built(dt, o.thread_ct);
+    const int n3 = dofs();
+    cudaStream_t st = stream_;
+    CUDA_OK(cudaMemcpyAsync(d_q.p, q, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_v.p, v, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_f.p, f_ext, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    forward_device(d_q.as<double>(), d_v.as<double>(), d_f.as<double>(), dt, o, d_qn.as<double>(),
+                   d_vn.as<double>(), st);
+    CUDA_OK(cudaMemcpyAsync(q_next, d_qn.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(v_next, d_vn.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    active.clear();
+}
+
+void Engine::backward(const double* q, const double* v, const double* f_ext, double dt, const double* q_next,
+                      const double* v_next, const double* dl_dq_next, const double* dl_dv_next, const Options& o,
+                      double* dl_dq, double* dl_dv, double* dl_df, double* dl_dmat_w, double* dl_dparams,
+                      double* dl_dstate_p) {
+    (void)q; (void)v; (void)f_ext; (void)v_next;
+    DPHD_CHECK(!M.has_plane || M.contact_nodes.empty(),
+               "Frictional contact is not available in this build of the adjoint.");
+    ensure_built(dt, o.thread_ct);
+    const int n = M.n, n3 = 3 * n, m = M.m;
+    const double h = dt, inv_h = 1.0 / h;
+    const double mass = M.mass(), inv_h2m = mass / (h * h), h2m = h * h / mass;
+    cudaStream_t st = stream_;
+    std::vector<double> gbar(n3);
+    for (int i = 0; i < n3; ++i) {
+        dl_dq[i] = -dl_dv_next[i] * inv_h;
+        dl_dv[i] = 0;
+        dl_df[i] = 0;
+        gbar[i] = dl_dq_next[i] + dl_dv_next[i] * inv_h;
+    }
+    CUDA_OK(cudaMemcpyAsync(d_qn.p, q_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_gbar.p, gbar.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    const EnergyPack ep = energy_pack();
+    const double vol_over_s = M.vol / M.s;
+    d_J.alloc((size_t)m * M.s * 81 * sizeof(double));
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
+    CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    launch_jac_build(m, M.k, M.s, dE.as<int>(), d_qn.as<double>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                     o.bwd_mean_stiffness, o.bwd_eigen_filter, d_J.as<double>(), c, st);
+    CUDA_OK(cudaMemsetAsync(d_x.p, 0, n3 * sizeof(double), st));
+    int launched = 0, chunk = std::min(o.poll_chunk, 4);
+    while (launched < o.max_pd_iter) {
+        const int todo = std::min(chunk, o.max_pd_iter - launched);
+        for (int it = 0; it < todo; ++it) {
+            launch_kpd_elem(m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
+                            d_J.as<double>(), d_elem_out64.as<double>(), c, st);
+            launch_gather_bwd(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
+                              d_gbar.as<double>(), d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                              d_vperm64.as<double>(), npad_, c, st);
+            launch_ainv(false, st);
+            launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
+                             d_lx.as<double>(), n3, d_part_aa.as<double>(), c, st);
+            launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3,
+                             d_part_upd.as<double>(), d_part_gate.as<double>(), 0, c, st);
+        }
+        CUDA_OK(cudaGetLastError());
+        launched += todo;
+        CUDA_OK(cudaMemcpyAsync(h_ctrl_, c, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        if (h_ctrl_->done) break;
+        chunk = std::min(chunk * 2, std::max(o.poll_chunk, 4));
+    }
+    stats.last_bwd_iters = h_ctrl_->iter;
+    stats.last_filtered = (int)h_ctrl_->arrive[3];
+    const int np = num_pd_params();
+    const int ne = (int)M.energies.size();
+    for (int i = 0; i < ne; ++i) dl_dmat_w[i] = 0;
+    for (int i = 0; i < np; ++i) dl_dparams[i] = 0;
+    for (int i = 0; i < num_state_params(); ++i) dl_dstate_p[i] = 0;
+    const bool diverged = (h_ctrl_->status & (kStatusDiverged | kStatusNonFinite)) != 0;
+    if (diverged) return;  // reference: a diverged backbone contributes nothing downstream
+    std::vector<double> mu(n3);
+    CUDA_OK(cudaMemcpyAsync(mu.data(), d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // parameter gradients at q_next
+    d_gw.alloc((size_t)kMaxEnergies * m * sizeof(double));
+    d_gmat.alloc((size_t)kMaxEnergies * m * sizeof(double));
+    d_gnh.alloc((size_t)kMaxEnergies * m * 2 * sizeof(double));
+    launch_param_grad(m, M.k, M.s, dE.as<int>(), d_qn.as<double>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
+                      vol_over_s, ep, d_gw.as<double>(), d_gmat.as<double>(), d_gnh.as<double>(), st);
+    std::vector<double> gw((size_t)ne * m), gmat((size_t)ne * m), gnh((size_t)ne * m * 2);
+    CUDA_OK(cudaMemcpyAsync(gw.data(), d_gw.p, gw.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(gmat.data(), d_gmat.p, gmat.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(gnh.data(), d_gnh.p, gnh.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    // downstream routing (backward_gpu.cpp:881-917)
+    std::vector<double> inj(n3);
+    double in2 = 0, g2 = 0;
+    for (int i = 0; i < n3; ++i) {
+        inj[i] = inv_h2m * mu[i];
+        in2 += inj[i] * inj[i];
+        g2 += gbar[i] * gbar[i];
+    }
+    if (o.bwd_cascade_cap) {
+        const double cap = std::sqrt(g2) + 1.0, in = std::sqrt(in2);
+        if (in > cap)
+            for (auto& x : inj) x *= cap / in;
+    }
+    for (int i = 0; i < n3; ++i) {
+        dl_dq[i] += inj[i];
+        dl_df[i] += h2m * inj[i];
+        dl_dv[i] += h * inj[i];
+    }
+    if (M.has_gravity)
+        for (int i = 0; i < n3; ++i) dl_dstate_p[i % 3] += h2m * inj[i] * mass;
+    int off = 0;
+    for (int k = 0; k < ne; ++k) {
+        const PdEnergy& en = M.energies[k];
+        const double* w = &gw[(size_t)k * m];
+        double tot = 0;
+        for (int e = 0; e < m; ++e) tot += gmat[(size_t)k * m + e];
+        dl_dmat_w[k] = tot;
+        const int npk = (int)en.params.size();
+        if (en.type != kNeoHookean) {
+            if (npk == 1) {
+                double s = 0;
+                for (int e = 0; e < m; ++e) s += w[e];
+                dl_dparams[off] = s;
+            } else {
+                for (int e = 0; e < m; ++e) dl_dparams[off + e] = w[e];
+            }
+        } else {
+            double gmb = 0, glb = 0;
+            for (int e = 0; e < m; ++e) {
+                gmb += gnh[((size_t)k * m + e) * 2];
+                glb += gnh[((size_t)k * m + e) * 2 + 1];
+            }
+            if (npk == 2) {
+                double s = 0;
+                for (int e = 0; e < m; ++e) s += w[e];
+                dl_dparams[off] = 2 * s + gmb;
+                dl_dparams[off + 1] = glb;
+            } else {
+                for (int e = 0; e < m; ++e) {
+                    dl_dparams[off + 2 * e] = 2 * w[e] + gmb / m;
+                    dl_dparams[off + 2 * e + 1] = glb / m;
+                }
+            }
+        }
+        off += npk;
+    }
+}
+
+void Engine::apply_ainv(double dt, const double* b, double* x, bool fp32) {
+    ensure_built(dt, 0);
+    const int n = M.n, n3 = 3 * n;
+    cudaStream_t st = stream_;
+    // permuted SoA input, Dirichlet rows zero (as the forward's b_bc)
+    std::vector<double> v((size_t)npad_ * 3, 0.0);
+    std::vector<unsigned char> fixed(n, 0);
+    for (const auto& kv : M.dirichlet) fixed[kv.first / 3] = 1;
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) v[(size_t)d * npad_ + S.iperm[i]] = fixed[i] ? 0.0 : b[3 * i + d];
+    init_ctrl(h_ctrl_, 0, Options(), 1, 0);
+    CUDA_OK(cudaMemcpyAsync(d_ctrl.p, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    if (fp32) {
+        std::vector<float> v32(v.begin(), v.end());
+        CUDA_OK(cudaMemcpyAsync(d_vperm32.p, v32.data(), v32.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        launch_ainv(true, st);
+        CUDA_OK(cudaStreamSynchronize(st));
+    } else {
+        CUDA_OK(cudaMemcpyAsync(d_vperm64.p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        launch_ainv(false, st);
+    }
+    CUDA_OK(cudaMemcpyAsync(x, d_xraw.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+}
+
+// Host self-check of the factor (the reference runs the same S^T S v vs LDL^T solve check on the host,
+// forward_gpu.cpp:653-670): x = S^T (S v) with the host copy of S, Dirichlet rows zero.
+void Engine::host_sts_apply(double dt, const double* b, double* x) {
+    DPHD_CHECK(M.n > 0 && !M.energies.empty(), "Deformable is not initialized.");
+    if (!(built_ && built_dt_ == dt)) {
+        std::map<int, int> per_node;
+        for (const auto& kv : M.dirichlet) per_node[kv.first / 3]++;
+        for (const auto& kv : per_node) DPHD_CHECK(kv.second == 3, "Dirichlet constraints must fix whole nodes.");
+        A = assemble_A(M, dt);
+        S = SFactor();
+        build_sfactor(A, nested_dissection(M, A), S, 0);
+        built_ = true;
+        built_dt_ = dt;
+        device_ready_ = false;
+    }
+    const int n = M.n;
+    std::vector<unsigned char> fixed(n, 0);
+    for (const auto& kv : M.dirichlet) fixed[kv.first / 3] = 1;
+    for (int d = 0; d < 3; ++d) {
+        std::vector<double> v(n), y(n, 0.0), z(n, 0.0);
+        for (int i = 0; i < n; ++i) v[S.iperm[i]] = fixed[i] ? 0.0 : b[3 * i + d];
+        for (int i = 0; i < n; ++i) {
+            const double* r = &S.vals[S.row_ptr[i]] - S.lo[i];
+            double s = 0;
+            for (int c = S.lo[i]; c <= i; ++c) s += r[c] * v[c];
+            y[i] = s;
+        }
+        for (int i = 0; i < n; ++i) {
+            const double* r = &S.vals[S.row_ptr[i]] - S.lo[i];
+            for (int c = S.lo[i]; c <= i; ++c) z[c] += r[c] * y[i];
+        }
+        for (int i = 0; i < n; ++i) x[3 * i + d] = z[S.iperm[i]];
+    }
+}
+
+void Engine::local_step(double dt, const double* q, double* rhs) {
+    ensure_built(dt, 0);
+    const int n = M.n, n3 = 3 * n;
+    cudaStream_t st = stream_;
+    CUDA_OK(cudaMemcpyAsync(d_x.p, q, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemsetAsync(d_prev_pd.p, 0, n3 * sizeof(double), st));
+    CUDA_OK(cudaMemsetAsync(d_qt.p, 0, n3 * sizeof(double), st));
+    init_ctrl(h_ctrl_, 0, Options(), 1, 0);
+    CUDA_OK(cudaMemcpyAsync(d_ctrl.p, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    const EnergyPack ep = energy_pack();
+    launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                            d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, M.vol / M.s, ep,
+                            d_elem_out64.as<double>(), d_ctrl.as<Ctrl>(), st);
+    launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
+                              d_qt.as<double>(), 0.0, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                              d_vperm64.as<double>(), npad_, nullptr, d_prev_pd.as<double>(), d_part_gate.as<double>(),
+                              d_ctrl.as<Ctrl>(), st);
+    // the gather leaves pd (node-major) in prev_pd
+    CUDA_OK(cudaMemcpyAsync(rhs, d_prev_pd.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(h_ctrl_, d_ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaGetLastError());
+    check_status("local_step");
+}
+
+}  // namespace dphd

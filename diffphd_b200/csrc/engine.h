@@ -1,0 +1,120 @@
+// Engine: one Deformable<3,k> on one GPU — builder state, the sparse-inverse factor in HBM, and the
+// forward / adjoint drivers of the projective-dynamics step.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "dphd_internal.h"
+#include "kernels.cuh"
+
+namespace dphd {
+
+struct Options {
+    int max_pd_iter = 0;
+    double abs_tol = 0, rel_tol = 0;
+    int verbose = 0, thread_ct = 0;
+    int aa_window = 5;
+    double friction_mu = 0, restitution = 0, contact_slop = 1e-8;
+    double bwd_clip = 1e6;
+    int bwd_mean_stiffness = 0;  // reference backward semantics: mean stiffness inside K_pd
+    int bwd_cascade_cap = 1;     // reference cap of the injected adjoint at |g_bar| + 1
+    int bwd_eigen_filter = 0;    // 0 off (exact adjoint), 1 clamp, 2 abs
+    int fp32_bulk = 0;           // projection and S/S^T SpMVs in FP32
+    int poll_chunk = 8;
+    static Options parse(const std::map<std::string, double>& m);
+};
+
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { release(); }
+    void release();
+    void alloc(size_t b);
+    template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+    template <typename T> void upload(const std::vector<T>& v) {
+        alloc(v.size() * sizeof(T));
+        if (!v.empty()) copy_in(v.data(), v.size() * sizeof(T));
+    }
+    void copy_in(const void* src, size_t b);
+};
+
+struct StepStats {
+    std::vector<int> frame_iters, frame_converged;
+    int last_bwd_iters = 0, last_filtered = 0;
+};
+
+class Engine {
+public:
+    Engine(int vertex_dim, int element_dim);
+    ~Engine();
+
+    // builder (mirrors Deformable's Python-facing API)
+    void init_from_arrays(const double* verts, int n, const int* elems, int m, double density,
+                          const std::string& material, double E, double nu);
+    void set_dirichlet(int dof, double val);
+    void add_pd_energy(const std::string& type, const double* params, int np, const int* idx, int nidx);
+    void add_state_force(const std::string& type, const double* params, int np);
+    void set_frictional_boundary(const std::string& type, const double* params, int np, const int* idx, int nidx);
+
+    int dofs() const { return 3 * M.n; }
+    int num_pd_energies() const { return (int)M.energies.size(); }
+    int num_pd_params() const;
+    int num_state_params() const { return M.has_gravity ? 3 : 0; }
+    long long s_memory_bytes() const;
+    long long s_nnz() const { return S.nnz(); }
+    int s_depth() const { return S.max_depth; }
+
+    // host-pointer step (drop-in for PyForward / PyBackward)
+    void forward(const double* q, const double* v, const double* f_ext, double dt, const Options& o, double* q_next,
+                 double* v_next, std::vector<int>& active);
+    void backward(const double* q, const double* v, const double* f_ext, double dt, const double* q_next,
+                  const double* v_next, const double* dl_dq_next, const double* dl_dv_next, const Options& o,
+                  double* dl_dq, double* dl_dv, double* dl_df, double* dl_dmat_w, double* dl_dparams,
+                  double* dl_dstate_p);
+    // device-pointer step (inputs and outputs already in HBM, launched on `stream`)
+    void forward_device(const double* d_q, const double* d_v, const double* d_f, double dt, const Options& o,
+                        double* d_q_next, double* d_v_next, cudaStream_t stream);
+
+    // diagnostics used by the tests
+    void apply_ainv(double dt, const double* b, double* x, bool fp32);
+    void host_sts_apply(double dt, const double* b, double* x);
+    void local_step(double dt, const double* q, double* rhs);
+
+    StepStats stats;
+    HostModel M;
+
+private:
+    void ensure_built(double dt, int threads);
+    void build_device(int threads);
+    EnergyPack energy_pack() const;
+    void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st);
+    void launch_ainv(bool fp32, cudaStream_t st);  // d_vperm -> d_xraw
+    void check_status(const char* where);
+
+    bool built_ = false;
+    double built_dt_ = -1;
+    SFactor S;
+    NodeMatrix A;
+    int npad_ = 0, ntiles_ = 0;
+    bool device_ready_ = false;
+    cudaStream_t stream_ = nullptr;
+
+    DeviceBuffer dE, dX, dgrad, d_elem_dir, d_fixed_node, d_fixed_dof, d_fixed_val, d_qb;
+    DeviceBuffer d_node_ptr, d_node_inc, d_perm, d_iperm;
+    DeviceBuffer d_row_off, d_row_a, d_row_len, d_vals64, d_vals32, d_tile_ptr, d_tile_rows;
+    DeviceBuffer d_w[kMaxEnergies], d_w32[kMaxEnergies], d_mask[kMaxEnergies];
+    DeviceBuffer d_q, d_v, d_f, d_qt, d_x, d_xraw, d_prev_pd, d_dG, d_dX, d_lg, d_lx;
+    DeviceBuffer d_part_gate, d_part_aa, d_part_upd, d_gravf;
+    DeviceBuffer d_elem_out64, d_elem_out32, d_vperm64, d_vperm32, d_y64, d_y32;
+    DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
+    DeviceBuffer d_ctrl;
+    Ctrl* h_ctrl_ = nullptr;  // pinned mirror
+};
+
+}  // namespace dphd

@@ -1,0 +1,928 @@
+// sm_100a kernels of the projective-dynamics step and its adjoint.
+//
+// All reductions are deterministic: fixed grids, per-block partials, and a last-arriving block that sums
+// the partials in block order.  No floating-point atomics are used.
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace dphd {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of NV values per thread; result valid in thread 0.  `sh` holds NV * 32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_sum(double* v, double* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        const double s = warp_sum(v[i]);
+        if (lane == 0) sh[i * 32 + wid] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            double s = lane < nw ? sh[i * 32 + lane] : 0.0;
+            s = warp_sum(s);
+            v[i] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// Last-block election after each block stored its partials.
+__device__ __forceinline__ bool arrive_last(unsigned int* counter) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return last;
+}
+
+template <typename T>
+__device__ __forceinline__ T ld_weight(const ElemEnergyDev& en, int e);
+template <>
+__device__ __forceinline__ double ld_weight<double>(const ElemEnergyDev& en, int e) {
+    return en.per_element ? __ldg(en.w + e) : en.w_mean;
+}
+template <>
+__device__ __forceinline__ float ld_weight<float>(const ElemEnergyDev& en, int e) {
+    return en.per_element ? __ldg(en.w32 + e) : (float)en.w_mean;
+}
+
+// Deformation gradient F(i,j) = sum_a x_a[i] grad_a[j] over the element's nodes (FP64 accumulation).
+template <int K>
+__device__ __forceinline__ void def_grad(const int* __restrict__ E, int e, const double* __restrict__ x,
+                                         const double* __restrict__ g, double* F) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) F[i] = 0.0;
+#pragma unroll
+    for (int a = 0; a < K; ++a) {
+        const int node = __ldg(E + (size_t)e * K + a);
+        const double x0 = x[3 * node], x1 = x[3 * node + 1], x2 = x[3 * node + 2];
+        const double g0 = __ldg(g + a * 3), g1 = __ldg(g + a * 3 + 1), g2 = __ldg(g + a * 3 + 2);
+        F[0] += x0 * g0; F[1] += x1 * g0; F[2] += x2 * g0;
+        F[3] += x0 * g1; F[4] += x1 * g1; F[5] += x2 * g1;
+        F[6] += x0 * g2; F[7] += x1 * g2; F[8] += x2 * g2;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Forward local step (deformable_projective_dynamics_forward.cpp:186-292), one thread per (element, sample);
+// for hexes the 8 samples of an element are 8 consecutive lanes and are summed by a shuffle butterfly.
+// ------------------------------------------------------------------------------------------------
+template <typename T, int K, int S>
+__global__ void __launch_bounds__(kThreads) k_elem_fwd(int m, const int* __restrict__ E, const double* __restrict__ q,
+                                                       const double* __restrict__ qb,
+                                                       const unsigned char* __restrict__ elem_dir,
+                                                       const double* __restrict__ grad, double vol_over_s,
+                                                       EnergyPack ep, T* __restrict__ out, Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = t / S, smp = t % S;
+    const bool valid = e < m;
+    T acc[K][3];
+#pragma unroll
+    for (int a = 0; a < K; ++a) acc[a][0] = acc[a][1] = acc[a][2] = T(0);
+    if (valid) {
+        const double* g = (S == 8) ? grad + smp * 24 : grad + (size_t)e * 12;
+        double Fd[9];
+        def_grad<K>(E, e, q, g, Fd);
+        T F[9], Fb[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) { F[i] = (T)Fd[i]; Fb[i] = T(0); }
+        if (elem_dir[e]) {
+            double Fbd[9];
+            def_grad<K>(E, e, qb, g, Fbd);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) Fb[i] = (T)Fbd[i];
+        }
+        T U[9], V[9], sig[3];
+        svd3<T>(F, U, sig, V);
+        T P[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) P[i] = T(0);
+        bool ok = true;
+        for (int k = 0; k < ep.count; ++k) {
+            const ElemEnergyDev& en = ep.en[k];
+            if (en.mask && !en.mask[e]) continue;
+            const T w = ld_weight<T>(en, e) * (T)vol_over_s;
+            T Bp[9];
+            ok = project<T>(en.type, (T)en.mu, (T)en.la, (T)en.w_mean, U, sig, V, Bp) && ok;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) P[i] += w * (Bp[i] - Fb[i]);
+        }
+        if (!ok) atomicOr(&ctrl->status, (int)kStatusSingularF);
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            const T g0 = (T)__ldg(g + a * 3), g1 = (T)__ldg(g + a * 3 + 1), g2 = (T)__ldg(g + a * 3 + 2);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) acc[a][i] = P[i] * g0 + P[i + 3] * g1 + P[i + 6] * g2;
+        }
+    }
+    if (S == 8) {
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+            for (int a = 0; a < K; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) acc[a][i] += __shfl_xor_sync(0xffffffffu, acc[a][i], o);
+        if (valid) {
+#pragma unroll
+            for (int a = 0; a < K; ++a)
+                if (a == smp) {
+                    T* o = out + ((size_t)e * K + a) * 3;
+                    o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
+                }
+        }
+    } else if (valid) {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            T* o = out + ((size_t)e * K + a) * 3;
+            o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __restrict__ node_ptr,
+                                                         const int* __restrict__ node_inc, const T* __restrict__ eo,
+                                                         const double* __restrict__ qt, double inv_h2m,
+                                                         const unsigned char* __restrict__ fixed,
+                                                         const int* __restrict__ iperm, T* __restrict__ v, int npad,
+                                                         double* __restrict__ prev, double* __restrict__ part,
+                                                         Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ double sh[2 * 32];
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double p0 = 0, p1 = 0, p2 = 0;
+        const int b = node_ptr[i], e = node_ptr[i + 1];
+        for (int idx = b; idx < e; ++idx) {
+            const T* c = eo + (size_t)node_inc[idx] * 3;
+            p0 += (double)c[0]; p1 += (double)c[1]; p2 += (double)c[2];
+        }
+        const double p[3] = {p0, p1, p2};
+        const int j = iperm[i];
+        const bool fx = fixed[i] != 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double pr = prev[3 * i + d];
+            acc[0] += (p[d] - pr) * (p[d] - pr);
+            acc[1] += pr * pr;
+            prev[3 * i + d] = p[d];
+            v[(size_t)d * npad + j] = fx ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d]);
+        }
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2] = acc[0];
+        part[blockIdx.x * 2 + 1] = acc[1];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Sparse-inverse SpMV pair.  S row i is a dense segment of row_len[i] values starting at column row_a[i]
+// (both multiples of 4, zero-padded), so loads are 16-byte vectors with implicit column indices.
+// ------------------------------------------------------------------------------------------------
+template <typename T> struct Vec4;
+template <> struct Vec4<float> {
+    float v[4];
+    __device__ __forceinline__ void load(const float* p) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+    __device__ __forceinline__ void load_stream(const float* p) {
+        const float4 x = __ldcs(reinterpret_cast<const float4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+};
+template <> struct Vec4<double> {
+    double v[4];
+    __device__ __forceinline__ void load(const double* p) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    __device__ __forceinline__ void load_stream(const double* p) {
+        const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_spmv_S(int n, const int64_t* __restrict__ row_off,
+                                                     const int* __restrict__ row_a, const int* __restrict__ row_len,
+                                                     const T* __restrict__ vals, const T* __restrict__ v, int npad,
+                                                     T* __restrict__ y, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int i = n - 1 - warp;  // rows near the etree root are the longest: schedule them first
+    const int64_t off = row_off[i];
+    const int a = row_a[i], len = row_len[i];
+    T s0 = T(0), s1 = T(0), s2 = T(0);
+    for (int c = lane * 4; c < len; c += 128) {
+        Vec4<T> sv, v0, v1, v2;
+        sv.load_stream(vals + off + c);
+        v0.load(v + a + c);
+        v1.load(v + npad + a + c);
+        v2.load(v + 2 * (size_t)npad + a + c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            s0 += sv.v[q] * v0.v[q];
+            s1 += sv.v[q] * v1.v[q];
+            s2 += sv.v[q] * v2.v[q];
+        }
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    if (lane == 0) {
+        y[i] = s0;
+        y[npad + i] = s1;
+        y[2 * (size_t)npad + i] = s2;
+    }
+}
+
+template <typename T, int NW>
+__global__ void __launch_bounds__(NW * 32) k_spmv_ST(int n, const int* __restrict__ tile_ptr,
+                                                     const int* __restrict__ tile_rows,
+                                                     const int64_t* __restrict__ row_off,
+                                                     const int* __restrict__ row_a, const int* __restrict__ row_len,
+                                                     const T* __restrict__ vals, const T* __restrict__ y, int npad,
+                                                     const int* __restrict__ perm, double* __restrict__ x_out,
+                                                     const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ T red[NW][3][kTileCols];
+    const int tile = blockIdx.x, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = tile * kTileCols + lane * 4;
+    T acc[3][4];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[d][q] = T(0);
+    const int pe = tile_ptr[tile + 1];
+    for (int p = tile_ptr[tile] + wid; p < pe; p += NW) {
+        const int i = __ldg(tile_rows + p);
+        const int a = __ldg(row_a + i), len = __ldg(row_len + i);
+        if (c >= a && c + 4 <= a + len) {
+            Vec4<T> sv;
+            sv.load_stream(vals + __ldg(row_off + i) + (c - a));
+            const T y0 = __ldg(y + i), y1 = __ldg(y + npad + i), y2 = __ldg(y + 2 * (size_t)npad + i);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc[0][q] += sv.v[q] * y0;
+                acc[1][q] += sv.v[q] * y1;
+                acc[2][q] += sv.v[q] * y2;
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) red[wid][d][lane * 4 + q] = acc[d][q];
+    __syncthreads();
+    for (int t = threadIdx.x; t < 3 * kTileCols; t += NW * 32) {
+        const int d = t / kTileCols, col = t % kTileCols;
+        T s = T(0);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) s += red[w][d][col];
+        const int j = tile * kTileCols + col;
+        if (j < n) x_out[3 * (size_t)__ldg(perm + j) + d] = (double)s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Type-II Anderson acceleration (forward_gpu.cpp:1340-1379; backward_gpu.cpp:825-859) and the gate.
+// History: `count` entries (x_prev, g); differences dG, dX live in a ring of `window` slots starting at
+// `head`.  k_aa_reduce pushes the new entry, forms the Gram system and solves it in the last block;
+// k_aa_update applies the extrapolation, re-imposes Dirichlet values and evaluates the stop rule.
+// ------------------------------------------------------------------------------------------------
+constexpr int kTri = kMaxWindow * (kMaxWindow + 1) / 2;
+constexpr int kAaVals = kTri + kMaxWindow + 2;
+
+__device__ __forceinline__ int tri_idx(int i, int j) { return j * (j + 1) / 2 + i; }  // i <= j
+
+__global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __restrict__ x,
+                                                        const double* __restrict__ xr,
+                                                        const unsigned char* __restrict__ fixed,
+                                                        const double* __restrict__ fval, double* __restrict__ dG,
+                                                        double* __restrict__ dX, double* __restrict__ lg,
+                                                        double* __restrict__ lx, int ld, double* __restrict__ part,
+                                                        Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ double sh[kAaVals * 32];
+    const int W = ctrl->window, count = ctrl->count, head = ctrl->head, mode = ctrl->mode;
+    const int m = W > 0 ? count : 0;
+    double acc[kAaVals];
+#pragma unroll
+    for (int i = 0; i < kAaVals; ++i) acc[i] = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n3; r += gridDim.x * blockDim.x) {
+        const double xp = x[r];
+        double xv = xr[r];
+        if (fixed[r]) xv = mode == 0 ? fval[r] : 0.0;
+        const double g = xv - xp;
+        if (W > 0) {
+            if (count >= 1) {
+                const int s = (head + count - 1) % W;
+                dG[(size_t)s * ld + r] = g - lg[r];
+                dX[(size_t)s * ld + r] = xp - lx[r];
+            }
+            lg[r] = g;
+            lx[r] = xp;
+            double dg[kMaxWindow];
+#pragma unroll
+            for (int j = 0; j < kMaxWindow; ++j) dg[j] = j < m ? dG[(size_t)((head + j) % W) * ld + r] : 0.0;
+#pragma unroll
+            for (int j = 0; j < kMaxWindow; ++j) {
+#pragma unroll
+                for (int i = 0; i <= j; ++i) acc[tri_idx(i, j)] += dg[i] * dg[j];
+                acc[kTri + j] += dg[j] * g;
+            }
+        }
+        acc[kAaVals - 2] += g * g;
+        acc[kAaVals - 1] += xv * xv;
+    }
+    block_sum<kAaVals>(acc, sh);
+    if (threadIdx.x == 0)
+        for (int i = 0; i < kAaVals; ++i) part[blockIdx.x * kAaVals + i] = acc[i];
+    if (!arrive_last(&ctrl->arrive[0])) return;
+    if (threadIdx.x != 0) return;
+    double tot[kAaVals];
+    for (int i = 0; i < kAaVals; ++i) tot[i] = 0.0;
+    for (int b = 0; b < gridDim.x; ++b)
+        for (int i = 0; i < kAaVals; ++i) tot[i] += __ldcg(part + b * kAaVals + i);
+    ctrl->arrive[0] = 0;
+    ctrl->err = sqrt(tot[kAaVals - 2]);
+    ctrl->xn = sqrt(tot[kAaVals - 1]);
+    ctrl->m = m;
+    ctrl->accept = 0;
+    ctrl->restart = 0;
+    if (mode == 1 && (!(ctrl->xn == ctrl->xn) || ctrl->xn > 1e300 ||
+                      (ctrl->clip > 0 && ctrl->xn > ctrl->clip))) {
+        ctrl->status |= (ctrl->xn == ctrl->xn && ctrl->xn <= 1e300) ? (int)kStatusDiverged
+                                                                    : (int)(kStatusDiverged | kStatusNonFinite);
+        return;
+    }
+    if (m < 1) return;
+    // Gram system (dG^T dG + reg I) gamma = dG^T g, reg = max(1e-6 |dG|_F^2 / m, 1e-12); Cholesky solve.
+    double A[kMaxWindow * kMaxWindow], b[kMaxWindow];
+    double fro = 0;
+    for (int j = 0; j < m; ++j) fro += tot[tri_idx(j, j)];
+    const double reg = fmax(1e-6 * fro / m, 1e-12);
+    for (int i = 0; i < m; ++i) {
+        for (int j = 0; j < m; ++j) A[i * m + j] = tot[i <= j ? tri_idx(i, j) : tri_idx(j, i)];
+        A[i * m + i] += reg;
+        b[i] = tot[kTri + i];
+    }
+    for (int j = 0; j < m; ++j) {
+        double d = A[j * m + j];
+        for (int k = 0; k < j; ++k) d -= A[j * m + k] * A[j * m + k];
+        d = sqrt(fmax(d, 1e-300));
+        A[j * m + j] = d;
+        for (int i = j + 1; i < m; ++i) {
+            double s = A[i * m + j];
+            for (int k = 0; k < j; ++k) s -= A[i * m + k] * A[j * m + k];
+            A[i * m + j] = s / d;
+        }
+    }
+    for (int i = 0; i < m; ++i) {
+        double s = b[i];
+        for (int k = 0; k < i; ++k) s -= A[i * m + k] * b[k];
+        b[i] = s / A[i * m + i];
+    }
+    for (int i = m - 1; i >= 0; --i) {
+        double s = b[i];
+        for (int k = i + 1; k < m; ++k) s -= A[k * m + i] * b[k];
+        b[i] = s / A[i * m + i];
+    }
+    double gn = 0;
+    for (int i = 0; i < m; ++i) gn += b[i] * b[i];
+    gn = sqrt(gn);
+    if (!(gn < 10.0)) {
+        ctrl->restart = 1;
+    } else {
+        ctrl->accept = 1;
+        for (int i = 0; i < m; ++i) ctrl->gamma[i] = b[i];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_aa_update(int n3, double* __restrict__ x, const double* __restrict__ xr,
+                                                        const unsigned char* __restrict__ fixed,
+                                                        const double* __restrict__ fval,
+                                                        const double* __restrict__ dG, const double* __restrict__ dX,
+                                                        int ld, double* __restrict__ part,
+                                                        const double* __restrict__ gate_part, int gate_blocks,
+                                                        Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ double sh[3 * 32];
+    const int W = ctrl->window, head = ctrl->head, mode = ctrl->mode;
+    const int accept = ctrl->accept, m = ctrl->m;
+    double gam[kMaxWindow];
+#pragma unroll
+    for (int j = 0; j < kMaxWindow; ++j) gam[j] = (accept && j < m) ? ctrl->gamma[j] : 0.0;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n3; r += gridDim.x * blockDim.x) {
+        const double xp = x[r];
+        double xv = xr[r];
+        const bool fx = fixed[r] != 0;
+        if (fx) xv = mode == 0 ? fval[r] : 0.0;
+        double xn = xv;
+        if (accept) {
+            xn = xv;  // = xp + g
+#pragma unroll
+            for (int j = 0; j < kMaxWindow; ++j)
+                if (j < m) {
+                    const size_t s = (size_t)((head + j) % W) * ld + r;
+                    xn -= (dX[s] + dG[s]) * gam[j];
+                }
+            if (fx) xn = mode == 0 ? fval[r] : 0.0;
+        }
+        x[r] = xn;
+        acc[0] += (xn - xp) * (xn - xp);
+        acc[1] += xp * xp;
+        acc[2] += xn * xn;
+    }
+    block_sum<3>(acc, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 3] = acc[0];
+        part[blockIdx.x * 3 + 1] = acc[1];
+        part[blockIdx.x * 3 + 2] = acc[2];
+    }
+    if (!arrive_last(&ctrl->arrive[1])) return;
+    if (threadIdx.x != 0) return;
+    double t0 = 0, t1 = 0, t2 = 0;
+    for (int b = 0; b < gridDim.x; ++b) {
+        t0 += __ldcg(part + b * 3);
+        t1 += __ldcg(part + b * 3 + 1);
+        t2 += __ldcg(part + b * 3 + 2);
+    }
+    ctrl->arrive[1] = 0;
+    const double dq = sqrt(t0), rn = sqrt(t1), xnorm = sqrt(t2);
+    bool conv = false;
+    const int it = ctrl->iter;
+    if (mode == 0) {
+        double p0 = 0, p1 = 0;
+        for (int b = 0; b < gate_blocks; ++b) {
+            p0 += __ldcg(gate_part + b * 2);
+            p1 += __ldcg(gate_part + b * 2 + 1);
+        }
+        const double pdc = sqrt(p0), pdr = sqrt(p1);
+        ctrl->dq = dq; ctrl->rn = rn; ctrl->pdc = pdc; ctrl->pdr = pdr;
+        conv = it > 0 && dq <= ctrl->rel_tol * rn + ctrl->abs_tol && pdc <= ctrl->rel_tol * pdr + ctrl->abs_tol;
+        if (!(dq == dq) || !(pdc == pdc)) ctrl->status |= kStatusNonFinite;
+    } else {
+        ctrl->dq = dq; ctrl->rn = xnorm;
+        conv = it > 0 && ctrl->err < ctrl->rel_tol * xnorm + ctrl->abs_tol;
+        if (!(xnorm == xnorm)) ctrl->status |= kStatusNonFinite | kStatusDiverged;
+        else if (ctrl->clip > 0 && xnorm > ctrl->clip) ctrl->status |= kStatusDiverged;
+    }
+    if (W > 0) {
+        if (ctrl->restart) {
+            ctrl->count = 0;
+            ctrl->head = 0;
+        } else {
+            int c = ctrl->count + 1;
+            if (c > W) {
+                c = W;
+                ctrl->head = (ctrl->head + 1) % W;
+            }
+            ctrl->count = c;
+        }
+    }
+    ctrl->iter = it + 1;
+    if (conv) ctrl->converged = 1;
+    if (conv || ctrl->iter >= ctrl->max_iter || (ctrl->status & (kStatusNonFinite | kStatusDiverged))) ctrl->done = 1;
+}
+
+__global__ void k_qtilde(int n3, const double* q, const double* v, const double* f, double h, double h2m,
+                         const double* gf, double* qt) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n3) return;
+    qt[r] = q[r] + h * v[r] + h2m * f[r] + h2m * gf[r % 3];
+}
+
+__global__ void k_velocity(int n3, const double* qn, const double* q, double inv_h, double* vn) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n3) return;
+    vn[r] = (qn[r] - q[r]) * inv_h;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Adjoint kernels
+// ------------------------------------------------------------------------------------------------
+// Cyclic Jacobi eigen-decomposition of a symmetric 9x9 matrix (row-major), eigenvectors in Q (columns).
+__device__ void jacobi_eig9(double* A, double* Q) {
+    for (int i = 0; i < 81; ++i) Q[i] = (i % 10 == 0) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 30; ++sweep) {
+        double off = 0, diag = 0;
+        for (int i = 0; i < 9; ++i)
+            for (int j = 0; j < 9; ++j) (i == j ? diag : off) += A[i * 9 + j] * A[i * 9 + j];
+        if (off <= 1e-30 * diag) break;
+        for (int p = 0; p < 8; ++p)
+            for (int q = p + 1; q < 9; ++q) {
+                const double apq = A[p * 9 + q];
+                if (fabs(apq) < 1e-300) continue;
+                const double tau = (A[q * 9 + q] - A[p * 9 + p]) / (2 * apq);
+                const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+                const double c = 1 / sqrt(1 + t * t), s = t * c;
+                for (int k = 0; k < 9; ++k) {  // columns p,q
+                    const double akp = A[k * 9 + p], akq = A[k * 9 + q];
+                    A[k * 9 + p] = c * akp - s * akq;
+                    A[k * 9 + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 9; ++k) {  // rows p,q
+                    const double apk = A[p * 9 + k], aqk = A[q * 9 + k];
+                    A[p * 9 + k] = c * apk - s * aqk;
+                    A[q * 9 + k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 9; ++k) {
+                    const double qkp = Q[k * 9 + p], qkq = Q[k * 9 + q];
+                    Q[k * 9 + p] = c * qkp - s * qkq;
+                    Q[k * 9 + q] = s * qkp + c * qkq;
+                }
+            }
+    }
+}
+
+template <int K, int S>
+__global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict__ E, const double* __restrict__ q,
+                                                   const double* __restrict__ grad, double vol_over_s, EnergyPack ep,
+                                                   int mean_w, int filter, double* __restrict__ J, Ctrl* ctrl) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = t / S, smp = t % S;
+    if (e >= m) return;
+    const double* g = (S == 8) ? grad + smp * 24 : grad + (size_t)e * 12;
+    double F[9], U[9], V[9], sig[3];
+    def_grad<K>(E, e, q, g, F);
+    svd3<double>(F, U, sig, V);
+    double* Jt = J + (size_t)t * 81;
+    double wsum = 0;
+    for (int col = 0; col < 9; ++col) {
+        double dF[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) dF[i] = (i == col) ? 1.0 : 0.0;
+        double out[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) out[i] = 0.0;
+        for (int k = 0; k < ep.count; ++k) {
+            const ElemEnergyDev& en = ep.en[k];
+            if (en.mask && !en.mask[e]) continue;
+            const double w = (mean_w ? en.w_mean : ld_weight<double>(en, e)) * vol_over_s;
+            if (col == 0) wsum += w;
+            double d[9];
+            project_diff<double>(en.type, en.mu, en.la, en.w_mean, U, sig, V, dF, d);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) out[i] += w * d[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Jt[col * 9 + i] = out[i];  // column col (column-major 9x9)
+    }
+    if (filter == 0) return;
+    // State-adaptive filter of the local Hessian H = wsum I - J (the PD energy's per-sample Hessian):
+    // kept as is when symmetric diagonally dominant with a non-negative diagonal (hence PSD); otherwise
+    // eigen-decomposed and its eigenvalues clamped at 0 (filter 1) or replaced by |lambda| (filter 2),
+    // following ProjectedNewtonMatrix (cpp/core/src/fem/deformable_newton_forward.cpp:394-434).
+    double H[81];
+    for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) H[i * 9 + j] = (i == j ? wsum : 0.0) - 0.5 * (Jt[j * 9 + i] + Jt[i * 9 + j]);
+    bool dd = true;
+    for (int i = 0; i < 9 && dd; ++i) {
+        double off = 0;
+        for (int j = 0; j < 9; ++j)
+            if (j != i) off += fabs(H[i * 9 + j]);
+        dd = H[i * 9 + i] >= off;
+    }
+    if (dd) return;
+    double Q[81];
+    jacobi_eig9(H, Q);
+    double lam[9];
+    for (int i = 0; i < 9; ++i) {
+        const double l = H[i * 9 + i];
+        lam[i] = filter == 1 ? fmax(l, 0.0) : fabs(l);
+    }
+    for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) {
+            double h = 0;
+            for (int k = 0; k < 9; ++k) h += Q[i * 9 + k] * lam[k] * Q[j * 9 + k];
+            Jt[j * 9 + i] = (i == j ? wsum : 0.0) - h;
+        }
+    atomicAdd(&ctrl->arrive[3], 1u);  // number of filtered samples (diagnostic)
+}
+
+template <int K, int S>
+__global__ void __launch_bounds__(kThreads) k_kpd_elem(int m, const int* __restrict__ E, const double* __restrict__ u,
+                                                       const double* __restrict__ grad, const double* __restrict__ J,
+                                                       double* __restrict__ out, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = t / S, smp = t % S;
+    const bool valid = e < m;
+    double acc[K][3];
+#pragma unroll
+    for (int a = 0; a < K; ++a) acc[a][0] = acc[a][1] = acc[a][2] = 0.0;
+    if (valid) {
+        const double* g = (S == 8) ? grad + smp * 24 : grad + (size_t)e * 12;
+        double dF[9];
+        def_grad<K>(E, e, u, g, dF);
+        const double* Jt = J + (size_t)t * 81;
+        double P[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) P[i] = 0.0;
+#pragma unroll
+        for (int col = 0; col < 9; ++col) {
+            const double f = dF[col];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) P[i] += __ldg(Jt + col * 9 + i) * f;
+        }
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            const double g0 = __ldg(g + a * 3), g1 = __ldg(g + a * 3 + 1), g2 = __ldg(g + a * 3 + 2);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) acc[a][i] = P[i] * g0 + P[i + 3] * g1 + P[i + 6] * g2;
+        }
+    }
+    if (S == 8) {
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+            for (int a = 0; a < K; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) acc[a][i] += __shfl_xor_sync(0xffffffffu, acc[a][i], o);
+        if (valid) {
+#pragma unroll
+            for (int a = 0; a < K; ++a)
+                if (a == smp) {
+                    double* o = out + ((size_t)e * K + a) * 3;
+                    o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
+                }
+        }
+    } else if (valid) {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            double* o = out + ((size_t)e * K + a) * 3;
+            o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_gather_bwd(int n, const int* __restrict__ node_ptr,
+                                                         const int* __restrict__ node_inc,
+                                                         const double* __restrict__ eo, const double* __restrict__ gbar,
+                                                         const unsigned char* __restrict__ fixed,
+                                                         const int* __restrict__ iperm, double* __restrict__ v,
+                                                         int npad, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double p0 = 0, p1 = 0, p2 = 0;
+        for (int idx = node_ptr[i]; idx < node_ptr[i + 1]; ++idx) {
+            const double* c = eo + (size_t)node_inc[idx] * 3;
+            p0 += c[0]; p1 += c[1]; p2 += c[2];
+        }
+        const int j = iperm[i];
+        const bool fx = fixed[i] != 0;
+        v[j] = fx ? 0.0 : gbar[3 * i] + p0;
+        v[npad + j] = fx ? 0.0 : gbar[3 * i + 1] + p1;
+        v[2 * (size_t)npad + j] = fx ? 0.0 : gbar[3 * i + 2] + p2;
+    }
+}
+
+// d(prox)/d(mu_bar), d(prox)/d(la_bar) of the Neo-Hookean proximal map with k = 2 mu_bar.
+__device__ void nh_param_diff(double mu, double la, const double* U, const double* sig, const double* V, double* dPm,
+                              double* dPl) {
+    const double k = 2 * mu;
+    double ss[3];
+    nh_prox<double>(mu, la, k, sig, ss);
+    double H[9];
+    nh_hessian<double>(mu, la, k, ss, H);
+    H[0] += 1e-9; H[4] += 1e-9; H[8] += 1e-9;
+    const double L = log(fmax(ss[0] * ss[1] * ss[2], 1e-12));
+    double gm[3], gl[3], H2[9];
+    for (int i = 0; i < 3; ++i) {
+        gm[i] = -(ss[i] - 1 / ss[i] + 2 * (ss[i] - sig[i]));
+        gl[i] = -(L / ss[i]);
+    }
+    for (int i = 0; i < 9; ++i) H2[i] = H[i];
+    small_solve<double, 3>(H, gm);
+    small_solve<double, 3>(H2, gl);
+    for (int i = 0; i < 3; ++i)
+        if (ss[i] <= 1e-4) { gm[i] = 0; gl[i] = 0; }
+    usvt(U, gm, V, dPm);
+    usvt(U, gl, V, dPl);
+}
+
+template <int K, int S>
+__global__ void __launch_bounds__(128) k_param_grad(int m, const int* __restrict__ E, const double* __restrict__ q,
+                                                    const double* __restrict__ mu, const double* __restrict__ grad,
+                                                    double vol_over_s, EnergyPack ep, double* __restrict__ gw,
+                                                    double* __restrict__ gmat, double* __restrict__ gnh) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = t / S, smp = t % S;
+    const bool valid = e < m;
+    double r[kMaxEnergies][4];
+#pragma unroll
+    for (int k = 0; k < kMaxEnergies; ++k) r[k][0] = r[k][1] = r[k][2] = r[k][3] = 0.0;
+    if (valid) {
+        const double* g = (S == 8) ? grad + smp * 24 : grad + (size_t)e * 12;
+        double F[9], U[9], V[9], sig[3];
+        def_grad<K>(E, e, q, g, F);
+        svd3<double>(F, U, sig, V);
+        // G(i,j) = sum_a mu_a[i] grad_a[j]: then mu_e^T A_s^T M = <G, M>
+        double G[9];
+        def_grad<K>(E, e, mu, g, G);
+        for (int k = 0; k < ep.count && k < kMaxEnergies; ++k) {
+            const ElemEnergyDev& en = ep.en[k];
+            if (en.mask && !en.mask[e]) continue;
+            double Bp[9];
+            project<double>(en.type, en.mu, en.la, en.w_mean, U, sig, V, Bp);
+            double dot = 0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) dot += G[i] * (F[i] - Bp[i]);
+            r[k][0] = -vol_over_s * dot;
+            if (en.type == 2) {
+                // reference dl_dmat_w term: NH first Piola stress over the mean stiffness
+                const double Jd = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) +
+                                  F[6] * (F[1] * F[5] - F[4] * F[2]);
+                const double lj = log(fmax(Jd, 1e-12));
+                double FiT[9];  // F^-T = cofactor(F) / det
+                FiT[0] = (F[4] * F[8] - F[5] * F[7]) / Jd;
+                FiT[1] = (F[5] * F[6] - F[3] * F[8]) / Jd;
+                FiT[2] = (F[3] * F[7] - F[4] * F[6]) / Jd;
+                FiT[3] = (F[2] * F[7] - F[1] * F[8]) / Jd;
+                FiT[4] = (F[0] * F[8] - F[2] * F[6]) / Jd;
+                FiT[5] = (F[1] * F[6] - F[0] * F[7]) / Jd;
+                FiT[6] = (F[1] * F[5] - F[2] * F[4]) / Jd;
+                FiT[7] = (F[2] * F[3] - F[0] * F[5]) / Jd;
+                FiT[8] = (F[0] * F[4] - F[1] * F[3]) / Jd;
+                double dp = 0;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) dp += G[i] * (en.mu * (F[i] - FiT[i]) + en.la * lj * FiT[i]) / en.w_mean;
+                r[k][1] = -vol_over_s * dp;
+                double dPm[9], dPl[9];
+                nh_param_diff(en.mu, en.la, U, sig, V, dPm, dPl);
+                const double w = ld_weight<double>(en, e) * vol_over_s;
+                double a1 = 0, a2 = 0;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) { a1 += G[i] * dPm[i]; a2 += G[i] * dPl[i]; }
+                r[k][2] = w * a1;
+                r[k][3] = w * a2;
+            } else {
+                r[k][1] = r[k][0];
+            }
+        }
+    }
+    if (S == 8) {
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < kMaxEnergies; ++k)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) r[k][i] += __shfl_xor_sync(0xffffffffu, r[k][i], o);
+    }
+    if (valid && smp == 0) {
+        for (int k = 0; k < ep.count && k < kMaxEnergies; ++k) {
+            gw[(size_t)k * m + e] = r[k][0];
+            gmat[(size_t)k * m + e] = r[k][1];
+            gnh[((size_t)k * m + e) * 2] = r[k][2];
+            gnh[((size_t)k * m + e) * 2 + 1] = r[k][3];
+        }
+    }
+}
+
+inline int blocks_for(long long work, int threads) { return (int)((work + threads - 1) / threads); }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// Launchers
+// ------------------------------------------------------------------------------------------------
+template <typename T>
+void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const double* qb, const unsigned char* elem_dir,
+                     const double* grad, int hex, double vol_over_s, const EnergyPack& ep, T* elem_out, Ctrl* ctrl,
+                     cudaStream_t st) {
+    const int grid = blocks_for((long long)m * s, kThreads);
+    if (hex) k_elem_fwd<T, 8, 8><<<grid, kThreads, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
+    else k_elem_fwd<T, 4, 1><<<grid, kThreads, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
+}
+
+template <typename T>
+void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
+                       double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
+                       double* pd, double* prev_pd, double* part, Ctrl* ctrl, cudaStream_t st) {
+    (void)pd;
+    k_gather_fwd<T><<<kRedBlocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
+                                                     v_perm, npad, prev_pd, part, ctrl);
+}
+
+template <typename T>
+void launch_spmv_S(int n, const int64_t* row_off, const int* row_a, const int* row_len, const T* vals, const T* v,
+                   int npad, T* y, const Ctrl* ctrl, cudaStream_t st) {
+    const int grid = blocks_for((long long)n * 32, kThreads);
+    k_spmv_S<T><<<grid, kThreads, 0, st>>>(n, row_off, row_a, row_len, vals, v, npad, y, ctrl);
+}
+
+template <typename T>
+void launch_spmv_ST(int n, int ntiles, const int* tile_ptr, const int* tile_rows, const int64_t* row_off,
+                    const int* row_a, const int* row_len, const T* vals, const T* y, int npad, const int* perm,
+                    double* x_out, const Ctrl* ctrl, cudaStream_t st) {
+    k_spmv_ST<T, 8><<<ntiles, 8 * 32, 0, st>>>(n, tile_ptr, tile_rows, row_off, row_a, row_len, vals, y, npad, perm,
+                                               x_out, ctrl);
+}
+
+void launch_aa_reduce(int n3, const double* x, const double* x_raw, const unsigned char* fixed_dof,
+                      const double* fixed_val, double* dG, double* dX, double* last_g, double* last_x, int ld,
+                      double* part, Ctrl* ctrl, cudaStream_t st) {
+    k_aa_reduce<<<kRedBlocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, last_g, last_x, ld, part,
+                                                ctrl);
+}
+
+void launch_aa_update(int n3, double* x, const double* x_raw, const unsigned char* fixed_dof, const double* fixed_val,
+                      const double* dG, const double* dX, int ld, double* part, const double* gate_part,
+                      int gate_blocks, Ctrl* ctrl, cudaStream_t st) {
+    k_aa_update<<<kRedBlocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, ld, part, gate_part,
+                                                gate_blocks, ctrl);
+}
+
+void launch_qtilde(int n3, const double* q, const double* v, const double* f_ext, double h, double h2m,
+                   const double* grav_force, double* qt, cudaStream_t st) {
+    k_qtilde<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, q, v, f_ext, h, h2m, grav_force, qt);
+}
+
+void launch_velocity(int n3, const double* q_next, const double* q, double inv_h, double* v_next, cudaStream_t st) {
+    k_velocity<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, q_next, q, inv_h, v_next);
+}
+
+void launch_jac_build(int m, int k, int s, const int* E, const double* q, const double* grad, int hex,
+                      double vol_over_s, const EnergyPack& ep, int mean_w, int filter, double* J, Ctrl* ctrl,
+                      cudaStream_t st) {
+    (void)k;
+    const int grid = blocks_for((long long)m * s, 128);
+    if (hex) k_jac_build<8, 8><<<grid, 128, 0, st>>>(m, E, q, grad, vol_over_s, ep, mean_w, filter, J, ctrl);
+    else k_jac_build<4, 1><<<grid, 128, 0, st>>>(m, E, q, grad, vol_over_s, ep, mean_w, filter, J, ctrl);
+}
+
+void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const double* grad, int hex, const double* J,
+                     double* elem_out, const Ctrl* ctrl, cudaStream_t st) {
+    (void)k;
+    const int grid = blocks_for((long long)m * s, kThreads);
+    if (hex) k_kpd_elem<8, 8><<<grid, kThreads, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
+    else k_kpd_elem<4, 1><<<grid, kThreads, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
+}
+
+void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* gbar,
+                       const unsigned char* fixed_node, const int* iperm, double* v_perm, int npad, const Ctrl* ctrl,
+                       cudaStream_t st) {
+    k_gather_bwd<<<kRedBlocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm,
+                                                 npad, ctrl);
+}
+
+void launch_param_grad(int m, int k, int s, const int* E, const double* q, const double* mu, const double* grad,
+                       int hex, double vol_over_s, const EnergyPack& ep, double* gw, double* gmat, double* gnh,
+                       cudaStream_t st) {
+    (void)k;
+    const int grid = blocks_for((long long)m * s, 128);
+    if (hex) k_param_grad<8, 8><<<grid, 128, 0, st>>>(m, E, q, mu, grad, vol_over_s, ep, gw, gmat, gnh);
+    else k_param_grad<4, 1><<<grid, 128, 0, st>>>(m, E, q, mu, grad, vol_over_s, ep, gw, gmat, gnh);
+}
+
+template void launch_elem_fwd<double>(int, int, int, const int*, const double*, const double*, const unsigned char*,
+                                      const double*, int, double, const EnergyPack&, double*, Ctrl*, cudaStream_t);
+template void launch_elem_fwd<float>(int, int, int, const int*, const double*, const double*, const unsigned char*,
+                                     const double*, int, double, const EnergyPack&, float*, Ctrl*, cudaStream_t);
+template void launch_gather_fwd<double>(int, const int*, const int*, const double*, const double*, double,
+                                        const unsigned char*, const int*, double*, int, double*, double*, double*,
+                                        Ctrl*, cudaStream_t);
+template void launch_gather_fwd<float>(int, const int*, const int*, const float*, const double*, double,
+                                       const unsigned char*, const int*, float*, int, double*, double*, double*, Ctrl*,
+                                       cudaStream_t);
+template void launch_spmv_S<double>(int, const int64_t*, const int*, const int*, const double*, const double*, int,
+                                    double*, const Ctrl*, cudaStream_t);
+template void launch_spmv_S<float>(int, const int64_t*, const int*, const int*, const float*, const float*, int,
+                                   float*, const Ctrl*, cudaStream_t);
+template void launch_spmv_ST<double>(int, int, const int*, const int*, const int64_t*, const int*, const int*,
+                                     const double*, const double*, int, const int*, double*, const Ctrl*,
+                                     cudaStream_t);
+template void launch_spmv_ST<float>(int, int, const int*, const int*, const int64_t*, const int*, const int*,
+                                    const float*, const float*, int, const int*, double*, const Ctrl*, cudaStream_t);
+
+}  // namespace dphd

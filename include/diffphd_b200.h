@@ -1,0 +1,111 @@
+/*
+ * diffphd_b200 — C ABI of the B200 (sm_100a) projective-dynamics time step and its adjoint.
+ *
+ * Drop-in boundary for DiffPhD's `Deformable<3,8>` / `Deformable<3,4>` on the "pd_eigen_alg_phd" path.
+ * Every entry point returns 0 on success and a non-zero status otherwise; the message of the last error
+ * on the calling thread is returned by dphd_last_error().  No C++ exception crosses this boundary.
+ * Vectors are node-major interleaved xyz, FP64 (the layout of the reference's q, v, f_ext).
+ * Option dictionaries are passed as parallel arrays of keys and values (the reference's
+ * std::map<std::string, real>, converted from a Python dict by common.py:195-200 `to_std_map`).
+ */
+#ifndef DIFFPHD_B200_H
+#define DIFFPHD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dphd_deformable dphd_deformable;
+
+/* Message of the last failed call on this thread (empty string when none). */
+const char* dphd_last_error(void);
+
+/* Replaces the HexDeformable()/TetDeformable() constructors (cpp/core/src/py_diff_pd_core.i:60-68;
+ * Deformable<vertex_dim, element_dim>, cpp/core/include/fem/deformable.h:17-21).
+ * vertex_dim must be 3; element_dim 8 (hex) or 4 (tet). */
+int dphd_create(int vertex_dim, int element_dim, dphd_deformable** out);
+int dphd_destroy(dphd_deformable* h);
+
+/* Deformable::Initialize(bin_file, density, material_type, E, nu) (deformable.h:24-28).
+ * Only material_type "none" is accepted on this path (elasticity comes from AddPdEnergy). */
+int dphd_init_from_bin(dphd_deformable* h, const char* bin_file, double density, const char* material_type,
+                       double youngs_modulus, double poissons_ratio);
+/* Deformable::Initialize(vertices, elements, ...) (deformable.h:26-28); verts: n*3 FP64 node-major,
+ * elems: m*element_dim int32. */
+int dphd_init_from_arrays(dphd_deformable* h, const double* verts, int n, const int* elems, int m, double density,
+                          const char* material_type, double youngs_modulus, double poissons_ratio);
+
+/* Deformable::SetDirichletBoundaryCondition(dof, val) (deformable.h:70-73). */
+int dphd_set_dirichlet(dphd_deformable* h, int dof, double val);
+/* Deformable::AddPdEnergy(type, params, indices) (cpp/core/src/fem/deformable_pd_energy.cpp:43-153);
+ * type "corotated" | "volume" (params: 1 or element_num values) | "pd_neohookean" (params: [mu, la] or
+ * 2*element_num interleaved); nidx == 0 means every element. */
+int dphd_add_pd_energy(dphd_deformable* h, const char* type, const double* params, int nparams, const int* indices,
+                       int nidx);
+/* Deformable::AddStateForce("gravity", [gx, gy, gz]) (cpp/core/src/fem/deformable_state_force.cpp:10-20). */
+int dphd_add_state_force(dphd_deformable* h, const char* type, const double* params, int nparams);
+/* Deformable::SetFrictionalBoundary("planar", [nx, ny, nz, offset], node_indices)
+ * (cpp/core/src/fem/deformable_friction.cpp:7-31). */
+int dphd_set_frictional_boundary(dphd_deformable* h, const char* type, const double* params, int nparams,
+                                 const int* indices, int nidx);
+
+/* Accessors (deformable.h:45-64): dofs(), act_dofs(), NumOfPdElementEnergies(), NumOfStateForceParameters();
+ * dphd_num_pd_params is the total length of all AddPdEnergy parameter arrays (size of dl_dparams). */
+int dphd_dofs(const dphd_deformable* h);
+int dphd_act_dofs(const dphd_deformable* h);
+int dphd_num_pd_element_energies(const dphd_deformable* h);
+int dphd_num_state_force_parameters(const dphd_deformable* h);
+int dphd_num_pd_params(const dphd_deformable* h);
+
+/* Deformable::PyForward(method, q, v, a, f_ext, dt, options, q_next&, v_next&, active_contact_idx&)
+ * (deformable.h:132-134; AlgPhd implementation forward_gpu.cpp:387-1594).  method: "pd_eigen_alg_phd" or
+ * its alias "pd_eigen_pcg_proj_gpu".  active_idx: capacity *n_active on input, count on output. */
+int dphd_forward(dphd_deformable* h, const char* method, const double* q, const double* v, const double* a,
+                 const double* f_ext, double dt, const char** opt_keys, const double* opt_vals, int nopts,
+                 double* q_next, double* v_next, int* active_idx, int* n_active);
+
+/* Deformable::PyBackward(method, q, v, a, f_ext, dt, q_next, v_next, active_contact_idx, dl_dq_next,
+ * dl_dv_next, options, dl_dq&, dl_dv&, dl_da&, dl_df_ext&, dl_dmat_w&, dl_dact_w&, dl_dstate_p&)
+ * (deformable.h:135-141; AlgPhd implementation backward_gpu.cpp:648-1250). */
+int dphd_backward(dphd_deformable* h, const char* method, const double* q, const double* v, const double* a,
+                  const double* f_ext, double dt, const double* q_next, const double* v_next, const int* active_idx,
+                  int n_active, const double* dl_dq_next, const double* dl_dv_next, const char** opt_keys,
+                  const double* opt_vals, int nopts, double* dl_dq, double* dl_dv, double* dl_da, double* dl_df_ext,
+                  double* dl_dmat_w, double* dl_dact_w, double* dl_dstate_p);
+/* Extension of dphd_backward: also returns dl_dparams, the gradient w.r.t. every AddPdEnergy parameter
+ * array concatenated in call order (per-element stiffnesses, or interleaved [mu_e, la_e]); the reference
+ * only returns one scalar per energy (dl_dmat_w). */
+int dphd_backward_ex(dphd_deformable* h, const char* method, const double* q, const double* v, const double* a,
+                     const double* f_ext, double dt, const double* q_next, const double* v_next,
+                     const int* active_idx, int n_active, const double* dl_dq_next, const double* dl_dv_next,
+                     const char** opt_keys, const double* opt_vals, int nopts, double* dl_dq, double* dl_dv,
+                     double* dl_da, double* dl_df_ext, double* dl_dmat_w, double* dl_dact_w, double* dl_dstate_p,
+                     double* dl_dparams);
+
+/* Device-pointer forward step: q, v, f_ext, q_next, v_next are device pointers (3n FP64) and the step is
+ * enqueued on `stream` (a cudaStream_t, NULL = legacy default).  Same semantics as dphd_forward. */
+int dphd_forward_device(dphd_deformable* h, const char* method, const double* d_q, const double* d_v,
+                        const double* d_f_ext, double dt, const char** opt_keys, const double* opt_vals, int nopts,
+                        double* d_q_next, double* d_v_next, void* stream);
+
+/* Per-frame statistics (AlgPhdFrameIters / AlgPhdFrameConverged / AlgPhdResetFrameStats,
+ * cpp/core/include/fem/alg_phd_gpu_memory.h:25-27; forward_gpu.cpp:324-332). */
+int dphd_num_frames(const dphd_deformable* h);
+int dphd_frame_stats(const dphd_deformable* h, int* frame_iters, int* frame_converged);
+int dphd_reset_frame_stats(dphd_deformable* h);
+int dphd_last_backward_iters(const dphd_deformable* h);
+/* AlgPhdSMemoryBytes / AlgPhdSNnz (forward_gpu.cpp:302-315): bytes of the S factor in HBM and its nnz. */
+long long dphd_s_memory_bytes(const dphd_deformable* h);
+long long dphd_s_nnz(const dphd_deformable* h);
+
+/* Diagnostics used by the tests: x = A^-1 b through the GPU S^T S pair (fp32 = 0 or 1), the same product
+ * with the host copy of S (the set-up self-check of forward_gpu.cpp:653-670), and the GPU local step
+ * (ProjectiveDynamicsLocalStep, deformable_projective_dynamics_forward.cpp:186-292). */
+int dphd_debug_ainv(dphd_deformable* h, double dt, const double* b, double* x, int fp32);
+int dphd_debug_host_sts(dphd_deformable* h, double dt, const double* b, double* x);
+int dphd_debug_local_step(dphd_deformable* h, double dt, const double* q, double* rhs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DIFFPHD_B200_H */

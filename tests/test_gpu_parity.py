@@ -1,0 +1,175 @@
+"""GPU parity of the CUDA path against the CPU oracle, through the C ABI (run with -m gpu on a B200).
+
+Tolerances: FP64 device path — A^-1 and local step 1e-12 relative, rollouts 1e-9 (plain PD, tight gate)
+and 1e-6 (Anderson-accelerated, 1e-6 dual gate); adjoint 1e-8 relative to the oracle's adjoint; FP32 bulk
+A^-1 5e-6 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from diffphd_b200 import core, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+SMALL = [
+    lambda: scenes.cantilever(cells=(6, 2, 3), steps=1),
+    lambda: scenes.cantilever(steps=1),
+    lambda: scenes.nh_tet_block(cells=(8, 4, 4), dx=0.01, steps=1),
+    lambda: scenes.nh_tet_block(steps=1),
+]
+
+
+@pytest.mark.parametrize("builder", SMALL)
+def test_ainv_fp64_matches_oracle(builder):
+    sc = builder()
+    d = core.from_scene(sc)
+    o = oracle.OracleDeformable.from_scene(sc)
+    b = np.random.default_rng(1).standard_normal(sc.dofs)
+    xr = o.ainv(b, sc.dt)
+    xr[sc.dirichlet_dofs] = 0.0
+    assert _rel(d.debug_ainv(b, sc.dt), xr) < 1e-12
+    x32 = d.debug_ainv(b, sc.dt, fp32=True)
+    assert _rel(x32, xr) < 5e-5
+
+
+@pytest.mark.parametrize("builder", SMALL)
+def test_local_step_matches_oracle(builder):
+    sc = builder()
+    d = core.from_scene(sc)
+    o = oracle.OracleDeformable.from_scene(sc)
+    rng = np.random.default_rng(2)
+    q = sc.q0 + 0.02 * np.abs(sc.verts).max() * rng.standard_normal(sc.dofs) * 0.05
+    q[sc.dirichlet_dofs] = sc.dirichlet_vals
+    r = d.debug_local_step(q, sc.dt)
+    rr = o.local_step(q)
+    assert _rel(r, rr) < 1e-11
+
+
+def _rollout_gpu(d, sc, steps, opts):
+    q, v = sc.q0.copy(), sc.v0.copy()
+    qs, vs = [q], [v]
+    for _ in range(steps):
+        qn, vn = np.zeros(sc.dofs), np.zeros(sc.dofs)
+        d.PyForward("pd_eigen_alg_phd", q, v, [], sc.f_ext, sc.dt, opts, qn, vn, [])
+        q, v = qn, vn
+        qs.append(q)
+        vs.append(v)
+    return qs, vs
+
+
+@pytest.mark.parametrize("aa", [0, 5])
+def test_forward_rollout_cantilever(aa):
+    sc = scenes.cantilever(steps=10)
+    opts = dict(sc.options)
+    if aa == 0:
+        opts.update(aa_window=0, rel_tol=1e-10, abs_tol=1e-12, max_pd_iter=5000)
+        tol = 1e-9
+    else:
+        opts.update(aa_window=5, rel_tol=1e-6, max_pd_iter=1000)
+        tol = 1e-5
+    d = core.from_scene(sc)
+    o = oracle.OracleDeformable.from_scene(sc)
+    qs, _ = _rollout_gpu(d, sc, 10, opts)
+    q_ref, _, it_ref = oracle.rollout(o, sc, steps=10, options=opts)
+    disp = np.abs(q_ref - sc.q0).max()
+    assert np.abs(qs[-1] - q_ref).max() <= tol * max(disp, 1e-12)
+    it_gpu, _ = d.frame_stats()
+    assert len(it_gpu) == 10
+
+
+def test_forward_rollout_nh_tets():
+    sc = scenes.nh_tet_block(cells=(8, 4, 4), dx=0.01, steps=5)
+    opts = dict(sc.options)
+    opts.update(aa_window=0, rel_tol=1e-10, abs_tol=1e-12, max_pd_iter=5000)
+    d = core.from_scene(sc)
+    o = oracle.OracleDeformable.from_scene(sc)
+    qs, _ = _rollout_gpu(d, sc, 5, opts)
+    q_ref, _, _ = oracle.rollout(o, sc, steps=5, options=opts)
+    disp = np.abs(q_ref - sc.q0).max()
+    assert np.abs(qs[-1] - q_ref).max() <= 1e-8 * disp
+
+
+@pytest.mark.parametrize("builder", [
+    lambda: scenes.cantilever(cells=(4, 2, 2), dx=0.02, steps=3, heterogeneous=True),
+    lambda: scenes.nh_tet_block(cells=(4, 2, 2), dx=0.01, steps=3),
+])
+def test_backward_matches_oracle(builder):
+    sc = builder()
+    opts = dict(sc.options)
+    opts.update(aa_window=0, rel_tol=1e-12, abs_tol=1e-14, max_pd_iter=5000)
+    o = oracle.OracleDeformable.from_scene(sc)
+    q, v, _, qs, vs = oracle.rollout(o, sc, steps=sc.steps, options=opts, record=True)
+    d = core.from_scene(sc)
+    rng = np.random.default_rng(4)
+    gq, gv = rng.standard_normal(sc.dofs), rng.standard_normal(sc.dofs) * 0.1
+    i = sc.steps - 1
+    ref = o.backward(qs[i], vs[i], sc.f_ext, sc.dt, qs[i + 1], gq, gv, opts)
+    out = d.backward("pd_eigen_alg_phd", qs[i], vs[i], [], sc.f_ext, sc.dt, qs[i + 1], vs[i + 1], [], gq, gv, opts)
+    for key in ("dl_dq", "dl_dv", "dl_df_ext"):
+        assert _rel(out[key], ref[key]) < 1e-8, key
+    assert _rel(out["dl_dstate_p"], ref["dl_dstate_p"]) < 1e-8
+    assert _rel(out["dl_dmat_w"], ref["dl_dmat_w"]) < 1e-8
+    assert _rel(out["dl_dparams"], np.concatenate(ref["dl_dparams"])) < 1e-7
+
+
+def test_adjoint_matches_finite_differences_on_gpu():
+    sc = scenes.cantilever(cells=(4, 2, 2), dx=0.02, steps=3, heterogeneous=True)
+    opts = dict(sc.options)
+    opts.update(aa_window=0, rel_tol=1e-12, abs_tol=1e-14, max_pd_iter=5000)
+    r = np.random.default_rng(3).standard_normal(sc.dofs)
+
+    def run(v0=None, params=None):
+        s2 = sc
+        d = core.HexDeformable()
+        d.Initialize(sc.verts, sc.elems, sc.density, "none", 0, 0)
+        for dof, val in zip(sc.dirichlet_dofs, sc.dirichlet_vals):
+            d.SetDirichletBoundaryCondition(int(dof), float(val))
+        ens = sc.energies if params is None else [(k, p, i) for (k, _, i), p in zip(sc.energies, params)]
+        for k, p, i in ens:
+            d.AddPdEnergy(k, p, i)
+        d.AddStateForce("gravity", sc.gravity)
+        q, v = sc.q0.copy(), (sc.v0 if v0 is None else v0).copy()
+        qs, vs = [q], [v]
+        for _ in range(s2.steps):
+            qn, vn = np.zeros(sc.dofs), np.zeros(sc.dofs)
+            d.PyForward("pd_eigen_alg_phd", q, v, [], sc.f_ext, sc.dt, opts, qn, vn, [])
+            q, v = qn, vn
+            qs.append(q)
+            vs.append(v)
+        return q @ r, d, qs, vs
+
+    L, d, qs, vs = run()
+    gq, gv = r.copy(), np.zeros(sc.dofs)
+    gp = [np.zeros(np.size(p)) for _, p, _ in sc.energies]
+    for i in reversed(range(sc.steps)):
+        out = d.backward("pd_eigen_alg_phd", qs[i], vs[i], [], sc.f_ext, sc.dt, qs[i + 1], vs[i + 1], [], gq, gv,
+                         opts)
+        gq, gv = out["dl_dq"], out["dl_dv"]
+        sizes = np.cumsum([np.size(p) for _, p, _ in sc.energies])[:-1]
+        for a, b in zip(gp, np.split(out["dl_dparams"], sizes)):
+            a += b
+    dirn = np.random.default_rng(5).standard_normal(sc.dofs)
+    dirn[sc.dirichlet_dofs] = 0
+    eps = 1e-5
+    fd = (run(v0=sc.v0 + eps * dirn)[0] - run(v0=sc.v0 - eps * dirn)[0]) / (2 * eps)
+    assert abs(gv @ dirn - fd) <= 1e-4 * abs(fd)
+    p0 = np.asarray(sc.energies[0][1], float)
+    dp = np.random.default_rng(6).standard_normal(p0.size) * p0 * 1e-3
+    ps = lambda s: [p0 + s * dp] + [np.asarray(p, float) for _, p, _ in sc.energies[1:]]
+    fd = (run(params=ps(1))[0] - run(params=ps(-1))[0]) / 2
+    assert abs(gp[0] @ dp - fd) <= 1e-3 * abs(fd)
+
+
+def test_singular_element_reports_error():
+    sc = scenes.cantilever(cells=(2, 1, 1), steps=1)
+    d = core.from_scene(sc)
+    q = sc.q0.copy().reshape(-1, 3)
+    q[:, 0] = 0.0  # flatten the mesh: every F is singular
+    with pytest.raises(RuntimeError, match="Singular F"):
+        d.debug_local_step(q.ravel(), sc.dt)
