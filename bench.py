@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark: simulation steps/s of the projective-dynamics step + its adjoint on B200.
+
+One bench "step" is one forward PD time step (run to the dual gate) plus the adjoint of that step
+(backbone fixed point to the same tolerance, routing and per-element parameter gradients).  The
+workload is the heterogeneous Neo-Hookean tet block (32x16x16 cells split into 5 tets: 40,960 tets,
+9,537 nodes, per-element (mu_e, lambda_e) from a seeded two-phase blob field, nu 0.45, dt 5e-3).
+Inputs are seeded synthetic meshes (no datasets).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision f64|mixed]
+
+value: K steps with inputs resident in HBM (device-pointer C-ABI entry points), CUDA events on the
+library stream, L2 flushed (256 MB write) between steps outside the timed windows.
+e2e: the same K steps through the host-buffer C-ABI calls (PyForward / PyBackward), host<->device copies
+inside the timed region.
+Multi-GPU: independent replicas (the path does not shard; no collective on the data path); value is the
+sum of replica throughputs computed from the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "sim steps/s fwd+adjoint, learned-warmstart FP32 vs plain FP64 GPU @1e-6 res"
+WORKLOAD = "nh_tet_block_32x16x16_5tet_heterogeneous"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def build_scene():
+    from diffphd_b200 import scenes
+    sc = scenes.nh_tet_block()
+    return sc
+
+
+def options(sc, precision):
+    o = dict(sc.options)
+    o["thread_ct"] = os.cpu_count() or 8
+    if precision == "mixed":
+        o["fp32_bulk"] = 1
+    return o
+
+
+def cpu_baseline(sc, opts, steps=1):
+    """Times the oracle (CPU restatement of the reference path, OpenMP on all host cores) on a bounded
+    sample: `steps` forward steps and their adjoints from the scene's rest state."""
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    o = oracle.OracleDeformable.from_scene(sc)
+    copts = dict(opts)
+    copts.pop("fp32_bulk", None)
+    copts["thread_ct"] = cores
+    t_setup = time.perf_counter()
+    o.ainv(np.zeros(sc.dofs), sc.dt)  # factorization, reported separately (not in the sample)
+    t_setup = time.perf_counter() - t_setup
+    q, v = sc.q0.copy(), sc.v0.copy()
+    qs, vs = [q], [v]
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        q, v, _ = o.forward(q, v, sc.f_ext, sc.dt, copts)
+        qs.append(q)
+        vs.append(v)
+    g = sc.extra["loss_r"].copy()
+    gv = np.zeros(sc.dofs)
+    for i in reversed(range(steps)):
+        out = o.backward(qs[i], vs[i], sc.f_ext, sc.dt, qs[i + 1], g, gv, copts)
+        g, gv = out["dl_dq"], out["dl_dv"]
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} forward step(s) + adjoint(s) of {WORKLOAD} from rest, oracle FP64, "
+                      f"factorization {t_setup:.2f}s excluded"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from diffphd_b200 import core
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc = build_scene()
+    opts = options(sc, args.precision)
+    d = core.from_scene(sc)
+    n3 = sc.dofs
+    method = "pd_eigen_alg_phd"
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev).contiguous()
+    f_ext = T(sc.f_ext)
+    g_final = T(sc.extra["loss_r"])
+    zeros = torch.zeros(n3, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+
+    def roll(q0, v0, k):
+        qs, vs = [q0], [v0]
+        for _ in range(k):
+            qn, vn = torch.empty_like(q0), torch.empty_like(q0)
+            d.forward_device(method, qs[-1], vs[-1], f_ext, sc.dt, opts, qn, vn, stream=sh)
+            qs.append(qn)
+            vs.append(vn)
+        return qs, vs
+
+    # warm-up: W steps forward + adjoint (builds S, captures the iteration graphs)
+    with torch.cuda.stream(stream):
+        qs, vs = roll(T(sc.q0), T(sc.v0), args.warmup)
+        gq, gv = g_final.clone(), zeros.clone()
+        for i in reversed(range(args.warmup)):
+            dq, dv, df = torch.empty_like(gq), torch.empty_like(gq), torch.empty_like(gq)
+            d.backward_device(method, qs[i + 1], gq, gv, sc.dt, opts, dq, dv, df, stream=sh)
+            gq, gv = dq, dv
+    stream.synchronize()
+    q_start, v_start = qs[-1], vs[-1]
+    d.reset_frame_stats()
+
+    # timed region 1 (value): device-resident inputs
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = d.kernel_launches()
+    ev = []
+    bwd_iters = []
+    with ClockSampler(local_rank) as clk, torch.cuda.stream(stream):
+        q, v = q_start, v_start
+        qs, vs = [q], [v]
+        for _ in range(args.steps):
+            flush.random_(0, 255)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            qn, vn = torch.empty_like(q), torch.empty_like(q)
+            d.forward_device(method, qs[-1], vs[-1], f_ext, sc.dt, opts, qn, vn, stream=sh)
+            e1.record(stream)
+            ev.append((e0, e1))
+            qs.append(qn)
+            vs.append(vn)
+        gq, gv = g_final.clone(), zeros.clone()
+        dpar = torch.empty(max(1, d.NumOfPdParams()), dtype=torch.float64, device=dev)
+        for i in reversed(range(args.steps)):
+            flush.random_(0, 255)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dq, dv, df = torch.empty_like(gq), torch.empty_like(gq), torch.empty_like(gq)
+            d.backward_device(method, qs[i + 1], gq, gv, sc.dt, opts, dq, dv, df, dl_dparams=dpar, stream=sh)
+            e1.record(stream)
+            ev.append((e0, e1))
+            bwd_iters.append(d._L.dphd_last_backward_iters(d._h))
+            gq, gv = dq, dv
+        stream.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = d.kernel_launches() - launches0
+    t_dev = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    fwd_iters, conv = d.frame_stats()
+
+    # timed region 2 (e2e): host buffers through the C ABI
+    qh, vh = q_start.cpu().numpy(), v_start.cpu().numpy()
+    fh = np.asarray(sc.f_ext)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t_e2e = 0.0
+    qs_h, vs_h = [qh], [vh]
+    for _ in range(args.steps):
+        flush.random_(0, 255)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        qn, vn = np.zeros(n3), np.zeros(n3)
+        d.PyForward(method, qs_h[-1], vs_h[-1], [], fh, sc.dt, opts, qn, vn, [])
+        t_e2e += time.perf_counter() - t0
+        qs_h.append(qn)
+        vs_h.append(vn)
+    gq_h, gv_h = np.asarray(sc.extra["loss_r"]), np.zeros(n3)
+    for i in reversed(range(args.steps)):
+        flush.random_(0, 255)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = d.backward(method, qs_h[i], vs_h[i], [], fh, sc.dt, qs_h[i + 1], vs_h[i + 1], [], gq_h, gv_h, opts)
+        t_e2e += time.perf_counter() - t0
+        gq_h, gv_h = out["dl_dq"], out["dl_dv"]
+    if world > 1:
+        torch.distributed.barrier()
+
+    # max over ranks
+    if world > 1:
+        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_dev, t_e2e = float(t[0]), float(t[1])
+    if rank != 0:
+        return None
+
+    # roofline of the dominant kernel pair (S v, S^T y): algorithmic bytes per A^-1 apply (3 RHS)
+    fp32 = args.precision == "mixed"
+    nnz = d.s_nnz()
+    n = sc.n
+    alg = 2 * nnz * (8 if fp32 else 12) + 4 * 3 * n * (4 if fp32 else 8)
+    raw = 2 * d.s_padded_values() * (4 if fp32 else 8) + 4 * 3 * n * (4 if fp32 else 8)
+    ms = d.time_ainv(sc.dt, reps=30, fp32=fp32, flush_l2=True)
+    peak, peak_kind = _peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "sts_pair_traffic.json"
+    if tp.exists():
+        tj = json.loads(tp.read_text())
+        traffic = tj.get("f32" if fp32 else "f64")
+    steps_total = args.steps * world
+    h2d = 3 * n3 * 8 + 3 * n3 * 8      # forward: q, v, f_ext; adjoint: q_next, dl_dq_next, dl_dv_next
+    d2h = 2 * n3 * 8 + 3 * n3 * 8 + 8 * (d.NumOfPdParams() + d.NumOfPdElementEnergies() + 3)
+    line = {
+        "metric": METRIC,
+        "value": steps_total / t_dev,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_dev / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64" if fp32 else "f64",
+        "data": "synthetic (seeded two-phase blob material field, rest-state start)",
+        "config": {"workload": WORKLOAD, "nodes": n, "elements": sc.m, "dt": sc.dt,
+                   "precision": "fp32 bulk (projection, S/S^T) + fp64 gate/AA" if fp32 else "plain fp64",
+                   "rel_tol": opts["rel_tol"], "abs_tol": opts["abs_tol"], "aa_window": opts["aa_window"],
+                   "max_pd_iter": opts["max_pd_iter"], "step": "forward PD step + adjoint step",
+                   "l2": "flushed (256 MB write) between steps, outside the timed windows",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "S v + S^T y pair (3 RHS)", "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "ms_per_apply": ms, "algorithmic_bytes": alg, "raw_bytes_streamed": raw, "nnz_S": nnz},
+        "e2e": {"value": steps_total / t_e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+        "pd_iters_per_step": float(np.mean(fwd_iters)) if len(fwd_iters) else None,
+        "adjoint_iters_per_step": float(np.mean(bwd_iters)) if bwd_iters else None,
+        "forward_converged_frac": float(np.mean(conv)) if len(conv) else None,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc, opts, steps=1)
+    return line
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    sc = build_scene()
+    opts = options(sc, "f64")
+    vals = []
+    for _ in range(args.warmup):
+        pass  # the CPU port has no warm-up state beyond its factorization (done inside cpu_baseline)
+    for _ in range(max(1, min(args.steps, 2))):
+        vals.append(cpu_baseline(sc, opts, steps=1))
+    v = float(np.mean([x["value"] for x in vals]))
+    cb = dict(vals[0])
+    cb["value"] = v
+    return {"metric": METRIC, "impl": "reference", "value": v, "unit": "steps/s", "n_gpus": world,
+            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nodes": sc.n, "elements": sc.m, "dt": sc.dt,
+                       "note": "reference has no buildable GPU path here; its CPU algorithm is timed via the "
+                               "oracle port (OpenMP, all host cores), bounded sample per step"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 only
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        else:
+            line = run_ours(args, rank, world, local_rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

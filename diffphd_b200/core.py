@@ -70,6 +70,13 @@ def load_library():
     L.dphd_backward_ex.argtypes = bw + [_dp]
     L.dphd_forward_device.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + kv + \
                                      [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.dphd_backward_device.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + \
+        kv + [C.c_void_p] * 7
+    L.dphd_kernel_launches.argtypes = [C.c_void_p]
+    L.dphd_kernel_launches.restype = C.c_longlong
+    L.dphd_s_padded_values.argtypes = [C.c_void_p]
+    L.dphd_s_padded_values.restype = C.c_longlong
+    L.dphd_debug_time_ainv.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, _dp]
     L.dphd_debug_ainv.argtypes = [C.c_void_p, C.c_double, _dp, _dp, C.c_int]
     L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
@@ -255,6 +262,28 @@ class Deformable:
                                                 C.c_void_p(v.data_ptr()), C.c_void_p(f_ext.data_ptr()), float(dt),
                                                 k, _ptr(vals), no, C.c_void_p(q_next.data_ptr()),
                                                 C.c_void_p(v_next.data_ptr()), C.c_void_p(int(stream))))
+
+    def backward_device(self, method, q_next, dl_dq_next, dl_dv_next, dt, options, dl_dq, dl_dv, dl_df_ext,
+                        dl_dmat_w=None, dl_dparams=None, dl_dstate_p=None, stream=0):
+        """Device-pointer adjoint step on torch CUDA tensors (float64, contiguous)."""
+        k, vals, no = _opts(options)
+        ptr = lambda t: C.c_void_p(t.data_ptr() if t is not None else 0)
+        self._check(self._L.dphd_backward_device(self._h, method.encode(), ptr(q_next), ptr(dl_dq_next),
+                                                 ptr(dl_dv_next), float(dt), k, _ptr(vals), no, ptr(dl_dq),
+                                                 ptr(dl_dv), ptr(dl_df_ext), ptr(dl_dmat_w), ptr(dl_dparams),
+                                                 ptr(dl_dstate_p), C.c_void_p(int(stream))))
+
+    def kernel_launches(self):
+        return int(self._L.dphd_kernel_launches(self._h))
+
+    def s_padded_values(self):
+        return int(self._L.dphd_s_padded_values(self._h))
+
+    def time_ainv(self, dt, reps=20, fp32=False, flush_l2=True):
+        ms = C.c_double(0)
+        self._check(self._L.dphd_debug_time_ainv(self._h, float(dt), int(reps), int(bool(fp32)), int(bool(flush_l2)),
+                                                 C.byref(ms)))
+        return ms.value
 
     # ---- statistics ------------------------------------------------------------------------------
     def frame_stats(self):

@@ -250,6 +250,32 @@ int dphd_forward_device(dphd_deformable* h, const char* method, const double* d_
     });
 }
 
+int dphd_backward_device(dphd_deformable* h, const char* method, const double* d_q_next, const double* d_dl_dq_next,
+                         const double* d_dl_dv_next, double dt, const char** keys, const double* vals, int nopts,
+                         double* d_dl_dq, double* d_dl_dv, double* d_dl_df_ext, double* d_dl_dmat_w,
+                         double* d_dl_dparams, double* d_dl_dstate_p, void* stream) {
+    return guard([&] {
+        check_method(method);
+        DPHD_CHECK(d_q_next && d_dl_dq_next && d_dl_dv_next && d_dl_dq && d_dl_dv && d_dl_df_ext,
+                   "null device pointer");
+        DPHD_CHECK(dt > 0, "dt must be positive");
+        const dphd::Options o = dphd::Options::parse(to_map(keys, vals, nopts));
+        E(h).backward_device(d_q_next, d_dl_dq_next, d_dl_dv_next, dt, o, d_dl_dq, d_dl_dv, d_dl_df_ext,
+                             d_dl_dmat_w, d_dl_dparams, d_dl_dstate_p, (cudaStream_t)stream);
+    });
+}
+
+long long dphd_kernel_launches(const dphd_deformable* h) { return h && h->eng ? h->eng->kernel_launches() : -1; }
+
+int dphd_debug_time_ainv(dphd_deformable* h, double dt, int reps, int fp32, int flush_l2, double* ms_per_apply) {
+    return guard([&] {
+        DPHD_CHECK(ms_per_apply && reps > 0, "bad arguments");
+        *ms_per_apply = E(h).time_ainv(dt, reps, fp32 != 0, flush_l2 != 0);
+    });
+}
+
+long long dphd_s_padded_values(const dphd_deformable* h) { return h && h->eng ? h->eng->s_padded_values() : -1; }
+
 int dphd_num_frames(const dphd_deformable* h) {
     return h && h->eng ? (int)h->eng->stats.frame_iters.size() : -1;
 }

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <numeric>
 #include <set>
+#include <type_traits>
 
 #include "engine.h"
 
@@ -77,7 +78,16 @@ Engine::Engine(int vertex_dim, int element_dim) {
     M.s = M.hex ? 8 : 1;
 }
 
+void Engine::drop_graphs() {
+    for (auto& g : graphs_)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
 Engine::~Engine() {
+    drop_graphs();
     if (h_ctrl_) cudaFreeHost(h_ctrl_);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -246,6 +256,51 @@ void Engine::build_device(int threads) {
     std::vector<int> trows(tcnt[ntiles_]), tpos(tcnt.begin(), tcnt.end() - 1);
     for (int i = 0; i < n; ++i)
         for (int t = ra[i] / kTileCols; t <= (ra[i] + rl[i] - 1) / kTileCols; ++t) trows[tpos[t]++] = i;
+    // y = S v schedule: long rows (> kShortRowMax) in groups sharing their first column, short rows by warp
+    std::vector<int> shorts, g_row0, g_g;
+    for (int i = 0; i < n;) {
+        if (rl[i] <= kShortRowMax) {
+            shorts.push_back(i);
+            ++i;
+            continue;
+        }
+        int j = i;
+        while (j < n && rl[j] > kShortRowMax && ra[j] == ra[i] && j - i < 8) ++j;
+        int len = j - i, r = i;
+        for (int g : {8, 4, 2, 1})
+            while (len >= g) {
+                g_row0.push_back(r);
+                g_g.push_back(g);
+                r += g;
+                len -= g;
+            }
+        i = j;
+    }
+    std::stable_sort(shorts.begin(), shorts.end(), [&](int x, int y) { return rl[x] > rl[y]; });
+    // x = S^T y schedule: each tile's row list in chunks of kChunkRows rows
+    std::vector<int> c_tile, c_p0, c_p1, t_cptr(ntiles_ + 1, 0);
+    for (int t = 0; t < ntiles_; ++t) {
+        for (int p0 = tcnt[t]; p0 < tcnt[t + 1]; p0 += kChunkRows) {
+            c_tile.push_back(t);
+            c_p0.push_back(p0);
+            c_p1.push_back(std::min(p0 + kChunkRows, tcnt[t + 1]));
+        }
+        if (tcnt[t] == tcnt[t + 1]) {  // keep every tile covered so stage 2 writes zeros
+            c_tile.push_back(t);
+            c_p0.push_back(tcnt[t]);
+            c_p1.push_back(tcnt[t]);
+        }
+        t_cptr[t + 1] = (int)c_tile.size();
+    }
+    d_short_rows.upload(shorts);
+    d_grp_row0.upload(g_row0);
+    d_grp_g.upload(g_g);
+    d_chunk_tile.upload(c_tile);
+    d_chunk_p0.upload(c_p0);
+    d_chunk_p1.upload(c_p1);
+    d_tile_chunk_ptr.upload(t_cptr);
+    d_xpart64.alloc(c_tile.size() * 3 * kTileCols * sizeof(double));
+    d_xpart32.alloc(c_tile.size() * 3 * kTileCols * sizeof(float));
     d_row_a.upload(ra);
     d_row_len.upload(rl);
     d_row_off.upload(ro);
@@ -255,6 +310,35 @@ void Engine::build_device(int threads) {
     d_tile_rows.upload(trows);
     d_perm.upload(S.perm);
     d_iperm.upload(S.iperm);
+    auto fill_plan = [&](auto& P, const void* vals) {
+        using PT = std::remove_reference_t<decltype(P)>;
+        P = PT();
+        P.n = n;
+        P.npad = npad_;
+        P.row_off = d_row_off.as<int64_t>();
+        P.row_a = d_row_a.as<int>();
+        P.row_len = d_row_len.as<int>();
+        P.n_short = (int)shorts.size();
+        P.n_groups = (int)g_row0.size();
+        P.short_rows = d_short_rows.as<int>();
+        P.grp_row0 = d_grp_row0.as<int>();
+        P.grp_g = d_grp_g.as<int>();
+        P.n_chunks = (int)c_tile.size();
+        P.ntiles = ntiles_;
+        P.chunk_tile = d_chunk_tile.as<int>();
+        P.chunk_p0 = d_chunk_p0.as<int>();
+        P.chunk_p1 = d_chunk_p1.as<int>();
+        P.tile_rows = d_tile_rows.as<int>();
+        P.tile_chunk_ptr = d_tile_chunk_ptr.as<int>();
+        P.perm = d_perm.as<int>();
+        (void)vals;
+    };
+    fill_plan(plan64_, nullptr);
+    fill_plan(plan32_, nullptr);
+    plan64_.vals = d_vals64.as<double>();
+    plan64_.xpart = d_xpart64.as<double>();
+    plan32_.vals = d_vals32.as<float>();
+    plan32_.xpart = d_xpart32.as<float>();
     // mesh, samples, constraints
     dE.upload(M.E);
     dX.upload(M.X);
@@ -305,6 +389,7 @@ void Engine::build_device(int threads) {
         b->alloc(ld * sizeof(double));
     d_dG.alloc(ld * kMaxWindow * sizeof(double));
     d_dX.alloc(ld * kMaxWindow * sizeof(double));
+    red_blocks_ = std::max(1, std::min(kRedBlocks, (n3 + 2047) / 2048));
     d_part_gate.alloc(kRedBlocks * 2 * sizeof(double));
     d_part_aa.alloc(kRedBlocks * 64 * sizeof(double));
     d_part_upd.alloc(kRedBlocks * 3 * sizeof(double));
@@ -325,6 +410,27 @@ void Engine::build_device(int threads) {
     if (M.has_gravity)
         for (int d = 0; d < 3; ++d) gf[d] = M.mass() * M.gravity[d];
     d_gravf.copy_in(gf, sizeof(gf));
+    {
+        std::vector<int> npk, tk, ok;
+        int off = 0;
+        for (const auto& en : M.energies) {
+            npk.push_back((int)en.params.size());
+            tk.push_back(en.type);
+            ok.push_back(off);
+            off += (int)en.params.size();
+        }
+        d_np_k.upload(npk);
+        d_type_k.upload(tk);
+        d_off_k.upload(ok);
+        d_dmat_dev.alloc(std::max<size_t>(1, npk.size()) * sizeof(double));
+        d_dpar_dev.alloc(std::max(1, off) * sizeof(double));
+        d_dstate_dev.alloc(3 * sizeof(double));
+        d_adjnorm.alloc(2 * sizeof(double));
+        CUDA_OK(cudaMemset(d_adjnorm.p, 0, 2 * sizeof(double)));
+        d_part_adj.alloc(kRedBlocks * 3 * sizeof(double));
+        for (DeviceBuffer* b : {&d_gq, &d_gv, &d_dq, &d_dv, &d_df}) b->alloc(ld * sizeof(double));
+    }
+    drop_graphs();
     device_ready_ = true;
 }
 
@@ -348,18 +454,88 @@ EnergyPack Engine::energy_pack() const {
 
 void Engine::launch_ainv(bool fp32, cudaStream_t st) {
     Ctrl* c = d_ctrl.as<Ctrl>();
-    if (fp32) {
-        launch_spmv_S<float>(M.n, d_row_off.as<int64_t>(), d_row_a.as<int>(), d_row_len.as<int>(),
-                             d_vals32.as<float>(), d_vperm32.as<float>(), npad_, d_y32.as<float>(), c, st);
-        launch_spmv_ST<float>(M.n, ntiles_, d_tile_ptr.as<int>(), d_tile_rows.as<int>(), d_row_off.as<int64_t>(),
-                              d_row_a.as<int>(), d_row_len.as<int>(), d_vals32.as<float>(), d_y32.as<float>(), npad_,
-                              d_perm.as<int>(), d_xraw.as<double>(), c, st);
+    if (fp32) launch_sts<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), d_xraw.as<double>(), c, st);
+    else launch_sts<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), d_xraw.as<double>(), c, st);
+}
+
+// One PD iteration: local step, gather to the permuted right-hand side, A^-1 pair, Anderson + gate.
+void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
+    const int n = M.n, n3 = 3 * n;
+    const double inv_h2m = M.mass() / (graph_dt_ * graph_dt_);
+    const double vol_over_s = M.vol / M.s;
+    const EnergyPack ep = energy_pack();
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    if (f32) {
+        launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                               d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                               d_elem_out32.as<float>(), c, st);
+        launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out32.as<float>(),
+                                 d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                                 d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
+                                 red_blocks_, c, st);
     } else {
-        launch_spmv_S<double>(M.n, d_row_off.as<int64_t>(), d_row_a.as<int>(), d_row_len.as<int>(),
-                              d_vals64.as<double>(), d_vperm64.as<double>(), npad_, d_y64.as<double>(), c, st);
-        launch_spmv_ST<double>(M.n, ntiles_, d_tile_ptr.as<int>(), d_tile_rows.as<int>(), d_row_off.as<int64_t>(),
-                               d_row_a.as<int>(), d_row_len.as<int>(), d_vals64.as<double>(), d_y64.as<double>(),
-                               npad_, d_perm.as<int>(), d_xraw.as<double>(), c, st);
+        launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                                d_elem_out64.as<double>(), c, st);
+        launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
+                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                                  d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
+                                  red_blocks_, c, st);
+    }
+    launch_ainv(f32, st);
+    launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
+                     d_lx.as<double>(), n3, d_part_aa.as<double>(), red_blocks_, c, st);
+    launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3, d_part_upd.as<double>(),
+                     d_part_gate.as<double>(), red_blocks_, red_blocks_, c, st);
+}
+
+// One adjoint iteration: K_pd mu, gather of g_bar + K_pd mu, A^-1 pair, Anderson + gate.
+void Engine::enqueue_bwd_iteration(cudaStream_t st) {
+    const int n = M.n, n3 = 3 * n;
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
+                    d_elem_out64.as<double>(), c, st);
+    launch_gather_bwd(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(), d_gbar.as<double>(),
+                      d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_, c, st);
+    launch_ainv(false, st);
+    launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
+                     d_lx.as<double>(), n3, d_part_aa.as<double>(), red_blocks_, c, st);
+    launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3, d_part_upd.as<double>(),
+                     d_part_gate.as<double>(), 0, red_blocks_, c, st);
+}
+
+// Runs iterations until the device-side gate sets `done`: one iteration is captured once as a CUDA graph and
+// replayed; the control block is read back every few iterations (doubling up to poll_chunk).
+void Engine::run_iterations(int mode, const Options& o, cudaStream_t st) {
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    cudaGraphExec_t& g = graphs_[mode];
+    if (!g) {
+        cudaStream_t cap;
+        CUDA_OK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t graph;
+        CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        if (mode == 2) enqueue_bwd_iteration(cap);
+        else enqueue_fwd_iteration(mode == 1, cap);
+        CUDA_OK(cudaStreamEndCapture(cap, &graph));
+        CUDA_OK(cudaGraphGetNodes(graph, nullptr, &graph_nodes_[mode]));
+        CUDA_OK(cudaGraphInstantiate(&g, graph, 0));
+        CUDA_OK(cudaGraphDestroy(graph));
+        CUDA_OK(cudaStreamDestroy(cap));
+    }
+    int launched = 0, chunk = std::min(o.poll_chunk, 4);
+    while (launched < o.max_pd_iter) {
+        const int todo = std::min(chunk, o.max_pd_iter - launched);
+        for (int it = 0; it < todo; ++it) CUDA_OK(cudaGraphLaunch(g, st));
+        launched += todo;
+        launches_ += (long long)todo * (long long)graph_nodes_[mode];
+        CUDA_OK(cudaMemcpyAsync(h_ctrl_, c, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        if (h_ctrl_->done) break;
+        chunk = std::min(chunk * 2, std::max(o.poll_chunk, 4));
     }
 }
 
@@ -379,53 +555,17 @@ void Engine::check_status(const char* where) {
 }
 
 void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st) {
-    const int n = M.n, n3 = 3 * n;
-    const double inv_h2m = M.mass() / (h * h);
-    const double vol_over_s = M.vol / M.s;
-    const EnergyPack ep = energy_pack();
+    const int n3 = 3 * M.n;
     Ctrl* c = d_ctrl.as<Ctrl>();
     CUDA_OK(cudaMemcpyAsync(d_x.p, dq_in, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CUDA_OK(cudaMemsetAsync(d_prev_pd.p, 0, n3 * sizeof(double), st));
     init_ctrl(h_ctrl_, 0, o, o.max_pd_iter, 0.0);
     CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
-    const bool f32 = o.fp32_bulk != 0;
-    int launched = 0;
-    int chunk = std::min(o.poll_chunk, 4);
-    while (launched < o.max_pd_iter) {
-        const int todo = std::min(chunk, o.max_pd_iter - launched);
-        for (int it = 0; it < todo; ++it) {
-            if (f32) {
-                launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
-                                       d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
-                                       d_elem_out32.as<float>(), c, st);
-                launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out32.as<float>(),
-                                         d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(),
-                                         d_iperm.as<int>(), d_vperm32.as<float>(), npad_, nullptr,
-                                         d_prev_pd.as<double>(), d_part_gate.as<double>(), c, st);
-            } else {
-                launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
-                                        d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
-                                        d_elem_out64.as<double>(), c, st);
-                launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
-                                          d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(),
-                                          d_iperm.as<int>(), d_vperm64.as<double>(), npad_, nullptr,
-                                          d_prev_pd.as<double>(), d_part_gate.as<double>(), c, st);
-            }
-            launch_ainv(f32, st);
-            launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
-                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
-                             d_lx.as<double>(), n3, d_part_aa.as<double>(), c, st);
-            launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
-                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3,
-                             d_part_upd.as<double>(), d_part_gate.as<double>(), kRedBlocks, c, st);
-        }
-        CUDA_OK(cudaGetLastError());
-        launched += todo;
-        CUDA_OK(cudaMemcpyAsync(h_ctrl_, c, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
-        CUDA_OK(cudaStreamSynchronize(st));
-        if (h_ctrl_->done) break;
-        chunk = std::min(chunk * 2, std::max(o.poll_chunk, 4));
+    if (graph_dt_ != h) {
+        drop_graphs();
+        graph_dt_ = h;
     }
+    run_iterations(o.fp32_bulk ? 1 : 0, o, st);
     check_status("forward");
     stats.frame_iters.push_back(h_ctrl_->iter);
     stats.frame_converged.push_back(h_ctrl_->converged);
@@ -444,6 +584,7 @@ void Engine::forward_device(const double* dq, const double* dv, const double* df
     run_forward_loop(dq, dt, o, st);
     CUDA_OK(cudaMemcpyAsync(dqn, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     launch_velocity(n3, d_x.as<double>(), dq, 1.0 / dt, dvn, st);
+    launches_ += 2;
     CUDA_OK(cudaGetLastError());
 }
 
@@ -463,139 +604,111 @@ void Engine::forward(const double* q, const double* v, const double* f_ext, doub
     active.clear();
 }
 
+void Engine::backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt,
+                             const Options& o, double* d_dq, double* d_dv, double* d_df, double* d_dmat_w,
+                             double* d_dparams, double* d_dstate_p, cudaStream_t st) {
+    DPHD_CHECK(!M.has_plane || M.contact_nodes.empty(),
+               "Frictional contact is not available in this build of the adjoint.");
+    ensure_built(dt, o.thread_ct);
+    const int n3 = 3 * M.n, m = M.m;
+    const double h = dt, mass = M.mass(), inv_h2m = mass / (h * h), h2m = h * h / mass;
+    const EnergyPack ep = energy_pack();
+    const double vol_over_s = M.vol / M.s;
+    launch_adj_prepare(n3, d_gq, d_gv, 1.0 / h, d_gbar.as<double>(), d_dq, d_part_adj.as<double>(),
+                       d_adjnorm.as<double>(), st);
+    d_J.alloc((size_t)m * M.s * 81 * sizeof(double));
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
+    CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    launch_jac_build(m, M.k, M.s, dE.as<int>(), d_q_next, dgrad.as<double>(), M.hex, vol_over_s, ep,
+                     o.bwd_mean_stiffness, o.bwd_eigen_filter, d_J.as<double>(), c, st);
+    CUDA_OK(cudaMemsetAsync(d_x.p, 0, n3 * sizeof(double), st));
+    launches_ += 2;
+    if (graph_dt_ != h) {
+        drop_graphs();
+        graph_dt_ = h;
+    }
+    run_iterations(2, o, st);
+    stats.last_bwd_iters = h_ctrl_->iter;
+    stats.last_filtered = (int)h_ctrl_->arrive[3];
+    const int ne = (int)M.energies.size(), np = num_pd_params();
+    const bool diverged = (h_ctrl_->status & (kStatusDiverged | kStatusNonFinite)) != 0;
+    if (diverged) {  // reference: a diverged backbone contributes nothing downstream (backward_gpu.cpp:873-880)
+        CUDA_OK(cudaMemsetAsync(d_dv, 0, n3 * sizeof(double), st));
+        CUDA_OK(cudaMemsetAsync(d_df, 0, n3 * sizeof(double), st));
+        if (d_dmat_w && ne) CUDA_OK(cudaMemsetAsync(d_dmat_w, 0, ne * sizeof(double), st));
+        if (d_dparams && np) CUDA_OK(cudaMemsetAsync(d_dparams, 0, np * sizeof(double), st));
+        if (d_dstate_p && M.has_gravity) CUDA_OK(cudaMemsetAsync(d_dstate_p, 0, 3 * sizeof(double), st));
+        return;
+    }
+    launch_adj_route(n3, d_x.as<double>(), h_ctrl_->rn, d_adjnorm.as<double>(), inv_h2m, h, h2m, mass,
+                     o.bwd_cascade_cap, M.has_gravity ? 1 : 0, d_dq, d_dv, d_df,
+                     d_dstate_p ? d_dstate_p : d_dstate_dev.as<double>(), d_part_adj.as<double>(),
+                     reinterpret_cast<unsigned int*>(d_adjnorm.as<double>() + 1), st);
+    d_gw.alloc((size_t)kMaxEnergies * m * sizeof(double));
+    d_gmat.alloc((size_t)kMaxEnergies * m * sizeof(double));
+    d_gnh.alloc((size_t)kMaxEnergies * m * 2 * sizeof(double));
+    launch_param_grad(m, M.k, M.s, dE.as<int>(), d_q_next, d_x.as<double>(), dgrad.as<double>(), M.hex, vol_over_s,
+                      ep, d_gw.as<double>(), d_gmat.as<double>(), d_gnh.as<double>(), st);
+    launch_param_reduce(m, ne, d_np_k.as<int>(), d_type_k.as<int>(), d_off_k.as<int>(), d_gw.as<double>(),
+                        d_gmat.as<double>(), d_gnh.as<double>(), d_dmat_w ? d_dmat_w : d_dmat_dev.as<double>(),
+                        d_dparams ? d_dparams : d_dpar_dev.as<double>(), st);
+    launches_ += 3;
+    CUDA_OK(cudaGetLastError());
+}
+
 void Engine::backward(const double* q, const double* v, const double* f_ext, double dt, const double* q_next,
                       const double* v_next, const double* dl_dq_next, const double* dl_dv_next, const Options& o,
                       double* dl_dq, double* dl_dv, double* dl_df, double* dl_dmat_w, double* dl_dparams,
                       double* dl_dstate_p) {
     (void)q; (void)v; (void)f_ext; (void)v_next;
-    DPHD_CHECK(!M.has_plane || M.contact_nodes.empty(),
-               "Frictional contact is not available in this build of the adjoint.");
     ensure_built(dt, o.thread_ct);
-    const int n = M.n, n3 = 3 * n, m = M.m;
-    const double h = dt, inv_h = 1.0 / h;
-    const double mass = M.mass(), inv_h2m = mass / (h * h), h2m = h * h / mass;
+    const int n3 = dofs();
     cudaStream_t st = stream_;
-    std::vector<double> gbar(n3);
-    for (int i = 0; i < n3; ++i) {
-        dl_dq[i] = -dl_dv_next[i] * inv_h;
-        dl_dv[i] = 0;
-        dl_df[i] = 0;
-        gbar[i] = dl_dq_next[i] + dl_dv_next[i] * inv_h;
-    }
     CUDA_OK(cudaMemcpyAsync(d_qn.p, q_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMemcpyAsync(d_gbar.p, gbar.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, st));
-    const EnergyPack ep = energy_pack();
-    const double vol_over_s = M.vol / M.s;
-    d_J.alloc((size_t)m * M.s * 81 * sizeof(double));
-    Ctrl* c = d_ctrl.as<Ctrl>();
-    init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
-    CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
-    launch_jac_build(m, M.k, M.s, dE.as<int>(), d_qn.as<double>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
-                     o.bwd_mean_stiffness, o.bwd_eigen_filter, d_J.as<double>(), c, st);
-    CUDA_OK(cudaMemsetAsync(d_x.p, 0, n3 * sizeof(double), st));
-    int launched = 0, chunk = std::min(o.poll_chunk, 4);
-    while (launched < o.max_pd_iter) {
-        const int todo = std::min(chunk, o.max_pd_iter - launched);
-        for (int it = 0; it < todo; ++it) {
-            launch_kpd_elem(m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
-                            d_J.as<double>(), d_elem_out64.as<double>(), c, st);
-            launch_gather_bwd(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
-                              d_gbar.as<double>(), d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
-                              d_vperm64.as<double>(), npad_, c, st);
-            launch_ainv(false, st);
-            launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
-                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
-                             d_lx.as<double>(), n3, d_part_aa.as<double>(), c, st);
-            launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
-                             d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3,
-                             d_part_upd.as<double>(), d_part_gate.as<double>(), 0, c, st);
-        }
-        CUDA_OK(cudaGetLastError());
-        launched += todo;
-        CUDA_OK(cudaMemcpyAsync(h_ctrl_, c, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
-        CUDA_OK(cudaStreamSynchronize(st));
-        if (h_ctrl_->done) break;
-        chunk = std::min(chunk * 2, std::max(o.poll_chunk, 4));
-    }
-    stats.last_bwd_iters = h_ctrl_->iter;
-    stats.last_filtered = (int)h_ctrl_->arrive[3];
-    const int np = num_pd_params();
-    const int ne = (int)M.energies.size();
-    for (int i = 0; i < ne; ++i) dl_dmat_w[i] = 0;
-    for (int i = 0; i < np; ++i) dl_dparams[i] = 0;
-    for (int i = 0; i < num_state_params(); ++i) dl_dstate_p[i] = 0;
-    const bool diverged = (h_ctrl_->status & (kStatusDiverged | kStatusNonFinite)) != 0;
-    if (diverged) return;  // reference: a diverged backbone contributes nothing downstream
-    std::vector<double> mu(n3);
-    CUDA_OK(cudaMemcpyAsync(mu.data(), d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    // parameter gradients at q_next
-    d_gw.alloc((size_t)kMaxEnergies * m * sizeof(double));
-    d_gmat.alloc((size_t)kMaxEnergies * m * sizeof(double));
-    d_gnh.alloc((size_t)kMaxEnergies * m * 2 * sizeof(double));
-    launch_param_grad(m, M.k, M.s, dE.as<int>(), d_qn.as<double>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
-                      vol_over_s, ep, d_gw.as<double>(), d_gmat.as<double>(), d_gnh.as<double>(), st);
-    std::vector<double> gw((size_t)ne * m), gmat((size_t)ne * m), gnh((size_t)ne * m * 2);
-    CUDA_OK(cudaMemcpyAsync(gw.data(), d_gw.p, gw.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaMemcpyAsync(gmat.data(), d_gmat.p, gmat.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaMemcpyAsync(gnh.data(), d_gnh.p, gnh.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaStreamSynchronize(st));
-    CUDA_OK(cudaGetLastError());
-    // downstream routing (backward_gpu.cpp:881-917)
-    std::vector<double> inj(n3);
-    double in2 = 0, g2 = 0;
-    for (int i = 0; i < n3; ++i) {
-        inj[i] = inv_h2m * mu[i];
-        in2 += inj[i] * inj[i];
-        g2 += gbar[i] * gbar[i];
-    }
-    if (o.bwd_cascade_cap) {
-        const double cap = std::sqrt(g2) + 1.0, in = std::sqrt(in2);
-        if (in > cap)
-            for (auto& x : inj) x *= cap / in;
-    }
-    for (int i = 0; i < n3; ++i) {
-        dl_dq[i] += inj[i];
-        dl_df[i] += h2m * inj[i];
-        dl_dv[i] += h * inj[i];
-    }
+    CUDA_OK(cudaMemcpyAsync(d_gq.p, dl_dq_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_gv.p, dl_dv_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    backward_device(d_qn.as<double>(), d_gq.as<double>(), d_gv.as<double>(), dt, o, d_dq.as<double>(),
+                    d_dv.as<double>(), d_df.as<double>(), d_dmat_dev.as<double>(), d_dpar_dev.as<double>(),
+                    d_dstate_dev.as<double>(), st);
+    const int ne = (int)M.energies.size(), np = num_pd_params();
+    CUDA_OK(cudaMemcpyAsync(dl_dq, d_dq.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(dl_dv, d_dv.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(dl_df, d_df.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (ne) CUDA_OK(cudaMemcpyAsync(dl_dmat_w, d_dmat_dev.p, ne * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (np) CUDA_OK(cudaMemcpyAsync(dl_dparams, d_dpar_dev.p, np * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (M.has_gravity)
-        for (int i = 0; i < n3; ++i) dl_dstate_p[i % 3] += h2m * inj[i] * mass;
-    int off = 0;
-    for (int k = 0; k < ne; ++k) {
-        const PdEnergy& en = M.energies[k];
-        const double* w = &gw[(size_t)k * m];
-        double tot = 0;
-        for (int e = 0; e < m; ++e) tot += gmat[(size_t)k * m + e];
-        dl_dmat_w[k] = tot;
-        const int npk = (int)en.params.size();
-        if (en.type != kNeoHookean) {
-            if (npk == 1) {
-                double s = 0;
-                for (int e = 0; e < m; ++e) s += w[e];
-                dl_dparams[off] = s;
-            } else {
-                for (int e = 0; e < m; ++e) dl_dparams[off + e] = w[e];
-            }
-        } else {
-            double gmb = 0, glb = 0;
-            for (int e = 0; e < m; ++e) {
-                gmb += gnh[((size_t)k * m + e) * 2];
-                glb += gnh[((size_t)k * m + e) * 2 + 1];
-            }
-            if (npk == 2) {
-                double s = 0;
-                for (int e = 0; e < m; ++e) s += w[e];
-                dl_dparams[off] = 2 * s + gmb;
-                dl_dparams[off + 1] = glb;
-            } else {
-                for (int e = 0; e < m; ++e) {
-                    dl_dparams[off + 2 * e] = 2 * w[e] + gmb / m;
-                    dl_dparams[off + 2 * e + 1] = glb / m;
-                }
-            }
-        }
-        off += npk;
+        CUDA_OK(cudaMemcpyAsync(dl_dstate_p, d_dstate_dev.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+}
+
+double Engine::time_ainv(double dt, int reps, bool fp32, bool flush_l2) {
+    ensure_built(dt, 0);
+    cudaStream_t st = stream_;
+    init_ctrl(h_ctrl_, 0, Options(), 1, 0);
+    CUDA_OK(cudaMemcpyAsync(d_ctrl.p, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    DeviceBuffer flush;
+    if (flush_l2) flush.alloc((size_t)256 << 20);  // larger than the 126 MB L2
+    launch_ainv(fp32, st);  // warm
+    cudaEvent_t e0, e1;
+    CUDA_OK(cudaEventCreate(&e0));
+    CUDA_OK(cudaEventCreate(&e1));
+    double total = 0;
+    for (int r = 0; r < reps; ++r) {
+        if (flush_l2) CUDA_OK(cudaMemsetAsync(flush.p, r & 0xff, flush.bytes, st));
+        CUDA_OK(cudaEventRecord(e0, st));
+        launch_ainv(fp32, st);
+        CUDA_OK(cudaEventRecord(e1, st));
+        CUDA_OK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+        total += ms;
     }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CUDA_OK(cudaGetLastError());
+    launches_ += 4LL * (reps + 1);
+    return total / reps;
 }
 
 void Engine::apply_ainv(double dt, const double* b, double* x, bool fp32) {
@@ -674,8 +787,8 @@ void Engine::local_step(double dt, const double* q, double* rhs) {
                             d_elem_out64.as<double>(), d_ctrl.as<Ctrl>(), st);
     launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                               d_qt.as<double>(), 0.0, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
-                              d_vperm64.as<double>(), npad_, nullptr, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                              d_ctrl.as<Ctrl>(), st);
+                              d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
+                              red_blocks_, d_ctrl.as<Ctrl>(), st);
     // the gather leaves pd (node-major) in prev_pd
     CUDA_OK(cudaMemcpyAsync(rhs, d_prev_pd.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(h_ctrl_, d_ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));

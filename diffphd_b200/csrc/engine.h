@@ -68,6 +68,8 @@ public:
     int num_state_params() const { return M.has_gravity ? 3 : 0; }
     long long s_memory_bytes() const;
     long long s_nnz() const { return S.nnz(); }
+    long long s_padded_values() const { return (long long)(d_vals64.bytes / sizeof(double)); }
+    int num_nodes() const { return M.n; }
     int s_depth() const { return S.max_depth; }
 
     // host-pointer step (drop-in for PyForward / PyBackward)
@@ -80,6 +82,13 @@ public:
     // device-pointer step (inputs and outputs already in HBM, launched on `stream`)
     void forward_device(const double* d_q, const double* d_v, const double* d_f, double dt, const Options& o,
                         double* d_q_next, double* d_v_next, cudaStream_t stream);
+
+    void backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,
+                         double* d_dq, double* d_dv, double* d_df, double* d_dmat_w, double* d_dparams,
+                         double* d_dstate_p, cudaStream_t stream);
+    // time `reps` applications of the S^T S pair on the device; returns ms per application
+    double time_ainv(double dt, int reps, bool fp32, bool flush_l2);
+    long long kernel_launches() const { return launches_; }
 
     // diagnostics used by the tests
     void apply_ainv(double dt, const double* b, double* x, bool fp32);
@@ -95,25 +104,38 @@ private:
     EnergyPack energy_pack() const;
     void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st);
     void launch_ainv(bool fp32, cudaStream_t st);  // d_vperm -> d_xraw
+    void enqueue_fwd_iteration(bool fp32, cudaStream_t st);
+    void enqueue_bwd_iteration(cudaStream_t st);
+    void run_iterations(int mode, const Options& o, cudaStream_t st);  // mode 0 fwd64, 1 fwd32, 2 bwd
+    void drop_graphs();
     void check_status(const char* where);
 
     bool built_ = false;
     double built_dt_ = -1;
     SFactor S;
     NodeMatrix A;
-    int npad_ = 0, ntiles_ = 0;
+    int npad_ = 0, ntiles_ = 0, red_blocks_ = 1;
+    double graph_dt_ = -1;
+    cudaGraphExec_t graphs_[3] = {nullptr, nullptr, nullptr};
+    size_t graph_nodes_[3] = {0, 0, 0};
+    long long launches_ = 0;
+    SpmvPlan<double> plan64_;
+    SpmvPlan<float> plan32_;
     bool device_ready_ = false;
     cudaStream_t stream_ = nullptr;
 
     DeviceBuffer dE, dX, dgrad, d_elem_dir, d_fixed_node, d_fixed_dof, d_fixed_val, d_qb;
     DeviceBuffer d_node_ptr, d_node_inc, d_perm, d_iperm;
     DeviceBuffer d_row_off, d_row_a, d_row_len, d_vals64, d_vals32, d_tile_ptr, d_tile_rows;
+    DeviceBuffer d_short_rows, d_grp_row0, d_grp_g, d_chunk_tile, d_chunk_p0, d_chunk_p1, d_tile_chunk_ptr;
+    DeviceBuffer d_xpart64, d_xpart32;
     DeviceBuffer d_w[kMaxEnergies], d_w32[kMaxEnergies], d_mask[kMaxEnergies];
     DeviceBuffer d_q, d_v, d_f, d_qt, d_x, d_xraw, d_prev_pd, d_dG, d_dX, d_lg, d_lx;
     DeviceBuffer d_part_gate, d_part_aa, d_part_upd, d_gravf;
     DeviceBuffer d_elem_out64, d_elem_out32, d_vperm64, d_vperm32, d_y64, d_y32;
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
-    DeviceBuffer d_ctrl;
+    DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
+    DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

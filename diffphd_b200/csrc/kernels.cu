@@ -4,6 +4,8 @@
 // the partials in block order.  No floating-point atomics are used.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace dphd {
@@ -55,6 +57,22 @@ __device__ __forceinline__ bool arrive_last(unsigned int* counter) {
     }
     __syncthreads();
     return last;
+}
+
+// Sum NV partial values over `nb` blocks (layout part[b * NV + i]) with all threads of the calling block in a
+// fixed order (thread t takes blocks t, t + blockDim, ...; then a fixed tree); result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void sum_partials(const double* part, int nb, double* out, double* sh) {
+    double v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] += __ldcg(part + (size_t)b * NV + i);
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) out[i] = v[i];
 }
 
 template <typename T>
@@ -229,29 +247,46 @@ template <> struct Vec4<double> {
     }
 };
 
+// y = S v, short rows: one warp per row (row length <= kShortRowMax), two 16-byte loads in flight per lane.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_spmv_S(int n, const int64_t* __restrict__ row_off,
-                                                     const int* __restrict__ row_a, const int* __restrict__ row_len,
-                                                     const T* __restrict__ vals, const T* __restrict__ v, int npad,
-                                                     T* __restrict__ y, const Ctrl* ctrl) {
+__global__ void __launch_bounds__(kThreads) k_spmv_S_short(SpmvPlan<T> p, const T* __restrict__ v,
+                                                           T* __restrict__ y, const Ctrl* ctrl) {
     if (ctrl->done) return;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const int i = n - 1 - warp;  // rows near the etree root are the longest: schedule them first
-    const int64_t off = row_off[i];
-    const int a = row_a[i], len = row_len[i];
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= p.n_short) return;
+    const int i = __ldg(p.short_rows + w);
+    const int64_t off = __ldg(p.row_off + i);
+    const int a = __ldg(p.row_a + i), len = __ldg(p.row_len + i);
+    const int npad = p.npad;
     T s0 = T(0), s1 = T(0), s2 = T(0);
-    for (int c = lane * 4; c < len; c += 128) {
+    for (int c = lane * 4; c < len; c += 256) {
         Vec4<T> sv, v0, v1, v2;
-        sv.load_stream(vals + off + c);
+        sv.load_stream(p.vals + off + c);
         v0.load(v + a + c);
         v1.load(v + npad + a + c);
         v2.load(v + 2 * (size_t)npad + a + c);
+        const int c2 = c + 128;
+        Vec4<T> tv, u0, u1, u2;
+        const bool two = c2 < len;
+        if (two) {
+            tv.load_stream(p.vals + off + c2);
+            u0.load(v + a + c2);
+            u1.load(v + npad + a + c2);
+            u2.load(v + 2 * (size_t)npad + a + c2);
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             s0 += sv.v[q] * v0.v[q];
             s1 += sv.v[q] * v1.v[q];
             s2 += sv.v[q] * v2.v[q];
+        }
+        if (two) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                s0 += tv.v[q] * u0.v[q];
+                s1 += tv.v[q] * u1.v[q];
+                s2 += tv.v[q] * u2.v[q];
+            }
         }
     }
     s0 = warp_sum(s0);
@@ -264,30 +299,88 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S(int n, const int64_t* __res
     }
 }
 
-template <typename T, int NW>
-__global__ void __launch_bounds__(NW * 32) k_spmv_ST(int n, const int* __restrict__ tile_ptr,
-                                                     const int* __restrict__ tile_rows,
-                                                     const int64_t* __restrict__ row_off,
-                                                     const int* __restrict__ row_a, const int* __restrict__ row_len,
-                                                     const T* __restrict__ vals, const T* __restrict__ y, int npad,
-                                                     const int* __restrict__ perm, double* __restrict__ x_out,
+// y = S v, long rows: one CTA (8 warps) per group of g rows that share their first column (members of one
+// nested-dissection separator).  The group's columns stream through shared memory in chunks of
+// kStageCols; each chunk of v is read once and used by all g rows; 8/g warps split a row's chunk.
+constexpr int kStageCols = 1024;
+template <typename T>
+__global__ void __launch_bounds__(256) k_spmv_S_long(SpmvPlan<T> p, const T* __restrict__ v, T* __restrict__ y,
                                                      const Ctrl* ctrl) {
     if (ctrl->done) return;
-    __shared__ T red[NW][3][kTileCols];
-    const int tile = blockIdx.x, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ __align__(16) T sv[3][kStageCols];
+    __shared__ T red[8][3];
+    const int grp = blockIdx.x;
+    const int row0 = __ldg(p.grp_row0 + grp), g = __ldg(p.grp_g + grp);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpr = 8 / g;                       // warps per row
+    const int row = row0 + wid / wpr, sub = wid % wpr;
+    const int a = __ldg(p.row_a + row0);
+    int glen = 0;                                // longest row of the group (the last one)
+    for (int r = 0; r < g; ++r) glen = max(glen, __ldg(p.row_len + row0 + r));
+    const int len = __ldg(p.row_len + row);
+    const int64_t off = __ldg(p.row_off + row);
+    const int npad = p.npad;
+    const int span = kStageCols / wpr;           // columns of one chunk handled by this warp
+    T s0 = T(0), s1 = T(0), s2 = T(0);
+    for (int c0 = 0; c0 < glen; c0 += kStageCols) {
+        __syncthreads();
+        for (int t = threadIdx.x * 4; t < 3 * kStageCols; t += 256 * 4) {
+            const int d = t / kStageCols, c = t % kStageCols;
+            Vec4<T> x;
+            if (a + c0 + c < npad) x.load(v + (size_t)d * npad + a + c0 + c);
+            else x.v[0] = x.v[1] = x.v[2] = x.v[3] = T(0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sv[d][c + q] = x.v[q];
+        }
+        __syncthreads();
+        const int cb = sub * span;
+        for (int c = cb + lane * 4; c < cb + span; c += 128) {
+            if (c0 + c >= len) break;
+            Vec4<T> s;
+            s.load_stream(p.vals + off + c0 + c);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                s0 += s.v[q] * sv[0][c + q];
+                s1 += s.v[q] * sv[1][c + q];
+                s2 += s.v[q] * sv[2][c + q];
+            }
+        }
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    if (lane == 0) { red[wid][0] = s0; red[wid][1] = s1; red[wid][2] = s2; }
+    __syncthreads();
+    if (threadIdx.x < 3 * g) {
+        const int r = threadIdx.x / 3, d = threadIdx.x % 3;
+        T t = T(0);
+        for (int k = 0; k < wpr; ++k) t += red[r * wpr + k][d];
+        y[(size_t)d * npad + row0 + r] = t;
+    }
+}
+
+// x = S^T y, stage 1: one CTA per (column tile, chunk of the tile's row list); partial tile sums are written
+// to xpart[chunk] and summed in chunk order by stage 2.
+template <typename T>
+__global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ T red[8][3][kTileCols];
+    const int ch = blockIdx.x, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = __ldg(p.chunk_tile + ch);
     const int c = tile * kTileCols + lane * 4;
+    const int npad = p.npad;
     T acc[3][4];
 #pragma unroll
     for (int d = 0; d < 3; ++d)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[d][q] = T(0);
-    const int pe = tile_ptr[tile + 1];
-    for (int p = tile_ptr[tile] + wid; p < pe; p += NW) {
-        const int i = __ldg(tile_rows + p);
-        const int a = __ldg(row_a + i), len = __ldg(row_len + i);
+    const int pe = __ldg(p.chunk_p1 + ch);
+    for (int pp = __ldg(p.chunk_p0 + ch) + wid; pp < pe; pp += 8) {
+        const int i = __ldg(p.tile_rows + pp);
+        const int a = __ldg(p.row_a + i), len = __ldg(p.row_len + i);
         if (c >= a && c + 4 <= a + len) {
             Vec4<T> sv;
-            sv.load_stream(vals + __ldg(row_off + i) + (c - a));
+            sv.load_stream(p.vals + __ldg(p.row_off + i) + (c - a));
             const T y0 = __ldg(y + i), y1 = __ldg(y + npad + i), y2 = __ldg(y + 2 * (size_t)npad + i);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -302,14 +395,30 @@ __global__ void __launch_bounds__(NW * 32) k_spmv_ST(int n, const int* __restric
 #pragma unroll
         for (int q = 0; q < 4; ++q) red[wid][d][lane * 4 + q] = acc[d][q];
     __syncthreads();
-    for (int t = threadIdx.x; t < 3 * kTileCols; t += NW * 32) {
+    for (int t = threadIdx.x; t < 3 * kTileCols; t += 256) {
         const int d = t / kTileCols, col = t % kTileCols;
         T s = T(0);
 #pragma unroll
-        for (int w = 0; w < NW; ++w) s += red[w][d][col];
-        const int j = tile * kTileCols + col;
-        if (j < n) x_out[3 * (size_t)__ldg(perm + j) + d] = (double)s;
+        for (int w = 0; w < 8; ++w) s += red[w][d][col];
+        p.xpart[(size_t)ch * 3 * kTileCols + t] = s;
     }
+}
+
+// x = S^T y, stage 2: per tile column, sum the chunk partials in order and scatter to node-major x.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double* __restrict__ x_out,
+                                                          const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= p.ntiles * 3 * kTileCols) return;
+    const int tile = t / (3 * kTileCols), r = t % (3 * kTileCols);
+    const int d = r / kTileCols, col = r % kTileCols;
+    const int j = tile * kTileCols + col;
+    if (j >= p.n) return;
+    double s = 0.0;
+    for (int ch = __ldg(p.tile_chunk_ptr + tile); ch < __ldg(p.tile_chunk_ptr + tile + 1); ++ch)
+        s += (double)p.xpart[(size_t)ch * 3 * kTileCols + r];
+    x_out[3 * (size_t)__ldg(p.perm + j) + d] = s;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -367,11 +476,9 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
     if (threadIdx.x == 0)
         for (int i = 0; i < kAaVals; ++i) part[blockIdx.x * kAaVals + i] = acc[i];
     if (!arrive_last(&ctrl->arrive[0])) return;
-    if (threadIdx.x != 0) return;
     double tot[kAaVals];
-    for (int i = 0; i < kAaVals; ++i) tot[i] = 0.0;
-    for (int b = 0; b < gridDim.x; ++b)
-        for (int i = 0; i < kAaVals; ++i) tot[i] += __ldcg(part + b * kAaVals + i);
+    sum_partials<kAaVals>(part, gridDim.x, tot, sh);
+    if (threadIdx.x != 0) return;
     ctrl->arrive[0] = 0;
     ctrl->err = sqrt(tot[kAaVals - 2]);
     ctrl->xn = sqrt(tot[kAaVals - 1]);
@@ -470,24 +577,17 @@ __global__ void __launch_bounds__(kThreads) k_aa_update(int n3, double* __restri
         part[blockIdx.x * 3 + 2] = acc[2];
     }
     if (!arrive_last(&ctrl->arrive[1])) return;
+    double tt[3], gp[2] = {0.0, 0.0};
+    sum_partials<3>(part, gridDim.x, tt, sh);
+    if (mode == 0) sum_partials<2>(gate_part, gate_blocks, gp, sh);
     if (threadIdx.x != 0) return;
-    double t0 = 0, t1 = 0, t2 = 0;
-    for (int b = 0; b < gridDim.x; ++b) {
-        t0 += __ldcg(part + b * 3);
-        t1 += __ldcg(part + b * 3 + 1);
-        t2 += __ldcg(part + b * 3 + 2);
-    }
+    const double t0 = tt[0], t1 = tt[1], t2 = tt[2];
     ctrl->arrive[1] = 0;
     const double dq = sqrt(t0), rn = sqrt(t1), xnorm = sqrt(t2);
     bool conv = false;
     const int it = ctrl->iter;
     if (mode == 0) {
-        double p0 = 0, p1 = 0;
-        for (int b = 0; b < gate_blocks; ++b) {
-            p0 += __ldcg(gate_part + b * 2);
-            p1 += __ldcg(gate_part + b * 2 + 1);
-        }
-        const double pdc = sqrt(p0), pdr = sqrt(p1);
+        const double pdc = sqrt(gp[0]), pdr = sqrt(gp[1]);
         ctrl->dq = dq; ctrl->rn = rn; ctrl->pdc = pdc; ctrl->pdr = pdr;
         conv = it > 0 && dq <= ctrl->rel_tol * rn + ctrl->abs_tol && pdc <= ctrl->rel_tol * pdr + ctrl->abs_tol;
         if (!(dq == dq) || !(pdc == pdc)) ctrl->status |= kStatusNonFinite;
@@ -809,6 +909,106 @@ __global__ void __launch_bounds__(128) k_param_grad(int m, const int* __restrict
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_adj_prepare(int n3, const double* __restrict__ gq,
+                                                          const double* __restrict__ gv, double inv_h,
+                                                          double* __restrict__ gbar, double* __restrict__ dq,
+                                                          double* __restrict__ part, double* norm_out,
+                                                          unsigned int* arrive) {
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n3; r += gridDim.x * blockDim.x) {
+        const double g = gq[r] + gv[r] * inv_h;
+        gbar[r] = g;
+        dq[r] = -gv[r] * inv_h;
+        acc[0] += g * g;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+    if (!arrive_last(arrive)) return;
+    double t[1];
+    sum_partials<1>(part, gridDim.x, t, sh);
+    if (threadIdx.x == 0) {
+        norm_out[0] = sqrt(t[0]);
+        *arrive = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_adj_route(int n3, const double* __restrict__ mu, double mu_norm,
+                                                        const double* __restrict__ gbar_norm, double inv_h2m, double h,
+                                                        double h2m, double mass, int cap, int gravity,
+                                                        double* __restrict__ dq, double* __restrict__ dv,
+                                                        double* __restrict__ df, double* __restrict__ dstate,
+                                                        double* __restrict__ part, unsigned int* arrive) {
+    __shared__ double sh[3 * 32];
+    double s = 1.0;
+    if (cap) {
+        const double c = gbar_norm[0] + 1.0, in = inv_h2m * mu_norm;
+        if (in > c) s = c / in;
+    }
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n3; r += gridDim.x * blockDim.x) {
+        const double inj = s * inv_h2m * mu[r];
+        dq[r] += inj;
+        dv[r] = h * inj;
+        df[r] = h2m * inj;
+        acc[r % 3] += h2m * inj * mass;
+    }
+    block_sum<3>(acc, sh);
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 3; ++d) part[blockIdx.x * 3 + d] = acc[d];
+    if (!arrive_last(arrive)) return;
+    double t[3];
+    sum_partials<3>(part, gridDim.x, t, sh);
+    if (threadIdx.x == 0) {
+        if (gravity)
+            for (int d = 0; d < 3; ++d) dstate[d] = t[d];
+        *arrive = 0;
+    }
+}
+
+// One block per energy: fixed-order sums (deterministic).
+__global__ void k_param_reduce(int m, const int* __restrict__ np_k, const int* __restrict__ type_k,
+                               const int* __restrict__ off_k, const double* __restrict__ gw,
+                               const double* __restrict__ gmat, const double* __restrict__ gnh,
+                               double* __restrict__ dmat, double* __restrict__ dpar) {
+    __shared__ double sh[4 * 32];
+    const int k = blockIdx.x;
+    const int npk = np_k[k], type = type_k[k], off = off_k[k];
+    const double* w = gw + (size_t)k * m;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+        acc[0] += gmat[(size_t)k * m + e];
+        acc[1] += w[e];
+        acc[2] += gnh[((size_t)k * m + e) * 2];
+        acc[3] += gnh[((size_t)k * m + e) * 2 + 1];
+    }
+    block_sum<4>(acc, sh);
+    __shared__ double tot[4];
+    if (threadIdx.x == 0)
+        for (int i = 0; i < 4; ++i) tot[i] = acc[i];
+    __syncthreads();
+    if (threadIdx.x == 0) dmat[k] = tot[0];
+    if (type != 2) {
+        if (npk == 1) {
+            if (threadIdx.x == 0) dpar[off] = tot[1];
+        } else {
+            for (int e = threadIdx.x; e < m; e += blockDim.x) dpar[off + e] = w[e];
+        }
+    } else {
+        if (npk == 2) {
+            if (threadIdx.x == 0) {
+                dpar[off] = 2 * tot[1] + tot[2];
+                dpar[off + 1] = tot[3];
+            }
+        } else {
+            for (int e = threadIdx.x; e < m; e += blockDim.x) {
+                dpar[off + 2 * e] = 2 * w[e] + tot[2] / m;
+                dpar[off + 2 * e + 1] = tot[3] / m;
+            }
+        }
+    }
+}
+
 inline int blocks_for(long long work, int threads) { return (int)((work + threads - 1) / threads); }
 
 }  // namespace
@@ -828,38 +1028,30 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
 template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
-                       double* pd, double* prev_pd, double* part, Ctrl* ctrl, cudaStream_t st) {
-    (void)pd;
-    k_gather_fwd<T><<<kRedBlocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
+                       double* prev_pd, double* part, int blocks, Ctrl* ctrl, cudaStream_t st) {
+    k_gather_fwd<T><<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
                                                      v_perm, npad, prev_pd, part, ctrl);
 }
 
 template <typename T>
-void launch_spmv_S(int n, const int64_t* row_off, const int* row_a, const int* row_len, const T* vals, const T* v,
-                   int npad, T* y, const Ctrl* ctrl, cudaStream_t st) {
-    const int grid = blocks_for((long long)n * 32, kThreads);
-    k_spmv_S<T><<<grid, kThreads, 0, st>>>(n, row_off, row_a, row_len, vals, v, npad, y, ctrl);
-}
-
-template <typename T>
-void launch_spmv_ST(int n, int ntiles, const int* tile_ptr, const int* tile_rows, const int64_t* row_off,
-                    const int* row_a, const int* row_len, const T* vals, const T* y, int npad, const int* perm,
-                    double* x_out, const Ctrl* ctrl, cudaStream_t st) {
-    k_spmv_ST<T, 8><<<ntiles, 8 * 32, 0, st>>>(n, tile_ptr, tile_rows, row_off, row_a, row_len, vals, y, npad, perm,
-                                               x_out, ctrl);
+void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
+    if (p.n_groups) k_spmv_S_long<T><<<p.n_groups, 256, 0, st>>>(p, v, y, ctrl);
+    if (p.n_short) k_spmv_S_short<T><<<blocks_for((long long)p.n_short * 32, kThreads), kThreads, 0, st>>>(p, v, y, ctrl);
+    k_spmv_ST_part<T><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
+    k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
 }
 
 void launch_aa_reduce(int n3, const double* x, const double* x_raw, const unsigned char* fixed_dof,
                       const double* fixed_val, double* dG, double* dX, double* last_g, double* last_x, int ld,
-                      double* part, Ctrl* ctrl, cudaStream_t st) {
-    k_aa_reduce<<<kRedBlocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, last_g, last_x, ld, part,
+                      double* part, int blocks, Ctrl* ctrl, cudaStream_t st) {
+    k_aa_reduce<<<blocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, last_g, last_x, ld, part,
                                                 ctrl);
 }
 
 void launch_aa_update(int n3, double* x, const double* x_raw, const unsigned char* fixed_dof, const double* fixed_val,
                       const double* dG, const double* dX, int ld, double* part, const double* gate_part,
-                      int gate_blocks, Ctrl* ctrl, cudaStream_t st) {
-    k_aa_update<<<kRedBlocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, ld, part, gate_part,
+                      int gate_blocks, int blocks, Ctrl* ctrl, cudaStream_t st) {
+    k_aa_update<<<blocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, ld, part, gate_part,
                                                 gate_blocks, ctrl);
 }
 
@@ -910,19 +1102,34 @@ template void launch_elem_fwd<double>(int, int, int, const int*, const double*, 
 template void launch_elem_fwd<float>(int, int, int, const int*, const double*, const double*, const unsigned char*,
                                      const double*, int, double, const EnergyPack&, float*, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<double>(int, const int*, const int*, const double*, const double*, double,
-                                        const unsigned char*, const int*, double*, int, double*, double*, double*,
-                                        Ctrl*, cudaStream_t);
+                                        const unsigned char*, const int*, double*, int, double*, double*, int, Ctrl*,
+                                        cudaStream_t);
 template void launch_gather_fwd<float>(int, const int*, const int*, const float*, const double*, double,
-                                       const unsigned char*, const int*, float*, int, double*, double*, double*, Ctrl*,
+                                       const unsigned char*, const int*, float*, int, double*, double*, int, Ctrl*,
                                        cudaStream_t);
-template void launch_spmv_S<double>(int, const int64_t*, const int*, const int*, const double*, const double*, int,
-                                    double*, const Ctrl*, cudaStream_t);
-template void launch_spmv_S<float>(int, const int64_t*, const int*, const int*, const float*, const float*, int,
-                                   float*, const Ctrl*, cudaStream_t);
-template void launch_spmv_ST<double>(int, int, const int*, const int*, const int64_t*, const int*, const int*,
-                                     const double*, const double*, int, const int*, double*, const Ctrl*,
-                                     cudaStream_t);
-template void launch_spmv_ST<float>(int, int, const int*, const int*, const int64_t*, const int*, const int*,
-                                    const float*, const float*, int, const int*, double*, const Ctrl*, cudaStream_t);
+void launch_adj_prepare(int n3, const double* gq, const double* gv, double inv_h, double* gbar, double* dq,
+                        double* part, double* norm_out, cudaStream_t st) {
+    // norm_out[1] doubles as the arrival counter of this kernel (zeroed by the caller)
+    k_adj_prepare<<<std::max(1, std::min(kRedBlocks, (n3 + 2047) / 2048)), kThreads, 0, st>>>(
+        n3, gq, gv, inv_h, gbar, dq, part, norm_out, reinterpret_cast<unsigned int*>(norm_out + 1));
+}
+
+void launch_adj_route(int n3, const double* mu, double mu_norm, const double* gbar_norm, double inv_h2m, double h,
+                      double h2m, double mass, int cap, int gravity, double* dl_dq, double* dl_dv, double* dl_df,
+                      double* dl_dstate_p, double* part, unsigned int* arrive, cudaStream_t st) {
+    k_adj_route<<<std::max(1, std::min(kRedBlocks, (n3 + 2047) / 2048)), kThreads, 0, st>>>(
+        n3, mu, mu_norm, gbar_norm, inv_h2m, h, h2m, mass, cap, gravity, dl_dq, dl_dv, dl_df, dl_dstate_p, part,
+        arrive);
+}
+
+void launch_param_reduce(int m, int ne, const int* np_k, const int* type_k, const int* off_k, const double* gw,
+                         const double* gmat, const double* gnh, double* dl_dmat_w, double* dl_dparams,
+                         cudaStream_t st) {
+    if (ne > 0) k_param_reduce<<<ne, kThreads, 0, st>>>(m, np_k, type_k, off_k, gw, gmat, gnh, dl_dmat_w, dl_dparams);
+}
+
+template void launch_sts<double>(const SpmvPlan<double>&, const double*, double*, double*, const Ctrl*,
+                                 cudaStream_t);
+template void launch_sts<float>(const SpmvPlan<float>&, const float*, float*, double*, const Ctrl*, cudaStream_t);
 
 }  // namespace dphd

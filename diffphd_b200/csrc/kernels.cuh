@@ -47,23 +47,44 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
 template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
-                       double* pd, double* prev_pd, double* part, Ctrl* ctrl, cudaStream_t st);
-// y = S v and x = S^T y (x scattered to node-major FP64 through perm).
+                       double* prev_pd, double* part, int blocks, Ctrl* ctrl, cudaStream_t st);
+// Sparse-inverse SpMV pair x = S^T (S v) (3 right-hand sides, permuted SoA v and y, x node-major FP64).
+// S row i: row_len[i] values from column row_a[i] (both multiples of 4) at vals[row_off[i]].
 template <typename T>
-void launch_spmv_S(int n, const int64_t* row_off, const int* row_a, const int* row_len, const T* vals, const T* v,
-                   int npad, T* y, const Ctrl* ctrl, cudaStream_t st);
+struct SpmvPlan {
+    int n = 0, npad = 0;
+    const int64_t* row_off = nullptr;
+    const int* row_a = nullptr;
+    const int* row_len = nullptr;
+    const T* vals = nullptr;
+    // y = S v: short rows one warp each, long rows in groups of g in {1,2,4,8} rows sharing row_a, one CTA each
+    int n_short = 0, n_groups = 0;
+    const int* short_rows = nullptr;
+    const int* grp_row0 = nullptr;
+    const int* grp_g = nullptr;
+    // x = S^T y: column tiles of kTileCols, each tile's row list split into chunks (one CTA each)
+    int n_chunks = 0, ntiles = 0;
+    const int* chunk_tile = nullptr;
+    const int* chunk_p0 = nullptr;
+    const int* chunk_p1 = nullptr;
+    const int* tile_rows = nullptr;
+    const int* tile_chunk_ptr = nullptr;
+    T* xpart = nullptr;
+    const int* perm = nullptr;
+};
+constexpr int kShortRowMax = 1024;   // rows up to this length are handled by one warp
+constexpr int kChunkRows = 128;      // rows per S^T chunk CTA
+
 template <typename T>
-void launch_spmv_ST(int n, int ntiles, const int* tile_ptr, const int* tile_rows, const int64_t* row_off,
-                    const int* row_a, const int* row_len, const T* vals, const T* y, int npad, const int* perm,
-                    double* x_out, const Ctrl* ctrl, cudaStream_t st);
+void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
 
 // Anderson acceleration + gate ------------------------------------------------------------------
 void launch_aa_reduce(int n3, const double* x, const double* x_raw, const unsigned char* fixed_dof,
                       const double* fixed_val, double* dG, double* dX, double* last_g, double* last_x, int ld,
-                      double* part, Ctrl* ctrl, cudaStream_t st);
+                      double* part, int blocks, Ctrl* ctrl, cudaStream_t st);
 void launch_aa_update(int n3, double* x, const double* x_raw, const unsigned char* fixed_dof, const double* fixed_val,
                       const double* dG, const double* dX, int ld, double* part, const double* gate_part,
-                      int gate_blocks, Ctrl* ctrl, cudaStream_t st);
+                      int gate_blocks, int blocks, Ctrl* ctrl, cudaStream_t st);
 
 // Misc vector kernels
 void launch_qtilde(int n3, const double* q, const double* v, const double* f_ext, double h, double h2m,
@@ -87,5 +108,19 @@ void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const do
 void launch_param_grad(int m, int k, int s, const int* E, const double* q, const double* mu, const double* grad,
                        int hex, double vol_over_s, const EnergyPack& ep, double* gw /* [energies][m] */,
                        double* gmat /* [energies][m] */, double* gnh /* [energies][m][2] */, cudaStream_t st);
+
+// Device-side adjoint routing (backward_gpu.cpp:881-917) and parameter-gradient reductions.
+// g_bar = dl_dq_next + dl_dv_next / h;  dl_dq = -dl_dv_next / h;  |g_bar| into norm_out[0].
+void launch_adj_prepare(int n3, const double* dl_dq_next, const double* dl_dv_next, double inv_h, double* gbar,
+                        double* dl_dq, double* part, double* norm_out, cudaStream_t st);
+// inj = s * inv_h2m * mu with s = min(1, (|g_bar| + 1) / |inj|) when cap is set; dl_dq += inj, dl_dv = h inj,
+// dl_df = h2m inj, gravity parameter gradient (3 values) = sum over axis of h2m * inj * mass.
+void launch_adj_route(int n3, const double* mu, double mu_norm, const double* gbar_norm, double inv_h2m, double h,
+                      double h2m, double mass, int cap, int gravity, double* dl_dq, double* dl_dv, double* dl_df,
+                      double* dl_dstate_p, double* part, unsigned int* arrive, cudaStream_t st);
+// per energy: dl_dmat_w[k] = sum_e gmat[k][e]; dl_dparams from gw / gnh in the parameter layout of the energy.
+void launch_param_reduce(int m, int ne, const int* np_k, const int* type_k, const int* off_k, const double* gw,
+                         const double* gmat, const double* gnh, double* dl_dmat_w, double* dl_dparams,
+                         cudaStream_t st);
 
 }  // namespace dphd

@@ -88,6 +88,17 @@ int dphd_forward_device(dphd_deformable* h, const char* method, const double* d_
                         const double* d_f_ext, double dt, const char** opt_keys, const double* opt_vals, int nopts,
                         double* d_q_next, double* d_v_next, void* stream);
 
+/* Device-pointer adjoint step (BackwardProjectiveDynamicsAlgPhd, backward_gpu.cpp:648-1250, contact-free): reads
+ * q_next, dl_dq_next, dl_dv_next (device, 3n FP64) and writes dl_dq, dl_dv, dl_df_ext (device, 3n) and, when
+ * non-null, dl_dmat_w (device, #energies), dl_dparams (device, dphd_num_pd_params) and dl_dstate_p (device, 3). */
+int dphd_backward_device(dphd_deformable* h, const char* method, const double* d_q_next, const double* d_dl_dq_next,
+                         const double* d_dl_dv_next, double dt, const char** opt_keys, const double* opt_vals,
+                         int nopts, double* d_dl_dq, double* d_dl_dv, double* d_dl_df_ext, double* d_dl_dmat_w,
+                         double* d_dl_dparams, double* d_dl_dstate_p, void* stream);
+
+/* Number of kernels this library launched on the GPU since the handle was created (graph nodes included). */
+long long dphd_kernel_launches(const dphd_deformable* h);
+
 /* Per-frame statistics (AlgPhdFrameIters / AlgPhdFrameConverged / AlgPhdResetFrameStats,
  * cpp/core/include/fem/alg_phd_gpu_memory.h:25-27; forward_gpu.cpp:324-332). */
 int dphd_num_frames(const dphd_deformable* h);
@@ -97,6 +108,8 @@ int dphd_last_backward_iters(const dphd_deformable* h);
 /* AlgPhdSMemoryBytes / AlgPhdSNnz (forward_gpu.cpp:302-315): bytes of the S factor in HBM and its nnz. */
 long long dphd_s_memory_bytes(const dphd_deformable* h);
 long long dphd_s_nnz(const dphd_deformable* h);
+/* Stored S values including the 16-byte alignment padding of each row segment. */
+long long dphd_s_padded_values(const dphd_deformable* h);
 
 /* Diagnostics used by the tests: x = A^-1 b through the GPU S^T S pair (fp32 = 0 or 1), the same product
  * with the host copy of S (the set-up self-check of forward_gpu.cpp:653-670), and the GPU local step
@@ -104,6 +117,9 @@ long long dphd_s_nnz(const dphd_deformable* h);
 int dphd_debug_ainv(dphd_deformable* h, double dt, const double* b, double* x, int fp32);
 int dphd_debug_host_sts(dphd_deformable* h, double dt, const double* b, double* x);
 int dphd_debug_local_step(dphd_deformable* h, double dt, const double* q, double* rhs);
+/* Average device time (ms, CUDA events on the library's stream) of one S^T S pair over `reps` applications,
+ * optionally writing 256 MB between applications so that S is not served from L2. */
+int dphd_debug_time_ainv(dphd_deformable* h, double dt, int reps, int fp32, int flush_l2, double* ms_per_apply);
 
 #ifdef __cplusplus
 }

@@ -173,3 +173,30 @@ def test_singular_element_reports_error():
     q[:, 0] = 0.0  # flatten the mesh: every F is singular
     with pytest.raises(RuntimeError, match="Singular F"):
         d.debug_local_step(q.ravel(), sc.dt)
+
+
+def test_device_entry_points_match_host_entry_points():
+    import torch
+    sc = scenes.nh_tet_block(cells=(8, 4, 4), dx=0.01, steps=2)
+    opts = dict(sc.options)
+    d = core.from_scene(sc)
+    qn_h, vn_h = np.zeros(sc.dofs), np.zeros(sc.dofs)
+    d.PyForward("pd_eigen_alg_phd", sc.q0, sc.v0, [], sc.f_ext, sc.dt, opts, qn_h, vn_h, [])
+    dev = torch.device("cuda")
+    T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev).contiguous()
+    qn, vn = torch.empty(sc.dofs, dtype=torch.float64, device=dev), torch.empty(sc.dofs, dtype=torch.float64,
+                                                                                device=dev)
+    s = torch.cuda.Stream()
+    d.forward_device("pd_eigen_alg_phd", T(sc.q0), T(sc.v0), T(sc.f_ext), sc.dt, opts, qn, vn, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(qn.cpu().numpy(), qn_h) and np.array_equal(vn.cpu().numpy(), vn_h)
+    g = np.random.default_rng(0).standard_normal(sc.dofs)
+    ref = d.backward("pd_eigen_alg_phd", sc.q0, sc.v0, [], sc.f_ext, sc.dt, qn_h, vn_h, [], g, 0 * g, opts)
+    dq, dv, df = (torch.empty(sc.dofs, dtype=torch.float64, device=dev) for _ in range(3))
+    dpar = torch.empty(d.NumOfPdParams(), dtype=torch.float64, device=dev)
+    d.backward_device("pd_eigen_alg_phd", qn, T(g), T(0 * g), sc.dt, opts, dq, dv, df, dl_dparams=dpar,
+                      stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(dq.cpu().numpy(), ref["dl_dq"])
+    assert np.array_equal(dpar.cpu().numpy(), ref["dl_dparams"])
+    assert d.kernel_launches() > 0
