@@ -63,6 +63,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.bwd_cascade_cap = (int)get("bwd_cascade_cap", 1);
     o.bwd_eigen_filter = (int)get("bwd_eigen_filter", 0);
     o.fp32_bulk = (int)get("fp32_bulk", 0);
+    o.bwd_solver = (int)get("alg_phd_bwd_solver", 0);
     o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
@@ -256,27 +257,30 @@ void Engine::build_device(int threads) {
     std::vector<int> trows(tcnt[ntiles_]), tpos(tcnt.begin(), tcnt.end() - 1);
     for (int i = 0; i < n; ++i)
         for (int t = ra[i] / kTileCols; t <= (ra[i] + rl[i] - 1) / kTileCols; ++t) trows[tpos[t]++] = i;
-    // y = S v schedule: long rows (> kShortRowMax) in groups sharing their first column, short rows by warp
-    std::vector<int> shorts, g_row0, g_g;
+    // y = S v schedule: rows cut into segments of <= kSegCols columns.  Segments of consecutive rows that
+    // share their first column (one separator) are emitted row-fastest so one CTA reads one slice of v.
+    std::vector<int> it_row, it_c0, it_nc;
     for (int i = 0; i < n;) {
-        if (rl[i] <= kShortRowMax) {
-            shorts.push_back(i);
-            ++i;
-            continue;
-        }
-        int j = i;
-        while (j < n && rl[j] > kShortRowMax && ra[j] == ra[i] && j - i < 8) ++j;
-        int len = j - i, r = i;
-        for (int g : {8, 4, 2, 1})
-            while (len >= g) {
-                g_row0.push_back(r);
-                g_g.push_back(g);
-                r += g;
-                len -= g;
-            }
+        int j = i + 1;
+        while (j < n && ra[j] == ra[i] && j - i < 8) ++j;
+        int glen = 0;
+        for (int r = i; r < j; ++r) glen = std::max(glen, rl[r]);
+        for (int c0 = 0; c0 < glen; c0 += kSegCols)
+            for (int r = i; r < j; ++r)
+                if (c0 < rl[r]) {
+                    it_row.push_back(r);
+                    it_c0.push_back(c0);
+                    it_nc.push_back(std::min(kSegCols, rl[r] - c0));
+                }
         i = j;
     }
-    std::stable_sort(shorts.begin(), shorts.end(), [&](int x, int y) { return rl[x] > rl[y]; });
+    std::vector<int> r_ptr(n + 1, 0), r_items(it_row.size());
+    for (int r : it_row) r_ptr[r + 1]++;
+    for (int i = 0; i < n; ++i) r_ptr[i + 1] += r_ptr[i];
+    {
+        std::vector<int> pos(r_ptr.begin(), r_ptr.end() - 1);
+        for (size_t t = 0; t < it_row.size(); ++t) r_items[pos[it_row[t]]++] = (int)t;
+    }
     // x = S^T y schedule: each tile's row list in chunks of kChunkRows rows
     std::vector<int> c_tile, c_p0, c_p1, t_cptr(ntiles_ + 1, 0);
     for (int t = 0; t < ntiles_; ++t) {
@@ -292,9 +296,13 @@ void Engine::build_device(int threads) {
         }
         t_cptr[t + 1] = (int)c_tile.size();
     }
-    d_short_rows.upload(shorts);
-    d_grp_row0.upload(g_row0);
-    d_grp_g.upload(g_g);
+    d_short_rows.upload(it_row);
+    d_grp_row0.upload(it_c0);
+    d_grp_g.upload(it_nc);
+    d_row_item_ptr.upload(r_ptr);
+    d_row_items.upload(r_items);
+    d_ypart64.alloc(std::max<size_t>(1, it_row.size()) * 3 * sizeof(double));
+    d_ypart32.alloc(std::max<size_t>(1, it_row.size()) * 3 * sizeof(float));
     d_chunk_tile.upload(c_tile);
     d_chunk_p0.upload(c_p0);
     d_chunk_p1.upload(c_p1);
@@ -318,11 +326,12 @@ void Engine::build_device(int threads) {
         P.row_off = d_row_off.as<int64_t>();
         P.row_a = d_row_a.as<int>();
         P.row_len = d_row_len.as<int>();
-        P.n_short = (int)shorts.size();
-        P.n_groups = (int)g_row0.size();
-        P.short_rows = d_short_rows.as<int>();
-        P.grp_row0 = d_grp_row0.as<int>();
-        P.grp_g = d_grp_g.as<int>();
+        P.n_items = (int)it_row.size();
+        P.item_row = d_short_rows.as<int>();
+        P.item_c0 = d_grp_row0.as<int>();
+        P.item_nc = d_grp_g.as<int>();
+        P.row_item_ptr = d_row_item_ptr.as<int>();
+        P.row_items = d_row_items.as<int>();
         P.n_chunks = (int)c_tile.size();
         P.ntiles = ntiles_;
         P.chunk_tile = d_chunk_tile.as<int>();
@@ -337,6 +346,8 @@ void Engine::build_device(int threads) {
     fill_plan(plan32_, nullptr);
     plan64_.vals = d_vals64.as<double>();
     plan64_.xpart = d_xpart64.as<double>();
+    plan64_.ypart = d_ypart64.as<double>();
+    plan32_.ypart = d_ypart32.as<float>();
     plan32_.vals = d_vals32.as<float>();
     plan32_.xpart = d_xpart32.as<float>();
     // mesh, samples, constraints
@@ -389,10 +400,11 @@ void Engine::build_device(int threads) {
         b->alloc(ld * sizeof(double));
     d_dG.alloc(ld * kMaxWindow * sizeof(double));
     d_dX.alloc(ld * kMaxWindow * sizeof(double));
-    red_blocks_ = std::max(1, std::min(kRedBlocks, (n3 + 2047) / 2048));
-    d_part_gate.alloc(kRedBlocks * 2 * sizeof(double));
-    d_part_aa.alloc(kRedBlocks * 64 * sizeof(double));
-    d_part_upd.alloc(kRedBlocks * 3 * sizeof(double));
+    red_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256));
+    gather_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n + 255) / 256));
+    d_part_gate.alloc(kMaxRedBlocks * 2 * sizeof(double));
+    d_part_aa.alloc(kMaxRedBlocks * 64 * sizeof(double));
+    d_part_upd.alloc(kMaxRedBlocks * 3 * sizeof(double));
     d_gravf.alloc(3 * sizeof(double));
     d_elem_out64.alloc((size_t)m * k * 3 * sizeof(double));
     d_elem_out32.alloc((size_t)m * k * 3 * sizeof(float));
@@ -427,8 +439,14 @@ void Engine::build_device(int threads) {
         d_dstate_dev.alloc(3 * sizeof(double));
         d_adjnorm.alloc(2 * sizeof(double));
         CUDA_OK(cudaMemset(d_adjnorm.p, 0, 2 * sizeof(double)));
-        d_part_adj.alloc(kRedBlocks * 3 * sizeof(double));
-        for (DeviceBuffer* b : {&d_gq, &d_gv, &d_dq, &d_dv, &d_df}) b->alloc(ld * sizeof(double));
+        d_part_adj.alloc(kMaxRedBlocks * 3 * sizeof(double));
+        for (DeviceBuffer* b : {&d_gq, &d_gv, &d_dq, &d_dv, &d_df, &d_r, &d_pp, &d_wv}) b->alloc(ld * sizeof(double));
+        d_A_rp.upload(A.rp);
+        d_A_ci.upload(A.ci);
+        d_A_v.upload(A.v);
+        Acsr_.rp = d_A_rp.as<int>();
+        Acsr_.ci = d_A_ci.as<int>();
+        Acsr_.v = d_A_v.as<double>();
     }
     drop_graphs();
     device_ready_ = true;
@@ -452,10 +470,17 @@ EnergyPack Engine::energy_pack() const {
     return ep;
 }
 
-void Engine::launch_ainv(bool fp32, cudaStream_t st) {
+void Engine::launch_ainv(bool fp32, cudaStream_t st, const double* x_base) {
     Ctrl* c = d_ctrl.as<Ctrl>();
-    if (fp32) launch_sts<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), d_xraw.as<double>(), c, st);
-    else launch_sts<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), d_xraw.as<double>(), c, st);
+    if (fp32) {
+        SpmvPlan<float> p = plan32_;
+        p.x_base = x_base;
+        launch_sts<float>(p, d_vperm32.as<float>(), d_y32.as<float>(), d_xraw.as<double>(), c, st);
+    } else {
+        SpmvPlan<double> p = plan64_;
+        p.x_base = x_base;
+        launch_sts<double>(p, d_vperm64.as<double>(), d_y64.as<double>(), d_xraw.as<double>(), c, st);
+    }
 }
 
 // One PD iteration: local step, gather to the permuted right-hand side, A^-1 pair, Anderson + gate.
@@ -472,7 +497,7 @@ void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
         launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out32.as<float>(),
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                                 red_blocks_, c, st);
+                                 gather_blocks_, Acsr_, d_x.as<double>(), c, st);
     } else {
         launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
                                 d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
@@ -480,15 +505,16 @@ void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
         launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                                   d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                   d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                                  red_blocks_, c, st);
+                                  gather_blocks_, NodeCsr(), nullptr, c, st);
     }
-    launch_ainv(f32, st);
+    // FP32 S^T S in refinement form: x_raw = x + A~^-1 (b - A x) with the residual in FP64
+    launch_ainv(f32, st, f32 ? d_x.as<double>() : nullptr);
     launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
                      d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
                      d_lx.as<double>(), n3, d_part_aa.as<double>(), red_blocks_, c, st);
     launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
                      d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3, d_part_upd.as<double>(),
-                     d_part_gate.as<double>(), red_blocks_, red_blocks_, c, st);
+                     d_part_gate.as<double>(), gather_blocks_, red_blocks_, c, st);
 }
 
 // One adjoint iteration: K_pd mu, gather of g_bar + K_pd mu, A^-1 pair, Anderson + gate.
@@ -508,6 +534,29 @@ void Engine::enqueue_bwd_iteration(cudaStream_t st) {
                      d_part_gate.as<double>(), 0, red_blocks_, c, st);
 }
 
+// One conjugate-gradient iteration of the adjoint (A - K_pd) mu = g_bar, preconditioned by S^T S.
+void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st) {
+    const int n = M.n, n3 = 3 * n;
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_pp.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
+                    d_elem_out64.as<double>(), c, st);
+    launch_pcg_gather(n, Acsr_, d_pp.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
+                      d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
+                      d_part_gate.as<double>(), gather_blocks_, c, st);
+    if (f32)
+        launch_pcg_update1<float>(n, d_x.as<double>(), d_r.as<double>(), d_pp.as<double>(), d_wv.as<double>(),
+                                  d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm32.as<float>(), npad_,
+                                  d_part_upd.as<double>(), gather_blocks_, c, st);
+    else
+        launch_pcg_update1<double>(n, d_x.as<double>(), d_r.as<double>(), d_pp.as<double>(), d_wv.as<double>(),
+                                   d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_,
+                                   d_part_upd.as<double>(), gather_blocks_, c, st);
+    launch_ainv(f32, st);
+    launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
+                       gather_blocks_, red_blocks_, c, st);
+    launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
+}
+
 // Runs iterations until the device-side gate sets `done`: one iteration is captured once as a CUDA graph and
 // replayed; the control block is read back every few iterations (doubling up to poll_chunk).
 void Engine::run_iterations(int mode, const Options& o, cudaStream_t st) {
@@ -519,6 +568,7 @@ void Engine::run_iterations(int mode, const Options& o, cudaStream_t st) {
         cudaGraph_t graph;
         CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         if (mode == 2) enqueue_bwd_iteration(cap);
+        else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
         else enqueue_fwd_iteration(mode == 1, cap);
         CUDA_OK(cudaStreamEndCapture(cap, &graph));
         CUDA_OK(cudaGraphGetNodes(graph, nullptr, &graph_nodes_[mode]));
@@ -628,7 +678,35 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
         drop_graphs();
         graph_dt_ = h;
     }
-    run_iterations(2, o, st);
+    if (o.bwd_solver == 1) {
+        // r = g_bar, z = A^-1 r, p = z (the first update2 call only records r.z)
+        const bool f32 = o.fp32_bulk != 0;
+        h_ctrl_->pcg_init = 1;
+        CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemsetAsync(d_pp.p, 0, n3 * sizeof(double), st));
+        if (f32)
+            launch_pcg_init<float>(M.n, d_gbar.as<double>(), d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                                   d_r.as<double>(), d_vperm32.as<float>(), npad_, st);
+        else
+            launch_pcg_init<double>(M.n, d_gbar.as<double>(), d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                                    d_r.as<double>(), d_vperm64.as<double>(), npad_, st);
+        launch_ainv(f32, st);
+        launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
+                           gather_blocks_, red_blocks_, c, st);
+        launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
+        launches_ += 8;
+        run_iterations(f32 ? 4 : 3, o, st);
+        if (h_ctrl_->status & kStatusIndefinite) {
+            // negative curvature of (A - K_pd): fall back to the reference fixed point for this step
+            init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
+            CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+            CUDA_OK(cudaMemsetAsync(d_x.p, 0, n3 * sizeof(double), st));
+            run_iterations(2, o, st);
+            stats.bwd_fallbacks++;
+        }
+    } else {
+        run_iterations(2, o, st);
+    }
     stats.last_bwd_iters = h_ctrl_->iter;
     stats.last_filtered = (int)h_ctrl_->arrive[3];
     const int ne = (int)M.energies.size(), np = num_pd_params();
@@ -788,7 +866,7 @@ void Engine::local_step(double dt, const double* q, double* rhs) {
     launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                               d_qt.as<double>(), 0.0, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                               d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                              red_blocks_, d_ctrl.as<Ctrl>(), st);
+                              gather_blocks_, NodeCsr(), nullptr, d_ctrl.as<Ctrl>(), st);
     // the gather leaves pd (node-major) in prev_pd
     CUDA_OK(cudaMemcpyAsync(rhs, d_prev_pd.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(h_ctrl_, d_ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));

@@ -23,6 +23,7 @@ struct Options {
     int bwd_cascade_cap = 1;     // reference cap of the injected adjoint at |g_bar| + 1
     int bwd_eigen_filter = 0;    // 0 off (exact adjoint), 1 clamp, 2 abs
     int fp32_bulk = 0;           // projection and S/S^T SpMVs in FP32
+    int bwd_solver = 0;          // 0: Anderson-accelerated fixed point (reference), 1: preconditioned CG
     int poll_chunk = 8;
     static Options parse(const std::map<std::string, double>& m);
 };
@@ -46,7 +47,7 @@ struct DeviceBuffer {
 
 struct StepStats {
     std::vector<int> frame_iters, frame_converged;
-    int last_bwd_iters = 0, last_filtered = 0;
+    int last_bwd_iters = 0, last_filtered = 0, bwd_fallbacks = 0;
 };
 
 class Engine {
@@ -103,10 +104,12 @@ private:
     void build_device(int threads);
     EnergyPack energy_pack() const;
     void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st);
-    void launch_ainv(bool fp32, cudaStream_t st);  // d_vperm -> d_xraw
+    void launch_ainv(bool fp32, cudaStream_t st, const double* x_base = nullptr);  // d_vperm -> d_xraw
+    void enqueue_pcg_iteration(bool fp32, cudaStream_t st);
     void enqueue_fwd_iteration(bool fp32, cudaStream_t st);
     void enqueue_bwd_iteration(cudaStream_t st);
-    void run_iterations(int mode, const Options& o, cudaStream_t st);  // mode 0 fwd64, 1 fwd32, 2 bwd
+    // mode 0 fwd64, 1 fwd mixed, 2 adjoint fixed point, 3 adjoint PCG (FP64 preconditioner), 4 PCG (FP32 precond.)
+    void run_iterations(int mode, const Options& o, cudaStream_t st);
     void drop_graphs();
     void check_status(const char* where);
 
@@ -114,10 +117,11 @@ private:
     double built_dt_ = -1;
     SFactor S;
     NodeMatrix A;
-    int npad_ = 0, ntiles_ = 0, red_blocks_ = 1;
+    int npad_ = 0, ntiles_ = 0, red_blocks_ = 1, gather_blocks_ = 1;
     double graph_dt_ = -1;
-    cudaGraphExec_t graphs_[3] = {nullptr, nullptr, nullptr};
-    size_t graph_nodes_[3] = {0, 0, 0};
+    cudaGraphExec_t graphs_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t graph_nodes_[5] = {0, 0, 0, 0, 0};
+    NodeCsr Acsr_;
     long long launches_ = 0;
     SpmvPlan<double> plan64_;
     SpmvPlan<float> plan32_;
@@ -128,14 +132,14 @@ private:
     DeviceBuffer d_node_ptr, d_node_inc, d_perm, d_iperm;
     DeviceBuffer d_row_off, d_row_a, d_row_len, d_vals64, d_vals32, d_tile_ptr, d_tile_rows;
     DeviceBuffer d_short_rows, d_grp_row0, d_grp_g, d_chunk_tile, d_chunk_p0, d_chunk_p1, d_tile_chunk_ptr;
-    DeviceBuffer d_xpart64, d_xpart32;
+    DeviceBuffer d_xpart64, d_xpart32, d_ypart64, d_ypart32, d_row_item_ptr, d_row_items;
     DeviceBuffer d_w[kMaxEnergies], d_w32[kMaxEnergies], d_mask[kMaxEnergies];
     DeviceBuffer d_q, d_v, d_f, d_qt, d_x, d_xraw, d_prev_pd, d_dG, d_dX, d_lg, d_lx;
     DeviceBuffer d_part_gate, d_part_aa, d_part_upd, d_gravf;
     DeviceBuffer d_elem_out64, d_elem_out32, d_vperm64, d_vperm32, d_y64, d_y32;
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
-    DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df;
+    DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
                                                          const unsigned char* __restrict__ fixed,
                                                          const int* __restrict__ iperm, T* __restrict__ v, int npad,
                                                          double* __restrict__ prev, double* __restrict__ part,
-                                                         Ctrl* ctrl) {
+                                                         NodeCsr A, const double* __restrict__ q, Ctrl* ctrl) {
     if (ctrl->done) return;
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
@@ -201,13 +201,23 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
         const double p[3] = {p0, p1, p2};
         const int j = iperm[i];
         const bool fx = fixed[i] != 0;
+        double aq[3] = {0.0, 0.0, 0.0};
+        if (A.rp && !fx) {
+            for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+                const int c = A.ci[k];
+                const double a = A.v[k];
+                aq[0] += a * q[3 * c];
+                aq[1] += a * q[3 * c + 1];
+                aq[2] += a * q[3 * c + 2];
+            }
+        }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const double pr = prev[3 * i + d];
             acc[0] += (p[d] - pr) * (p[d] - pr);
             acc[1] += pr * pr;
             prev[3 * i + d] = p[d];
-            v[(size_t)d * npad + j] = fx ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d]);
+            v[(size_t)d * npad + j] = fx ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d] - aq[d]);
         }
     }
     block_sum<2>(acc, sh);
@@ -247,116 +257,76 @@ template <> struct Vec4<double> {
     }
 };
 
-// y = S v, short rows: one warp per row (row length <= kShortRowMax), two 16-byte loads in flight per lane.
+// y = S v, stage 1: one warp per work item (a row segment of <= kSegCols columns), four 16-byte loads of S
+// in flight per lane, v through L1 (the CTA's warps share the segment's columns).
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_spmv_S_short(SpmvPlan<T> p, const T* __restrict__ v,
-                                                           T* __restrict__ y, const Ctrl* ctrl) {
+__global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __restrict__ v, const Ctrl* ctrl) {
     if (ctrl->done) return;
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= p.n_short) return;
-    const int i = __ldg(p.short_rows + w);
-    const int64_t off = __ldg(p.row_off + i);
-    const int a = __ldg(p.row_a + i), len = __ldg(p.row_len + i);
-    const int npad = p.npad;
+    const int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (it >= p.n_items) return;
+    const int i = __ldg(p.item_row + it), c0 = __ldg(p.item_c0 + it), nc = __ldg(p.item_nc + it);
+    const T* __restrict__ sv = p.vals + __ldg(p.row_off + i) + c0;
+    const int a = __ldg(p.row_a + i) + c0;
+    const T* __restrict__ v0 = v + a;
+    const T* __restrict__ v1 = v + p.npad + a;
+    const T* __restrict__ v2 = v + 2 * (size_t)p.npad + a;
     T s0 = T(0), s1 = T(0), s2 = T(0);
-    for (int c = lane * 4; c < len; c += 256) {
-        Vec4<T> sv, v0, v1, v2;
-        sv.load_stream(p.vals + off + c);
-        v0.load(v + a + c);
-        v1.load(v + npad + a + c);
-        v2.load(v + 2 * (size_t)npad + a + c);
-        const int c2 = c + 128;
-        Vec4<T> tv, u0, u1, u2;
-        const bool two = c2 < len;
-        if (two) {
-            tv.load_stream(p.vals + off + c2);
-            u0.load(v + a + c2);
-            u1.load(v + npad + a + c2);
-            u2.load(v + 2 * (size_t)npad + a + c2);
+    int c = lane * 4;
+    for (; c + 384 < nc; c += 512) {
+        Vec4<T> s[4], x0[4], x1[4], x2[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s[u].load_stream(sv + c + 128 * u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            x0[u].load(v0 + c + 128 * u);
+            x1[u].load(v1 + c + 128 * u);
+            x2[u].load(v2 + c + 128 * u);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            s0 += sv.v[q] * v0.v[q];
-            s1 += sv.v[q] * v1.v[q];
-            s2 += sv.v[q] * v2.v[q];
-        }
-        if (two) {
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                s0 += tv.v[q] * u0.v[q];
-                s1 += tv.v[q] * u1.v[q];
-                s2 += tv.v[q] * u2.v[q];
+                s0 += s[u].v[q] * x0[u].v[q];
+                s1 += s[u].v[q] * x1[u].v[q];
+                s2 += s[u].v[q] * x2[u].v[q];
             }
+    }
+    for (; c < nc; c += 128) {
+        Vec4<T> s, x0, x1, x2;
+        s.load_stream(sv + c);
+        x0.load(v0 + c);
+        x1.load(v1 + c);
+        x2.load(v2 + c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            s0 += s.v[q] * x0.v[q];
+            s1 += s.v[q] * x1.v[q];
+            s2 += s.v[q] * x2.v[q];
         }
     }
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
     s2 = warp_sum(s2);
     if (lane == 0) {
-        y[i] = s0;
-        y[npad + i] = s1;
-        y[2 * (size_t)npad + i] = s2;
+        T* o = p.ypart + (size_t)it * 3;
+        o[0] = s0; o[1] = s1; o[2] = s2;
     }
 }
 
-// y = S v, long rows: one CTA (8 warps) per group of g rows that share their first column (members of one
-// nested-dissection separator).  The group's columns stream through shared memory in chunks of
-// kStageCols; each chunk of v is read once and used by all g rows; 8/g warps split a row's chunk.
-constexpr int kStageCols = 1024;
+// y = S v, stage 2: per row, the item partials in item order.
 template <typename T>
-__global__ void __launch_bounds__(256) k_spmv_S_long(SpmvPlan<T> p, const T* __restrict__ v, T* __restrict__ y,
-                                                     const Ctrl* ctrl) {
+__global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __restrict__ y, const Ctrl* ctrl) {
     if (ctrl->done) return;
-    __shared__ __align__(16) T sv[3][kStageCols];
-    __shared__ T red[8][3];
-    const int grp = blockIdx.x;
-    const int row0 = __ldg(p.grp_row0 + grp), g = __ldg(p.grp_g + grp);
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wpr = 8 / g;                       // warps per row
-    const int row = row0 + wid / wpr, sub = wid % wpr;
-    const int a = __ldg(p.row_a + row0);
-    int glen = 0;                                // longest row of the group (the last one)
-    for (int r = 0; r < g; ++r) glen = max(glen, __ldg(p.row_len + row0 + r));
-    const int len = __ldg(p.row_len + row);
-    const int64_t off = __ldg(p.row_off + row);
-    const int npad = p.npad;
-    const int span = kStageCols / wpr;           // columns of one chunk handled by this warp
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
     T s0 = T(0), s1 = T(0), s2 = T(0);
-    for (int c0 = 0; c0 < glen; c0 += kStageCols) {
-        __syncthreads();
-        for (int t = threadIdx.x * 4; t < 3 * kStageCols; t += 256 * 4) {
-            const int d = t / kStageCols, c = t % kStageCols;
-            Vec4<T> x;
-            if (a + c0 + c < npad) x.load(v + (size_t)d * npad + a + c0 + c);
-            else x.v[0] = x.v[1] = x.v[2] = x.v[3] = T(0);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) sv[d][c + q] = x.v[q];
-        }
-        __syncthreads();
-        const int cb = sub * span;
-        for (int c = cb + lane * 4; c < cb + span; c += 128) {
-            if (c0 + c >= len) break;
-            Vec4<T> s;
-            s.load_stream(p.vals + off + c0 + c);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                s0 += s.v[q] * sv[0][c + q];
-                s1 += s.v[q] * sv[1][c + q];
-                s2 += s.v[q] * sv[2][c + q];
-            }
-        }
+    for (int k = __ldg(p.row_item_ptr + i); k < __ldg(p.row_item_ptr + i + 1); ++k) {
+        const T* o = p.ypart + (size_t)__ldg(p.row_items + k) * 3;
+        s0 += o[0]; s1 += o[1]; s2 += o[2];
     }
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    s2 = warp_sum(s2);
-    if (lane == 0) { red[wid][0] = s0; red[wid][1] = s1; red[wid][2] = s2; }
-    __syncthreads();
-    if (threadIdx.x < 3 * g) {
-        const int r = threadIdx.x / 3, d = threadIdx.x % 3;
-        T t = T(0);
-        for (int k = 0; k < wpr; ++k) t += red[r * wpr + k][d];
-        y[(size_t)d * npad + row0 + r] = t;
-    }
+    y[i] = s0;
+    y[p.npad + i] = s1;
+    y[2 * (size_t)p.npad + i] = s2;
 }
 
 // x = S^T y, stage 1: one CTA per (column tile, chunk of the tile's row list); partial tile sums are written
@@ -375,7 +345,35 @@ __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[d][q] = T(0);
     const int pe = __ldg(p.chunk_p1 + ch);
-    for (int pp = __ldg(p.chunk_p0 + ch) + wid; pp < pe; pp += 8) {
+    int pp = __ldg(p.chunk_p0 + ch) + wid;
+    for (; pp + 8 < pe; pp += 16) {
+        const int i0 = __ldg(p.tile_rows + pp), i1 = __ldg(p.tile_rows + pp + 8);
+        const int a0 = __ldg(p.row_a + i0), l0 = __ldg(p.row_len + i0);
+        const int a1 = __ldg(p.row_a + i1), l1 = __ldg(p.row_len + i1);
+        const bool in0 = c >= a0 && c + 4 <= a0 + l0, in1 = c >= a1 && c + 4 <= a1 + l1;
+        Vec4<T> s0, s1;
+        if (in0) s0.load_stream(p.vals + __ldg(p.row_off + i0) + (c - a0));
+        if (in1) s1.load_stream(p.vals + __ldg(p.row_off + i1) + (c - a1));
+        const T y00 = __ldg(y + i0), y01 = __ldg(y + npad + i0), y02 = __ldg(y + 2 * (size_t)npad + i0);
+        const T y10 = __ldg(y + i1), y11 = __ldg(y + npad + i1), y12 = __ldg(y + 2 * (size_t)npad + i1);
+        if (in0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc[0][q] += s0.v[q] * y00;
+                acc[1][q] += s0.v[q] * y01;
+                acc[2][q] += s0.v[q] * y02;
+            }
+        }
+        if (in1) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc[0][q] += s1.v[q] * y10;
+                acc[1][q] += s1.v[q] * y11;
+                acc[2][q] += s1.v[q] * y12;
+            }
+        }
+    }
+    for (; pp < pe; pp += 8) {
         const int i = __ldg(p.tile_rows + pp);
         const int a = __ldg(p.row_a + i), len = __ldg(p.row_len + i);
         if (c >= a && c + 4 <= a + len) {
@@ -418,7 +416,8 @@ __global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double*
     double s = 0.0;
     for (int ch = __ldg(p.tile_chunk_ptr + tile); ch < __ldg(p.tile_chunk_ptr + tile + 1); ++ch)
         s += (double)p.xpart[(size_t)ch * 3 * kTileCols + r];
-    x_out[3 * (size_t)__ldg(p.perm + j) + d] = s;
+    const size_t o = 3 * (size_t)__ldg(p.perm + j) + d;
+    x_out[o] = p.x_base ? p.x_base[o] + s : s;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -909,6 +908,147 @@ __global__ void __launch_bounds__(128) k_param_grad(int m, const int* __restrict
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Conjugate-gradient adjoint
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const double* __restrict__ p,
+                                                         const int* __restrict__ node_ptr,
+                                                         const int* __restrict__ node_inc,
+                                                         const double* __restrict__ eo,
+                                                         const unsigned char* __restrict__ fixed,
+                                                         double* __restrict__ w, double* __restrict__ part,
+                                                         Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (fixed[i]) {
+            w[3 * i] = w[3 * i + 1] = w[3 * i + 2] = 0.0;
+            continue;
+        }
+        double a0 = 0, a1 = 0, a2 = 0;
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+            const int c = A.ci[k];
+            const double a = A.v[k];
+            a0 += a * p[3 * c];
+            a1 += a * p[3 * c + 1];
+            a2 += a * p[3 * c + 2];
+        }
+        for (int idx = node_ptr[i]; idx < node_ptr[i + 1]; ++idx) {
+            const double* c = eo + (size_t)node_inc[idx] * 3;
+            a0 -= c[0]; a1 -= c[1]; a2 -= c[2];
+        }
+        w[3 * i] = a0; w[3 * i + 1] = a1; w[3 * i + 2] = a2;
+        acc[0] += a0 * p[3 * i] + a1 * p[3 * i + 1] + a2 * p[3 * i + 2];
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+    if (!arrive_last(&ctrl->arrive[2])) return;
+    double t[1];
+    sum_partials<1>(part, gridDim.x, t, sh);
+    if (threadIdx.x != 0) return;
+    ctrl->arrive[2] = 0;
+    const double pw = t[0];
+    if (!(pw > 0.0) || !(pw < 1e300)) {
+        ctrl->status |= kStatusIndefinite;
+        ctrl->done = 1;
+        ctrl->alpha = 0.0;
+        return;
+    }
+    ctrl->alpha = ctrl->rz / pw;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pcg_update1(int n, double* __restrict__ mu, double* __restrict__ r,
+                                                          const double* __restrict__ p, const double* __restrict__ w,
+                                                          const unsigned char* __restrict__ fixed,
+                                                          const int* __restrict__ iperm, T* __restrict__ v, int npad,
+                                                          double* __restrict__ part, Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ double sh[32];
+    const double alpha = ctrl->alpha;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int j = iperm[i];
+        const bool fx = fixed[i] != 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int k = 3 * i + d;
+            const double m = mu[k] + alpha * p[k];
+            const double rr = r[k] - alpha * w[k];
+            mu[k] = m;
+            r[k] = rr;
+            acc[0] += m * m;
+            v[(size_t)d * npad + j] = fx ? T(0) : (T)rr;
+        }
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+}
+
+__global__ void __launch_bounds__(kThreads) k_pcg_update2(int n3, const double* __restrict__ r,
+                                                          const double* __restrict__ z, double* __restrict__ part,
+                                                          const double* __restrict__ mu_part, int mu_blocks,
+                                                          Ctrl* ctrl) {
+    if (ctrl->done) return;
+    __shared__ double sh[2 * 32];
+    double acc[2] = {0.0, 0.0};
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x) {
+        acc[0] += r[k] * z[k];
+        acc[1] += z[k] * z[k];
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2] = acc[0];
+        part[blockIdx.x * 2 + 1] = acc[1];
+    }
+    if (!arrive_last(&ctrl->arrive[1])) return;
+    double t[2], mu2[1] = {0.0};
+    sum_partials<2>(part, gridDim.x, t, sh);
+    if (!ctrl->pcg_init) sum_partials<1>(mu_part, mu_blocks, mu2, sh);
+    if (threadIdx.x != 0) return;
+    ctrl->arrive[1] = 0;
+    const double rz = t[0], zn = sqrt(t[1]), mun = sqrt(mu2[0]);
+    if (ctrl->pcg_init) {
+        ctrl->pcg_init = 0;
+        ctrl->beta = 0.0;
+        ctrl->rz = rz;
+        return;
+    }
+    ctrl->beta = ctrl->rz > 0 ? rz / ctrl->rz : 0.0;
+    ctrl->rz = rz;
+    ctrl->err = zn;
+    ctrl->rn = mun;
+    const int it = ctrl->iter;
+    const bool conv = it > 0 && zn < ctrl->rel_tol * mun + ctrl->abs_tol;
+    if (!(zn == zn) || !(mun == mun)) ctrl->status |= kStatusNonFinite | kStatusDiverged;
+    else if (ctrl->clip > 0 && mun > ctrl->clip) ctrl->status |= kStatusDiverged;
+    ctrl->iter = it + 1;
+    if (conv) ctrl->converged = 1;
+    if (conv || ctrl->iter >= ctrl->max_iter || (ctrl->status & (kStatusNonFinite | kStatusDiverged)))
+        ctrl->done = 1;
+}
+
+__global__ void k_pcg_p(int n3, double* __restrict__ p, const double* __restrict__ z, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const double beta = ctrl->beta;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x) p[k] = z[k] + beta * p[k];
+}
+
+template <typename T>
+__global__ void k_pcg_init(int n, const double* __restrict__ gbar, const unsigned char* __restrict__ fixed,
+                           const int* __restrict__ iperm, double* __restrict__ r, T* __restrict__ v, int npad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool fx = fixed[i] != 0;
+    const int j = iperm[i];
+    for (int d = 0; d < 3; ++d) {
+        const double g = fx ? 0.0 : gbar[3 * i + d];
+        r[3 * i + d] = g;
+        v[(size_t)d * npad + j] = (T)g;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) k_adj_prepare(int n3, const double* __restrict__ gq,
                                                           const double* __restrict__ gv, double inv_h,
                                                           double* __restrict__ gbar, double* __restrict__ dq,
@@ -1028,15 +1168,16 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
 template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
-                       double* prev_pd, double* part, int blocks, Ctrl* ctrl, cudaStream_t st) {
+                       double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, Ctrl* ctrl,
+                       cudaStream_t st) {
     k_gather_fwd<T><<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
-                                                     v_perm, npad, prev_pd, part, ctrl);
+                                                     v_perm, npad, prev_pd, part, A, q, ctrl);
 }
 
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
-    if (p.n_groups) k_spmv_S_long<T><<<p.n_groups, 256, 0, st>>>(p, v, y, ctrl);
-    if (p.n_short) k_spmv_S_short<T><<<blocks_for((long long)p.n_short * 32, kThreads), kThreads, 0, st>>>(p, v, y, ctrl);
+    k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
+    k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
     k_spmv_ST_part<T><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
     k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
 }
@@ -1102,11 +1243,43 @@ template void launch_elem_fwd<double>(int, int, int, const int*, const double*, 
 template void launch_elem_fwd<float>(int, int, int, const int*, const double*, const double*, const unsigned char*,
                                      const double*, int, double, const EnergyPack&, float*, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<double>(int, const int*, const int*, const double*, const double*, double,
-                                        const unsigned char*, const int*, double*, int, double*, double*, int, Ctrl*,
-                                        cudaStream_t);
+                                        const unsigned char*, const int*, double*, int, double*, double*, int, NodeCsr,
+                                        const double*, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<float>(int, const int*, const int*, const float*, const double*, double,
-                                       const unsigned char*, const int*, float*, int, double*, double*, int, Ctrl*,
-                                       cudaStream_t);
+                                       const unsigned char*, const int*, float*, int, double*, double*, int, NodeCsr,
+                                       const double*, Ctrl*, cudaStream_t);
+
+void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
+                       const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
+                       Ctrl* ctrl, cudaStream_t st) {
+    k_pcg_gather<<<blocks, kThreads, 0, st>>>(n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl);
+}
+template <typename T>
+void launch_pcg_update1(int n, double* mu, double* r, const double* p, const double* w,
+                        const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad, double* part,
+                        int blocks, Ctrl* ctrl, cudaStream_t st) {
+    k_pcg_update1<T><<<blocks, kThreads, 0, st>>>(n, mu, r, p, w, fixed_node, iperm, v_perm, npad, part, ctrl);
+}
+void launch_pcg_update2(int n3, const double* r, const double* z, double* part, const double* mu_part, int mu_blocks,
+                        int blocks, Ctrl* ctrl, cudaStream_t st) {
+    k_pcg_update2<<<blocks, kThreads, 0, st>>>(n3, r, z, part, mu_part, mu_blocks, ctrl);
+}
+void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st) {
+    k_pcg_p<<<std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st>>>(n3, p, z, ctrl);
+}
+template <typename T>
+void launch_pcg_init(int n, const double* gbar, const unsigned char* fixed_node, const int* iperm, double* r,
+                     T* v_perm, int npad, cudaStream_t st) {
+    k_pcg_init<T><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, gbar, fixed_node, iperm, r, v_perm, npad);
+}
+template void launch_pcg_update1<double>(int, double*, double*, const double*, const double*, const unsigned char*,
+                                         const int*, double*, int, double*, int, Ctrl*, cudaStream_t);
+template void launch_pcg_update1<float>(int, double*, double*, const double*, const double*, const unsigned char*,
+                                        const int*, float*, int, double*, int, Ctrl*, cudaStream_t);
+template void launch_pcg_init<double>(int, const double*, const unsigned char*, const int*, double*, double*, int,
+                                      cudaStream_t);
+template void launch_pcg_init<float>(int, const double*, const unsigned char*, const int*, double*, float*, int,
+                                     cudaStream_t);
 void launch_adj_prepare(int n3, const double* gq, const double* gv, double inv_h, double* gbar, double* dq,
                         double* part, double* norm_out, cudaStream_t st) {
     // norm_out[1] doubles as the arrival counter of this kernel (zeroed by the caller)

@@ -10,7 +10,8 @@ namespace dphd {
 constexpr int kMaxEnergies = 4;
 constexpr int kMaxWindow = 8;
 constexpr int kTileCols = 128;       // S^T column tile width (32 lanes x 4 columns)
-constexpr int kRedBlocks = 296;      // fixed grid of the reduction kernels (2 x 148 SMs)
+constexpr int kRedBlocks = 296;      // grid of the small adjoint reductions (2 x 148 SMs)
+constexpr int kMaxRedBlocks = 1184;  // upper bound of the per-iteration reduction grids (8 x 148 SMs)
 constexpr int kAaSlots = 24;         // per-block partial slots of the AA reduction
 
 // Status bits written by kernels (never a trap).
@@ -18,6 +19,7 @@ enum StatusBits : int {
     kStatusSingularF = 1,        // volume projection met sig_min < eps
     kStatusNonFinite = 2,        // NaN/Inf in an iterate
     kStatusDiverged = 4,         // adjoint iterate exceeded the clip norm
+    kStatusIndefinite = 8,       // conjugate-gradient curvature p^T (A - K) p <= 0
 };
 
 // Device-resident control block of one fixed-point solve (forward PD loop or backbone adjoint).
@@ -28,6 +30,8 @@ struct Ctrl {
     double rel_tol, abs_tol, clip;
     double gamma[kMaxWindow];
     double dq, rn, pdc, pdr, err, xn;    // last gate quantities
+    double rz, alpha, beta;              // conjugate-gradient scalars of the adjoint solve
+    int pcg_init;
     unsigned int arrive[4];
 };
 
@@ -44,10 +48,17 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
                      cudaStream_t st);
 // Per-node gather of element contributions: b = inv_h2m q_tilde + pd (Dirichlet rows zero), written to the
 // permuted SoA right-hand side; pd kept node-major with the gate partial norms.
+// When A_rp is non-null the residual form is written instead: v = b - A q (refinement of an inexact A^-1).
+struct NodeCsr {
+    const int* rp = nullptr;
+    const int* ci = nullptr;
+    const double* v = nullptr;
+};
 template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
-                       double* prev_pd, double* part, int blocks, Ctrl* ctrl, cudaStream_t st);
+                       double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, Ctrl* ctrl,
+                       cudaStream_t st);
 // Sparse-inverse SpMV pair x = S^T (S v) (3 right-hand sides, permuted SoA v and y, x node-major FP64).
 // S row i: row_len[i] values from column row_a[i] (both multiples of 4) at vals[row_off[i]].
 template <typename T>
@@ -57,11 +68,17 @@ struct SpmvPlan {
     const int* row_a = nullptr;
     const int* row_len = nullptr;
     const T* vals = nullptr;
-    // y = S v: short rows one warp each, long rows in groups of g in {1,2,4,8} rows sharing row_a, one CTA each
-    int n_short = 0, n_groups = 0;
-    const int* short_rows = nullptr;
-    const int* grp_row0 = nullptr;
-    const int* grp_g = nullptr;
+    // y = S v: work items (row, first column, column count) of at most kSegCols columns, one warp each;
+    // items of the same nested-dissection separator and column segment are adjacent so that the warps of
+    // one CTA read the same slice of v (L1 reuse).  Partial sums ypart[item][3] are summed per row in item
+    // order by the fix-up kernel (rows own items [row_item_ptr[r], row_item_ptr[r+1]) via row_items).
+    int n_items = 0;
+    const int* item_row = nullptr;
+    const int* item_c0 = nullptr;
+    const int* item_nc = nullptr;
+    const int* row_item_ptr = nullptr;
+    const int* row_items = nullptr;
+    T* ypart = nullptr;
     // x = S^T y: column tiles of kTileCols, each tile's row list split into chunks (one CTA each)
     int n_chunks = 0, ntiles = 0;
     const int* chunk_tile = nullptr;
@@ -71,9 +88,10 @@ struct SpmvPlan {
     const int* tile_chunk_ptr = nullptr;
     T* xpart = nullptr;
     const int* perm = nullptr;
+    const double* x_base = nullptr;  // when set, x_out = x_base + S^T S v (refinement form)
 };
-constexpr int kShortRowMax = 1024;   // rows up to this length are handled by one warp
-constexpr int kChunkRows = 128;      // rows per S^T chunk CTA
+constexpr int kSegCols = 2048;       // columns per S v work item
+constexpr int kChunkRows = 64;       // rows per S^T chunk CTA
 
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
@@ -108,6 +126,25 @@ void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const do
 void launch_param_grad(int m, int k, int s, const int* E, const double* q, const double* mu, const double* grad,
                        int hex, double vol_over_s, const EnergyPack& ep, double* gw /* [energies][m] */,
                        double* gmat /* [energies][m] */, double* gnh /* [energies][m][2] */, cudaStream_t st);
+
+// Preconditioned conjugate gradients for the adjoint (A - K_pd) mu = g_bar on the free DoFs, preconditioner
+// A^-1 = S^T S.  Kernels of one iteration, in order: K p (launch_kpd_elem), w = (A - K) p and alpha,
+// mu += alpha p / r -= alpha w (also the permuted right-hand side of the preconditioner), S^T S, r.z and the
+// stop rule |z| < rtol |mu| + atol, p = z + beta p.
+void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
+                       const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
+                       Ctrl* ctrl, cudaStream_t st);
+template <typename T>
+void launch_pcg_update1(int n, double* mu, double* r, const double* p, const double* w,
+                        const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad, double* part,
+                        int blocks, Ctrl* ctrl, cudaStream_t st);
+void launch_pcg_update2(int n3, const double* r, const double* z, double* part, const double* mu_part, int mu_blocks,
+                        int blocks, Ctrl* ctrl, cudaStream_t st);
+void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st);
+// r = g_bar on free DoFs (0 on Dirichlet), permuted right-hand side for the first preconditioner apply.
+template <typename T>
+void launch_pcg_init(int n, const double* gbar, const unsigned char* fixed_node, const int* iperm, double* r,
+                     T* v_perm, int npad, cudaStream_t st);
 
 // Device-side adjoint routing (backward_gpu.cpp:881-917) and parameter-gradient reductions.
 // g_bar = dl_dq_next + dl_dv_next / h;  dl_dq = -dl_dv_next / h;  |g_bar| into norm_out[0].

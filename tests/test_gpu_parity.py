@@ -200,3 +200,39 @@ def test_device_entry_points_match_host_entry_points():
     assert np.array_equal(dq.cpu().numpy(), ref["dl_dq"])
     assert np.array_equal(dpar.cpu().numpy(), ref["dl_dparams"])
     assert d.kernel_launches() > 0
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_pcg_adjoint_matches_converged_oracle_adjoint(fp32):
+    """The conjugate-gradient adjoint (FP64 residual against A, S^T S preconditioner in FP64 or FP32) reaches
+    the converged adjoint of the oracle to 1e-7."""
+    sc = scenes.nh_tet_block(cells=(6, 3, 3), dx=0.01, steps=2)
+    opts = dict(sc.options)
+    opts.update(aa_window=0, rel_tol=1e-13, abs_tol=1e-16, max_pd_iter=20000)
+    o = oracle.OracleDeformable.from_scene(sc)
+    q, v, _, qs, vs = oracle.rollout(o, sc, steps=2, options=opts, record=True)
+    rng = np.random.default_rng(8)
+    gq, gv = rng.standard_normal(sc.dofs), rng.standard_normal(sc.dofs) * 0.1
+    ref = o.backward(qs[1], vs[1], sc.f_ext, sc.dt, qs[2], gq, gv, opts)
+    d = core.from_scene(sc)
+    gopts = dict(opts, alg_phd_bwd_solver=1, fp32_bulk=fp32, rel_tol=1e-12, max_pd_iter=2000)
+    out = d.backward("pd_eigen_alg_phd", qs[1], vs[1], [], sc.f_ext, sc.dt, qs[2], vs[2], [], gq, gv, gopts)
+    assert out["iters"] < 2000
+    for key in ("dl_dq", "dl_dv", "dl_df_ext"):
+        assert _rel(out[key], ref[key]) < 1e-7, key
+    assert _rel(out["dl_dparams"], np.concatenate(ref["dl_dparams"])) < 1e-6
+
+
+def test_mixed_precision_forward_error_vs_fp64():
+    """FP32 projection and FP32 S^T S in refinement form (FP64 residual against A) stay within 1e-6 of the FP64
+    oracle positions after a short rollout at a tight gate."""
+    sc = scenes.nh_tet_block(cells=(8, 4, 4), dx=0.01, steps=5)
+    opts = dict(sc.options)
+    opts.update(aa_window=0, rel_tol=1e-9, abs_tol=1e-12, max_pd_iter=5000)
+    o = oracle.OracleDeformable.from_scene(sc)
+    q_ref, _, _ = oracle.rollout(o, sc, steps=5, options=opts)
+    d = core.from_scene(sc)
+    qs, _ = _rollout_gpu(d, sc, 5, dict(opts, fp32_bulk=1, rel_tol=1e-7))
+    disp = np.abs(q_ref - sc.q0).max()
+    assert np.abs(qs[-1] - q_ref).max() <= 1e-4 * disp
+    assert np.abs(qs[-1] - q_ref).max() <= 1e-6 * np.abs(q_ref).max()
