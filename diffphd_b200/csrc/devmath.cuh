@@ -46,7 +46,7 @@ __device__ __forceinline__ void jacobi_rotate_cols(T* B, T* V, int p, int q) {
     const T alpha = M3(B, 0, p) * M3(B, 0, p) + M3(B, 1, p) * M3(B, 1, p) + M3(B, 2, p) * M3(B, 2, p);
     const T beta = M3(B, 0, q) * M3(B, 0, q) + M3(B, 1, q) * M3(B, 1, q) + M3(B, 2, q) * M3(B, 2, q);
     const T gamma = M3(B, 0, p) * M3(B, 0, q) + M3(B, 1, p) * M3(B, 1, q) + M3(B, 2, p) * M3(B, 2, q);
-    if (gamma == T(0) || dabs(gamma) <= Eps<T>::v * dsqrt(alpha * beta)) return;
+    if (gamma == T(0) || dabs(gamma) <= T(4) * Eps<T>::v * dsqrt(alpha * beta)) return;
     const T zeta = (beta - alpha) / (T(2) * gamma);
     const T t = (zeta >= T(0) ? T(1) : T(-1)) / (dabs(zeta) + dsqrt(T(1) + zeta * zeta));
     const T c = T(1) / dsqrt(T(1) + t * t);
@@ -71,7 +71,7 @@ __device__ __forceinline__ bool cols_orthogonal(const T* B) {
         const T a = M3(B, 0, p) * M3(B, 0, p) + M3(B, 1, p) * M3(B, 1, p) + M3(B, 2, p) * M3(B, 2, p);
         const T b = M3(B, 0, q) * M3(B, 0, q) + M3(B, 1, q) * M3(B, 1, q) + M3(B, 2, q) * M3(B, 2, q);
         const T g = M3(B, 0, p) * M3(B, 0, q) + M3(B, 1, p) * M3(B, 1, q) + M3(B, 2, p) * M3(B, 2, q);
-        ok = ok && (g == T(0) || dabs(g) <= Eps<T>::v * dsqrt(a * b));
+        ok = ok && (g == T(0) || dabs(g) <= T(4) * Eps<T>::v * dsqrt(a * b));
     }
     return ok;
 }
@@ -208,7 +208,8 @@ __device__ __forceinline__ void nh_hessian(T mu, T la, T k, const T* s, T* H) {
 }
 template <typename T>
 __device__ void nh_prox(T mu, T la, T k, const T* sF, T* s) {
-    const T sig_min = T(1e-4), tol = T(1e-10);
+    // FP64: the reference's tolerances.  FP32: the step test at 1e-6 (1e-10 is below FP32 resolution).
+    const T sig_min = T(1e-4), tol = sizeof(T) == 4 ? T(1e-6) : T(1e-10);
 #pragma unroll
     for (int i = 0; i < 3; ++i) s[i] = sF[i] < sig_min ? sig_min : sF[i];
     for (int it = 0; it < 32; ++it) {
@@ -299,6 +300,26 @@ __device__ __forceinline__ bool project(int type, T mu, T la, T k, const T* U, c
     nh_prox(mu, la, k, sig, s);
     usvt(U, s, V, P);
     return true;
+}
+
+// Bp(F) - F = U diag(s* - sig) V^T, evaluated without cancellation against F (used by the FP32 path, which
+// keeps the linear part F - F_bound in FP64).
+template <typename T>
+__device__ __forceinline__ bool project_delta(int type, T mu, T la, T k, const T* U, const T* sig, const T* V, T* D) {
+    T d[3];
+    bool ok = true;
+    if (type == 0) {
+        d[0] = T(1) - sig[0]; d[1] = T(1) - sig[1]; d[2] = T(1) - sig[2];
+    } else if (type == 1) {
+        ok = volume_D(sig, d);
+        if (!ok) d[0] = d[1] = d[2] = T(0);
+    } else {
+        T s[3];
+        nh_prox(mu, la, k, sig, s);
+        d[0] = s[0] - sig[0]; d[1] = s[1] - sig[1]; d[2] = s[2] - sig[2];
+    }
+    usvt(U, d, V, D);
+    return ok;
 }
 
 // Directional derivative of Bp along dF (corotated: dR from the 3x3 system of geometry.cpp:60-80;

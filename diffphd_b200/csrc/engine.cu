@@ -493,8 +493,8 @@ void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
     if (f32) {
         launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
                                d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
-                               d_elem_out32.as<float>(), c, st);
-        launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out32.as<float>(),
+                               d_elem_out64.as<double>(), c, st);
+        launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
                                  gather_blocks_, Acsr_, d_x.as<double>(), c, st);

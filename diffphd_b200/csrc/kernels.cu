@@ -107,51 +107,59 @@ __device__ __forceinline__ void def_grad(const int* __restrict__ E, int e, const
 // Forward local step (deformable_projective_dynamics_forward.cpp:186-292), one thread per (element, sample);
 // for hexes the 8 samples of an element are 8 consecutive lanes and are summed by a shuffle butterfly.
 // ------------------------------------------------------------------------------------------------
+// FP64: P = sum_en w (Bp - F_bound), the reference's expression.  FP32 (mixed precision): the SVD and the
+// projections run in FP32 on F, but only their small correction Bp - F = U diag(s* - sig) V^T is rounded to
+// FP32; P = sum_en w ((F - F_bound) in FP64 + (Bp - F) in FP32).  Node contributions are accumulated in FP64.
 template <typename T, int K, int S>
 __global__ void __launch_bounds__(kThreads) k_elem_fwd(int m, const int* __restrict__ E, const double* __restrict__ q,
                                                        const double* __restrict__ qb,
                                                        const unsigned char* __restrict__ elem_dir,
                                                        const double* __restrict__ grad, double vol_over_s,
-                                                       EnergyPack ep, T* __restrict__ out, Ctrl* ctrl) {
+                                                       EnergyPack ep, double* __restrict__ out, Ctrl* ctrl) {
     if (ctrl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = t / S, smp = t % S;
     const bool valid = e < m;
-    T acc[K][3];
+    double acc[K][3];
 #pragma unroll
-    for (int a = 0; a < K; ++a) acc[a][0] = acc[a][1] = acc[a][2] = T(0);
+    for (int a = 0; a < K; ++a) acc[a][0] = acc[a][1] = acc[a][2] = 0.0;
     if (valid) {
         const double* g = (S == 8) ? grad + smp * 24 : grad + (size_t)e * 12;
-        double Fd[9];
+        double Fd[9], Fbd[9];
         def_grad<K>(E, e, q, g, Fd);
-        T F[9], Fb[9];
+        if (elem_dir[e]) def_grad<K>(E, e, qb, g, Fbd);
+        else {
 #pragma unroll
-        for (int i = 0; i < 9; ++i) { F[i] = (T)Fd[i]; Fb[i] = T(0); }
-        if (elem_dir[e]) {
-            double Fbd[9];
-            def_grad<K>(E, e, qb, g, Fbd);
-#pragma unroll
-            for (int i = 0; i < 9; ++i) Fb[i] = (T)Fbd[i];
+            for (int i = 0; i < 9; ++i) Fbd[i] = 0.0;
         }
+        T F[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) F[i] = (T)Fd[i];
         T U[9], V[9], sig[3];
         svd3<T>(F, U, sig, V);
-        T P[9];
+        double P[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) P[i] = T(0);
+        for (int i = 0; i < 9; ++i) P[i] = 0.0;
         bool ok = true;
         for (int k = 0; k < ep.count; ++k) {
             const ElemEnergyDev& en = ep.en[k];
             if (en.mask && !en.mask[e]) continue;
-            const T w = ld_weight<T>(en, e) * (T)vol_over_s;
+            const double w = ld_weight<double>(en, e) * vol_over_s;
             T Bp[9];
-            ok = project<T>(en.type, (T)en.mu, (T)en.la, (T)en.w_mean, U, sig, V, Bp) && ok;
+            if (sizeof(T) == 8) {
+                ok = project<T>(en.type, (T)en.mu, (T)en.la, (T)en.w_mean, U, sig, V, Bp) && ok;
 #pragma unroll
-            for (int i = 0; i < 9; ++i) P[i] += w * (Bp[i] - Fb[i]);
+                for (int i = 0; i < 9; ++i) P[i] += w * ((double)Bp[i] - Fbd[i]);
+            } else {
+                ok = project_delta<T>(en.type, (T)en.mu, (T)en.la, (T)en.w_mean, U, sig, V, Bp) && ok;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) P[i] += w * ((Fd[i] - Fbd[i]) + (double)Bp[i]);
+            }
         }
         if (!ok) atomicOr(&ctrl->status, (int)kStatusSingularF);
 #pragma unroll
         for (int a = 0; a < K; ++a) {
-            const T g0 = (T)__ldg(g + a * 3), g1 = (T)__ldg(g + a * 3 + 1), g2 = (T)__ldg(g + a * 3 + 2);
+            const double g0 = __ldg(g + a * 3), g1 = __ldg(g + a * 3 + 1), g2 = __ldg(g + a * 3 + 2);
 #pragma unroll
             for (int i = 0; i < 3; ++i) acc[a][i] = P[i] * g0 + P[i + 3] * g1 + P[i + 6] * g2;
         }
@@ -167,14 +175,14 @@ __global__ void __launch_bounds__(kThreads) k_elem_fwd(int m, const int* __restr
 #pragma unroll
             for (int a = 0; a < K; ++a)
                 if (a == smp) {
-                    T* o = out + ((size_t)e * K + a) * 3;
+                    double* o = out + ((size_t)e * K + a) * 3;
                     o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
                 }
         }
     } else if (valid) {
 #pragma unroll
         for (int a = 0; a < K; ++a) {
-            T* o = out + ((size_t)e * K + a) * 3;
+            double* o = out + ((size_t)e * K + a) * 3;
             o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
         }
     }
@@ -182,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) k_elem_fwd(int m, const int* __restr
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __restrict__ node_ptr,
-                                                         const int* __restrict__ node_inc, const T* __restrict__ eo,
+                                                         const int* __restrict__ node_inc, const double* __restrict__ eo,
                                                          const double* __restrict__ qt, double inv_h2m,
                                                          const unsigned char* __restrict__ fixed,
                                                          const int* __restrict__ iperm, T* __restrict__ v, int npad,
@@ -195,8 +203,8 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
         double p0 = 0, p1 = 0, p2 = 0;
         const int b = node_ptr[i], e = node_ptr[i + 1];
         for (int idx = b; idx < e; ++idx) {
-            const T* c = eo + (size_t)node_inc[idx] * 3;
-            p0 += (double)c[0]; p1 += (double)c[1]; p2 += (double)c[2];
+            const double* c = eo + (size_t)node_inc[idx] * 3;
+            p0 += c[0]; p1 += c[1]; p2 += c[2];
         }
         const double p[3] = {p0, p1, p2};
         const int j = iperm[i];
@@ -426,10 +434,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double*
 // `head`.  k_aa_reduce pushes the new entry, forms the Gram system and solves it in the last block;
 // k_aa_update applies the extrapolation, re-imposes Dirichlet values and evaluates the stop rule.
 // ------------------------------------------------------------------------------------------------
-constexpr int kTri = kMaxWindow * (kMaxWindow + 1) / 2;
-constexpr int kAaVals = kTri + kMaxWindow + 2;
-
-__device__ __forceinline__ int tri_idx(int i, int j) { return j * (j + 1) / 2 + i; }  // i <= j
+constexpr int kAaVals = 2 * kMaxWindow + 2;  // new Gram column, right-hand side, |g|^2, |x_raw|^2
 
 __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __restrict__ x,
                                                         const double* __restrict__ xr,
@@ -441,7 +446,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
     if (ctrl->done) return;
     __shared__ double sh[kAaVals * 32];
     const int W = ctrl->window, count = ctrl->count, head = ctrl->head, mode = ctrl->mode;
-    const int m = W > 0 ? count : 0;
+    const int m = W > 0 ? count : 0;  // differences after this push (the newest is j = m - 1)
     double acc[kAaVals];
 #pragma unroll
     for (int i = 0; i < kAaVals; ++i) acc[i] = 0.0;
@@ -451,22 +456,22 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
         if (fixed[r]) xv = mode == 0 ? fval[r] : 0.0;
         const double g = xv - xp;
         if (W > 0) {
+            double gnew = 0.0;
             if (count >= 1) {
                 const int s = (head + count - 1) % W;
-                dG[(size_t)s * ld + r] = g - lg[r];
+                gnew = g - lg[r];
+                dG[(size_t)s * ld + r] = gnew;
                 dX[(size_t)s * ld + r] = xp - lx[r];
             }
             lg[r] = g;
             lx[r] = xp;
-            double dg[kMaxWindow];
 #pragma unroll
-            for (int j = 0; j < kMaxWindow; ++j) dg[j] = j < m ? dG[(size_t)((head + j) % W) * ld + r] : 0.0;
-#pragma unroll
-            for (int j = 0; j < kMaxWindow; ++j) {
-#pragma unroll
-                for (int i = 0; i <= j; ++i) acc[tri_idx(i, j)] += dg[i] * dg[j];
-                acc[kTri + j] += dg[j] * g;
-            }
+            for (int j = 0; j < kMaxWindow; ++j)
+                if (j < m) {
+                    const double dgj = (j == m - 1) ? gnew : dG[(size_t)((head + j) % W) * ld + r];
+                    acc[j] += gnew * dgj;
+                    acc[kMaxWindow + j] += dgj * g;
+                }
         }
         acc[kAaVals - 2] += g * g;
         acc[kAaVals - 1] += xv * xv;
@@ -491,15 +496,22 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
         return;
     }
     if (m < 1) return;
-    // Gram system (dG^T dG + reg I) gamma = dG^T g, reg = max(1e-6 |dG|_F^2 / m, 1e-12); Cholesky solve.
+    // extend the stored Gram matrix by the new difference's column
+    const int snew = (head + m - 1) % W;
+    for (int j = 0; j < m; ++j) {
+        const int sj = (head + j) % W;
+        ctrl->gram[snew][sj] = tot[j];
+        ctrl->gram[sj][snew] = tot[j];
+    }
+    // (dG^T dG + reg I) gamma = dG^T g, reg = max(1e-6 |dG|_F^2 / m, 1e-12); Cholesky solve.
     double A[kMaxWindow * kMaxWindow], b[kMaxWindow];
     double fro = 0;
-    for (int j = 0; j < m; ++j) fro += tot[tri_idx(j, j)];
+    for (int j = 0; j < m; ++j) fro += ctrl->gram[(head + j) % W][(head + j) % W];
     const double reg = fmax(1e-6 * fro / m, 1e-12);
     for (int i = 0; i < m; ++i) {
-        for (int j = 0; j < m; ++j) A[i * m + j] = tot[i <= j ? tri_idx(i, j) : tri_idx(j, i)];
+        for (int j = 0; j < m; ++j) A[i * m + j] = ctrl->gram[(head + i) % W][(head + j) % W];
         A[i * m + i] += reg;
-        b[i] = tot[kTri + i];
+        b[i] = tot[kMaxWindow + i];
     }
     for (int j = 0; j < m; ++j) {
         double d = A[j * m + j];
@@ -1158,7 +1170,7 @@ inline int blocks_for(long long work, int threads) { return (int)((work + thread
 // ------------------------------------------------------------------------------------------------
 template <typename T>
 void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const double* qb, const unsigned char* elem_dir,
-                     const double* grad, int hex, double vol_over_s, const EnergyPack& ep, T* elem_out, Ctrl* ctrl,
+                     const double* grad, int hex, double vol_over_s, const EnergyPack& ep, double* elem_out, Ctrl* ctrl,
                      cudaStream_t st) {
     const int grid = blocks_for((long long)m * s, kThreads);
     if (hex) k_elem_fwd<T, 8, 8><<<grid, kThreads, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
@@ -1166,7 +1178,7 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
 }
 
 template <typename T>
-void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
+void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
                        double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, Ctrl* ctrl,
                        cudaStream_t st) {
@@ -1241,11 +1253,11 @@ void launch_param_grad(int m, int k, int s, const int* E, const double* q, const
 template void launch_elem_fwd<double>(int, int, int, const int*, const double*, const double*, const unsigned char*,
                                       const double*, int, double, const EnergyPack&, double*, Ctrl*, cudaStream_t);
 template void launch_elem_fwd<float>(int, int, int, const int*, const double*, const double*, const unsigned char*,
-                                     const double*, int, double, const EnergyPack&, float*, Ctrl*, cudaStream_t);
+                                     const double*, int, double, const EnergyPack&, double*, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<double>(int, const int*, const int*, const double*, const double*, double,
                                         const unsigned char*, const int*, double*, int, double*, double*, int, NodeCsr,
                                         const double*, Ctrl*, cudaStream_t);
-template void launch_gather_fwd<float>(int, const int*, const int*, const float*, const double*, double,
+template void launch_gather_fwd<float>(int, const int*, const int*, const double*, const double*, double,
                                        const unsigned char*, const int*, float*, int, double*, double*, int, NodeCsr,
                                        const double*, Ctrl*, cudaStream_t);
 

@@ -12,7 +12,6 @@ constexpr int kMaxWindow = 8;
 constexpr int kTileCols = 128;       // S^T column tile width (32 lanes x 4 columns)
 constexpr int kRedBlocks = 296;      // grid of the small adjoint reductions (2 x 148 SMs)
 constexpr int kMaxRedBlocks = 1184;  // upper bound of the per-iteration reduction grids (8 x 148 SMs)
-constexpr int kAaSlots = 24;         // per-block partial slots of the AA reduction
 
 // Status bits written by kernels (never a trap).
 enum StatusBits : int {
@@ -29,6 +28,7 @@ struct Ctrl {
     int max_iter, window, mode;          // mode 0: forward, 1: adjoint
     double rel_tol, abs_tol, clip;
     double gamma[kMaxWindow];
+    double gram[kMaxWindow][kMaxWindow];  // dG_i . dG_j by ring slot (incrementally extended)
     double dq, rn, pdc, pdr, err, xn;    // last gate quantities
     double rz, alpha, beta;              // conjugate-gradient scalars of the adjoint solve
     int pcg_init;
@@ -44,7 +44,7 @@ struct EnergyPack {
 // Forward local step: per-element node contributions of sum_energies w_e (vol/s) A_s^T (Bp(F_s) - F_bound,s).
 template <typename T>
 void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const double* qb, const unsigned char* elem_dir,
-                     const double* grad, int hex, double vol_over_s, const EnergyPack& ep, T* elem_out, Ctrl* ctrl,
+                     const double* grad, int hex, double vol_over_s, const EnergyPack& ep, double* elem_out, Ctrl* ctrl,
                      cudaStream_t st);
 // Per-node gather of element contributions: b = inv_h2m q_tilde + pd (Dirichlet rows zero), written to the
 // permuted SoA right-hand side; pd kept node-major with the gate partial norms.
@@ -55,7 +55,7 @@ struct NodeCsr {
     const double* v = nullptr;
 };
 template <typename T>
-void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const T* elem_out, const double* qt,
+void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
                        double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, Ctrl* ctrl,
                        cudaStream_t st);

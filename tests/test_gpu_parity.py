@@ -224,15 +224,16 @@ def test_pcg_adjoint_matches_converged_oracle_adjoint(fp32):
 
 
 def test_mixed_precision_forward_error_vs_fp64():
-    """FP32 projection and FP32 S^T S in refinement form (FP64 residual against A) stay within 1e-6 of the FP64
-    oracle positions after a short rollout at a tight gate."""
+    """FP32 projection (delta form) and FP32 S^T S in refinement form (FP64 residual against A) converge to a
+    tight 1e-9 dual gate and stay within 1e-5 of the displacement of the FP64 oracle after a short rollout."""
     sc = scenes.nh_tet_block(cells=(8, 4, 4), dx=0.01, steps=5)
     opts = dict(sc.options)
     opts.update(aa_window=0, rel_tol=1e-9, abs_tol=1e-12, max_pd_iter=5000)
     o = oracle.OracleDeformable.from_scene(sc)
     q_ref, _, _ = oracle.rollout(o, sc, steps=5, options=opts)
     d = core.from_scene(sc)
-    qs, _ = _rollout_gpu(d, sc, 5, dict(opts, fp32_bulk=1, rel_tol=1e-7))
+    qs, _ = _rollout_gpu(d, sc, 5, dict(opts, fp32_bulk=1))
+    it, conv = d.frame_stats()
+    assert conv.all()
     disp = np.abs(q_ref - sc.q0).max()
-    assert np.abs(qs[-1] - q_ref).max() <= 1e-4 * disp
-    assert np.abs(qs[-1] - q_ref).max() <= 1e-6 * np.abs(q_ref).max()
+    assert np.abs(qs[-1] - q_ref).max() <= 1e-5 * disp
