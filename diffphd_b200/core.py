@@ -77,6 +77,7 @@ def load_library():
     L.dphd_s_padded_values.argtypes = [C.c_void_p]
     L.dphd_s_padded_values.restype = C.c_longlong
     L.dphd_debug_time_ainv.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, _dp]
+    L.dphd_ainv_noalloc.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.dphd_debug_ainv.argtypes = [C.c_void_p, C.c_double, _dp, _dp, C.c_int]
     L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]

@@ -274,6 +274,10 @@ int dphd_debug_time_ainv(dphd_deformable* h, double dt, int reps, int fp32, int 
     });
 }
 
+int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream) {
+    return guard([&] { E(h).ainv_noalloc(dt, d_b, d_x, fp32 != 0, (cudaStream_t)stream); });
+}
+
 long long dphd_s_padded_values(const dphd_deformable* h) { return h && h->eng ? h->eng->s_padded_values() : -1; }
 
 int dphd_num_frames(const dphd_deformable* h) {

@@ -760,6 +760,18 @@ void Engine::backward(const double* q, const double* v, const double* f_ext, dou
     CUDA_OK(cudaStreamSynchronize(st));
 }
 
+void ainv_noalloc(const SpmvPlan<double>& p64, const SpmvPlan<float>& p32, const unsigned char* fixed_node,
+                  const double* d_b, double* d_x, bool fp32, cudaStream_t st);
+
+void Engine::ainv_noalloc(double dt, const double* d_b, double* d_x, bool fp32, cudaStream_t st) {
+    DPHD_CHECK(built_ && built_dt_ == dt && device_ready_,
+               "dphd_ainv_noalloc: the factor for this dt is not on the device yet; make one allocating call "
+               "first (dphd_forward, dphd_forward_device or dphd_debug_ainv with the same dt)");
+    DPHD_CHECK(d_b && d_x, "null device pointer");
+    dphd::ainv_noalloc(plan64_, plan32_, d_fixed_node.as<unsigned char>(), d_b, d_x, fp32, st);
+    launches_ += 5;
+}
+
 double Engine::time_ainv(double dt, int reps, bool fp32, bool flush_l2) {
     ensure_built(dt, 0);
     cudaStream_t st = stream_;

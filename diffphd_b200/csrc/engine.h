@@ -91,6 +91,10 @@ public:
     double time_ainv(double dt, int reps, bool fp32, bool flush_l2);
     long long kernel_launches() const { return launches_; }
 
+    // x = A^-1 b on device pointers without allocating (temporaries in a static device array); the factor
+    // for this dt must already be built by an earlier (allocating) call on this handle.
+    void ainv_noalloc(double dt, const double* d_b, double* d_x, bool fp32, cudaStream_t stream);
+
     // diagnostics used by the tests
     void apply_ainv(double dt, const double* b, double* x, bool fp32);
     void host_sts_apply(double dt, const double* b, double* x);

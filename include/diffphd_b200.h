@@ -111,6 +111,16 @@ long long dphd_s_nnz(const dphd_deformable* h);
 /* Stored S values including the 16-byte alignment padding of each row segment. */
 long long dphd_s_padded_values(const dphd_deformable* h);
 
+/* x = A^-1 b through the S^T S pair on device pointers (b, x: 3n FP64 node-major; Dirichlet rows of b are
+ * taken as zero, as in the forward step), allocating no GPU memory: its temporaries live in a static 32 MiB
+ * device array instead.  No counterpart in the reference.  For callers that cannot call cudaMalloc during a
+ * step (a fixed memory budget, a host framework that owns the allocator, or no implicit device syncs).
+ * Requires the factor for this dt to be on the device already (one earlier allocating call on the handle);
+ * fails with a clear error when the mesh needs more scratch than the array holds.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up the array's address; make it before any stream capture. */
+int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream);
+
 /* Diagnostics used by the tests: x = A^-1 b through the GPU S^T S pair (fp32 = 0 or 1), the same product
  * with the host copy of S (the set-up self-check of forward_gpu.cpp:653-670), and the GPU local step
  * (ProjectiveDynamicsLocalStep, deformable_projective_dynamics_forward.cpp:186-292). */
