@@ -87,10 +87,34 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def build_scene():
+SCENE = "nh_tet_block"
+
+
+def build_scene(name=None):
+    """The bench workload, or (for kernel-only profiling) the 24^3 hex block without contact, whose S is
+    larger than L2."""
     from diffphd_b200 import scenes
-    sc = scenes.nh_tet_block()
-    return sc
+    name = name or SCENE
+    if name == "nh_tet_block":
+        return scenes.nh_tet_block()
+    if name == "hex24":
+        sc = scenes.contact_drop()
+        sc.plane = None
+        return sc
+    raise SystemExit(f"unknown scene {name}")
+
+
+def run_ainv_only(args):
+    """Kernel-only mode for profiling: builds the scene's factor, then applies the S^T S pair `reps` times."""
+    import numpy as np
+    from diffphd_b200 import core
+    sc = build_scene(args.scene)
+    d = core.from_scene(sc)
+    fp32 = args.precision == "mixed"
+    d.debug_ainv(np.ones(sc.dofs), sc.dt, fp32=fp32)
+    ms = d.time_ainv(sc.dt, reps=args.ainv_reps, fp32=fp32, flush_l2=False)
+    print(json.dumps({"scene": args.scene, "precision": args.precision, "ms_per_apply": ms, "nnz_S": d.s_nnz(),
+                      "stored_values": d.s_padded_values()}))
 
 
 def options(sc, precision):
@@ -135,12 +159,24 @@ def cpu_baseline(sc, opts, steps=1):
 
 
 def run_ours(args, rank, world, local_rank):
+    line = _measure(args, rank, world, local_rank, args.precision, full=True)
+    if args.precision == "mixed" and not args.no_fp64_compare:
+        ref = _measure(args, rank, world, local_rank, "f64", full=False)
+        if line is not None and ref is not None:
+            line["plain_fp64_gpu"] = {"value": ref["value"], "unit": "steps/s", "ms_per_step": ref["ms_per_step"],
+                                      "pd_iters_per_step": ref["pd_iters_per_step"],
+                                      "adjoint_iters_per_step": ref["adjoint_iters_per_step"],
+                                      "speedup_of_mixed": line["value"] / ref["value"]}
+    return line
+
+
+def _measure(args, rank, world, local_rank, precision, full):
     import torch
     from diffphd_b200 import core
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     sc = build_scene()
-    opts = options(sc, args.precision)
+    opts = options(sc, precision)
     d = core.from_scene(sc)
     n3 = sc.dofs
     method = "pd_eigen_alg_phd"
@@ -213,6 +249,17 @@ def run_ours(args, rank, world, local_rank):
     t_dev = sum(a.elapsed_time(b) for a, b in ev) / 1e3
     fwd_iters, conv = d.frame_stats()
 
+    if not full:
+        if world > 1:
+            t = torch.tensor([t_dev], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            t_dev = float(t[0])
+        if rank != 0:
+            return None
+        return {"value": args.steps * world / t_dev, "ms_per_step": t_dev / args.steps * 1e3,
+                "pd_iters_per_step": float(np.mean(fwd_iters)) if len(fwd_iters) else None,
+                "adjoint_iters_per_step": float(np.mean(bwd_iters)) if bwd_iters else None}
+
     # timed region 2 (e2e): host buffers through the C ABI
     qh, vh = q_start.cpu().numpy(), v_start.cpu().numpy()
     fh = np.asarray(sc.f_ext)
@@ -250,7 +297,7 @@ def run_ours(args, rank, world, local_rank):
         return None
 
     # roofline of the dominant kernel pair (S v, S^T y): algorithmic bytes per A^-1 apply (3 RHS)
-    fp32 = args.precision == "mixed"
+    fp32 = precision == "mixed"
     nnz = d.s_nnz()
     n = sc.n
     alg = 2 * nnz * (8 if fp32 else 12) + 4 * 3 * n * (4 if fp32 else 8)
@@ -331,11 +378,18 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["f64", "mixed"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--scene", default="nh_tet_block", choices=["nh_tet_block", "hex24"])
+    ap.add_argument("--ainv-reps", type=int, default=0,
+                    help="profiling mode: only apply the S^T S pair this many times on --scene")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.ainv_reps > 0:
+        run_ainv_only(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
