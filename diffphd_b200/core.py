@@ -72,6 +72,7 @@ def load_library():
                                      [C.c_void_p, C.c_void_p, C.c_void_p]
     L.dphd_backward_device.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + \
         kv + [C.c_void_p] * 7
+    L.dphd_reset_warm_start.argtypes = [C.c_void_p]
     L.dphd_kernel_launches.argtypes = [C.c_void_p]
     L.dphd_kernel_launches.restype = C.c_longlong
     L.dphd_s_padded_values.argtypes = [C.c_void_p]
@@ -273,6 +274,9 @@ class Deformable:
                                                  ptr(dl_dv_next), float(dt), k, _ptr(vals), no, ptr(dl_dq),
                                                  ptr(dl_dv), ptr(dl_df_ext), ptr(dl_dmat_w), ptr(dl_dparams),
                                                  ptr(dl_dstate_p), C.c_void_p(int(stream))))
+
+    def reset_warm_start(self):
+        self._check(self._L.dphd_reset_warm_start(self._h))
 
     def kernel_launches(self):
         return int(self._L.dphd_kernel_launches(self._h))

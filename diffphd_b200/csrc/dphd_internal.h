@@ -76,6 +76,18 @@ struct NodeMatrix {
     std::vector<double> v;
 };
 
+// Root-first etree paths of the S columns of contact candidates: for candidate c (permuted column col_c),
+// entries k = 0 .. depth_c-1 walk from the etree root down to col_c; path_row[off_c + k] is the S row and
+// path_val[off_c + k] = S(row, col_c).  Two candidates' paths share exactly the prefix from the root to
+// their lowest common ancestor, so (A^-1)_{ij} = sum over the shared prefix of path_val_i * path_val_j.
+struct ContactPaths {
+    std::vector<int64_t> off;   // K + 1
+    std::vector<int> row;
+    std::vector<double> val;
+    int max_depth = 0;
+};
+ContactPaths build_contact_paths(const SFactor& S, const std::vector<int>& cand_nodes);
+
 void init_samples(HostModel& M);
 double element_volume(const HostModel& M, int e);
 NodeMatrix assemble_A(const HostModel& M, double dt);

@@ -191,6 +191,7 @@ void Engine::set_frictional_boundary(const std::string& type, const double* para
     for (int v : u) DPHD_CHECK(v >= 0 && v < M.n, "Frictional boundary vertex out of range.");
     M.contact_nodes.assign(u.begin(), u.end());
     M.has_plane = true;
+    device_ready_ = false;
 }
 
 int Engine::num_pd_params() const {
@@ -448,8 +449,125 @@ void Engine::build_device(int threads) {
         Acsr_.ci = d_A_ci.as<int>();
         Acsr_.v = d_A_v.as<double>();
     }
+    d_q0.alloc(ld * sizeof(double));
+    d_vcon.alloc((size_t)npad_ * 3 * sizeof(double));
+    CUDA_OK(cudaMemset(d_vcon.p, 0, d_vcon.bytes));
+    build_contact(built_dt_);
     drop_graphs();
     device_ready_ = true;
+}
+
+// Planar contact candidates (every listed boundary node, ascending, as frictional_boundary_vertex_indices_
+// orders them), the local frame of PlanarFrictionalBoundary::GetLocalFrame
+// (cpp/core/src/friction/planar_frictional_boundary.cpp:25-40), the candidates' S column paths and the
+// Delassus node block G.
+void Engine::build_contact(double dt) {
+    has_contact_ = M.has_plane && !M.contact_nodes.empty();
+    contact_ = ContactDev();
+    if (!has_contact_) return;
+    const int K = (int)M.contact_nodes.size();
+    DPHD_CHECK((double)K * K * 8 * 2 < 64e9, "too many contact candidates for the dense Delassus block");
+    ContactDev& c = contact_;
+    c.K = K;
+    for (int d = 0; d < 3; ++d) c.n[d] = M.plane_n[d];
+    c.offset = M.plane_off;
+    double best = -1, t1[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        double e[3] = {0, 0, 0};
+        e[i] = 1;
+        const double x[3] = {c.n[1] * e[2] - c.n[2] * e[1], c.n[2] * e[0] - c.n[0] * e[2], c.n[0] * e[1] - c.n[1] * e[0]};
+        const double sq = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (sq > best) {
+            best = sq;
+            t1[0] = x[0]; t1[1] = x[1]; t1[2] = x[2];
+        }
+    }
+    const double l1 = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    for (int d = 0; d < 3; ++d) c.t1[d] = t1[d] / l1;
+    double t2[3] = {c.n[1] * c.t1[2] - c.n[2] * c.t1[1], c.n[2] * c.t1[0] - c.n[0] * c.t1[2],
+                    c.n[0] * c.t1[1] - c.n[1] * c.t1[0]};
+    const double l2 = std::sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+    for (int d = 0; d < 3; ++d) c.t2[d] = t2[d] / l2;
+    const ContactPaths P = build_contact_paths(S, M.contact_nodes);
+    dc_cand.upload(M.contact_nodes);
+    dc_off.upload(P.off);
+    dc_prow.upload(P.row);
+    dc_pval.upload(P.val);
+    dc_G.alloc((size_t)K * K * sizeof(double));
+    launch_delassus(K, dc_off.as<int64_t>(), dc_prow.as<int>(), dc_pval.as<double>(), dc_G.as<double>(), 0);
+    CUDA_OK(cudaDeviceSynchronize());
+    std::vector<double> gdiag(K), rp(K);
+    CUDA_OK(cudaMemcpy2D(gdiag.data(), sizeof(double), dc_G.p, (K + 1) * sizeof(double), sizeof(double), K,
+                         cudaMemcpyDeviceToHost));
+    for (int k = 0; k < K; ++k) rp[k] = std::max(dt * dt * gdiag[k], 1e-10);
+    dc_rprec.upload(rp);
+    for (DeviceBuffer* b : {&dc_lam, &dc_lt1, &dc_lt2, &dc_omega, &dc_E, &dc_h, &dc_rhs}) {
+        b->alloc((size_t)K * sizeof(double));
+        CUDA_OK(cudaMemset(b->p, 0, b->bytes));
+    }
+    dc_ltmp.alloc((size_t)2 * K * sizeof(double));
+    dc_act.alloc((size_t)K * sizeof(int));
+    dc_kact.alloc(sizeof(int));
+    CUDA_OK(cudaMemset(dc_kact.p, 0, sizeof(int)));
+    dc_ainvb.alloc((size_t)3 * K * sizeof(double));
+    dc_M.alloc((size_t)K * K * sizeof(double));
+    c.cand = dc_cand.as<int>();
+    c.off = dc_off.as<int64_t>();
+    c.prow = dc_prow.as<int>();
+    c.pval = dc_pval.as<double>();
+    c.G = dc_G.as<double>();
+    c.rprec = dc_rprec.as<double>();
+    c.lam = dc_lam.as<double>();
+    c.lt1 = dc_lt1.as<double>();
+    c.lt2 = dc_lt2.as<double>();
+    c.omega = dc_omega.as<double>();
+    c.Ediag = dc_E.as<double>();
+    c.hvec = dc_h.as<double>();
+    c.act = dc_act.as<int>();
+    c.kact = dc_kact.as<int>();
+    c.ainvb = dc_ainvb.as<double>();
+    c.rhs = dc_rhs.as<double>();
+    c.Mwork = dc_M.as<double>();
+    c.ltmp = dc_ltmp.as<double>();
+}
+
+void Engine::reset_warm_start() {
+    if (has_contact_ && dc_lam.p) CUDA_OK(cudaMemset(dc_lam.p, 0, dc_lam.bytes));
+}
+
+std::vector<double> Engine::contact_lambda() {
+    std::vector<double> l(has_contact_ ? contact_.K : 0);
+    if (!l.empty()) CUDA_OK(cudaMemcpy(l.data(), dc_lam.p, l.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    return l;
+}
+
+// One PD iteration with contact (FP64): b (Dirichlet rows kept, as the reference's contact branch),
+// y = S b, NCP on the active set, y += S J^T f, x_raw = S^T y, Anderson + gate.
+void Engine::enqueue_contact_iteration(cudaStream_t st) {
+    const int n = M.n, n3 = 3 * n;
+    const double inv_h2m = M.mass() / (graph_dt_ * graph_dt_);
+    const EnergyPack ep = energy_pack();
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                            d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, M.vol / M.s, ep,
+                            d_elem_out64.as<double>(), c, st);
+    launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
+                              d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                              d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
+                              gather_blocks_, NodeCsr(), nullptr, 0, c, st);
+    launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
+    launch_ncp_iteration(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, nullptr, d_q0.as<double>(),
+                         d_iperm.as<int>(), d_vcon.as<double>(), c, st);
+    SpmvPlan<double> acc = plan64_;
+    acc.y_accumulate = 1;
+    launch_s_only<double>(acc, d_vcon.as<double>(), d_y64.as<double>(), c, st);
+    launch_st_only<double>(plan64_, d_y64.as<double>(), d_xraw.as<double>(), c, st);
+    launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
+                     d_lx.as<double>(), n3, d_part_aa.as<double>(), red_blocks_, c, st);
+    launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3, d_part_upd.as<double>(),
+                     d_part_gate.as<double>(), gather_blocks_, red_blocks_, c, st);
 }
 
 EnergyPack Engine::energy_pack() const {
@@ -497,7 +615,7 @@ void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
         launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                                 gather_blocks_, Acsr_, d_x.as<double>(), c, st);
+                                 gather_blocks_, Acsr_, d_x.as<double>(), 1, c, st);
     } else {
         launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
                                 d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
@@ -505,7 +623,7 @@ void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
         launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                                   d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                   d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                                  gather_blocks_, NodeCsr(), nullptr, c, st);
+                                  gather_blocks_, NodeCsr(), nullptr, 1, c, st);
     }
     // FP32 S^T S in refinement form: x_raw = x + A~^-1 (b - A x) with the residual in FP64
     launch_ainv(f32, st, f32 ? d_x.as<double>() : nullptr);
@@ -568,6 +686,7 @@ void Engine::run_iterations(int mode, const Options& o, cudaStream_t st) {
         cudaGraph_t graph;
         CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         if (mode == 2) enqueue_bwd_iteration(cap);
+        else if (mode == 5) enqueue_contact_iteration(cap);
         else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
         else enqueue_fwd_iteration(mode == 1, cap);
         CUDA_OK(cudaStreamEndCapture(cap, &graph));
@@ -615,7 +734,20 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
         drop_graphs();
         graph_dt_ = h;
     }
-    run_iterations(o.fp32_bulk ? 1 : 0, o, st);
+    if (has_contact_) {
+        DPHD_CHECK(!o.fp32_bulk, "fp32_bulk is not available with frictional contact on this path yet.");
+        contact_.mu = o.friction_mu;
+        CUDA_OK(cudaMemsetAsync(dc_lt1.p, 0, dc_lt1.bytes, st));
+        CUDA_OK(cudaMemsetAsync(dc_lt2.p, 0, dc_lt2.bytes, st));
+        if (graphs_[5] && graph_mu_ != o.friction_mu) {
+            cudaGraphExecDestroy(graphs_[5]);
+            graphs_[5] = nullptr;
+        }
+        graph_mu_ = o.friction_mu;
+        run_iterations(5, o, st);
+    } else {
+        run_iterations(o.fp32_bulk ? 1 : 0, o, st);
+    }
     check_status("forward");
     stats.frame_iters.push_back(h_ctrl_->iter);
     stats.frame_converged.push_back(h_ctrl_->converged);
@@ -625,13 +757,16 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
 
 void Engine::forward_device(const double* dq, const double* dv, const double* df, double dt, const Options& o,
                             double* dqn, double* dvn, cudaStream_t st) {
-    DPHD_CHECK(!M.has_plane || M.contact_nodes.empty(),
-               "Frictional contact is not available in this build of the device step.");
     ensure_built(dt, o.thread_ct);
     const int n3 = dofs();
     const double h2m = dt * dt / M.mass();
     launch_qtilde(n3, dq, dv, df, dt, h2m, d_gravf.as<double>(), d_qt.as<double>(), st);
+    CUDA_OK(cudaMemcpyAsync(d_q0.p, dq, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     run_forward_loop(dq, dt, o, st);
+    if (has_contact_ && o.restitution > 0) {
+        launch_restitution(contact_, d_x.as<double>(), dq, dv, dt, o.restitution, o.contact_slop, st);
+        launches_ += 1;
+    }
     CUDA_OK(cudaMemcpyAsync(dqn, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     launch_velocity(n3, d_x.as<double>(), dq, 1.0 / dt, dvn, st);
     launches_ += 2;
@@ -652,13 +787,16 @@ void Engine::forward(const double* q, const double* v, const double* f_ext, doub
     CUDA_OK(cudaMemcpyAsync(v_next, d_vn.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
     active.clear();
+    if (has_contact_) {  // active_contact_idx = candidates with lambda > 0 (forward_gpu.cpp:1537-1541)
+        const std::vector<double> l = contact_lambda();
+        for (int k = 0; k < (int)l.size(); ++k)
+            if (l[k] > 0) active.push_back(M.contact_nodes[k]);
+    }
 }
 
 void Engine::backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt,
                              const Options& o, double* d_dq, double* d_dv, double* d_df, double* d_dmat_w,
                              double* d_dparams, double* d_dstate_p, cudaStream_t st) {
-    DPHD_CHECK(!M.has_plane || M.contact_nodes.empty(),
-               "Frictional contact is not available in this build of the adjoint.");
     ensure_built(dt, o.thread_ct);
     const int n3 = 3 * M.n, m = M.m;
     const double h = dt, mass = M.mass(), inv_h2m = mass / (h * h), h2m = h * h / mass;
@@ -878,7 +1016,7 @@ void Engine::local_step(double dt, const double* q, double* rhs) {
     launch_gather_fwd<double>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                               d_qt.as<double>(), 0.0, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                               d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
-                              gather_blocks_, NodeCsr(), nullptr, d_ctrl.as<Ctrl>(), st);
+                              gather_blocks_, NodeCsr(), nullptr, 1, d_ctrl.as<Ctrl>(), st);
     // the gather leaves pd (node-major) in prev_pd
     CUDA_OK(cudaMemcpyAsync(rhs, d_prev_pd.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(h_ctrl_, d_ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));

@@ -91,6 +91,11 @@ public:
     double time_ainv(double dt, int reps, bool fp32, bool flush_l2);
     long long kernel_launches() const { return launches_; }
 
+    // contact state: normal multipliers of the planar candidates (the frame-to-frame warm start)
+    void reset_warm_start();
+    std::vector<double> contact_lambda();
+    int num_contact_candidates() const { return (int)M.contact_nodes.size(); }
+
     // x = A^-1 b on device pointers without allocating (temporaries in a static device array); the factor
     // for this dt must already be built by an earlier (allocating) call on this handle.
     void ainv_noalloc(double dt, const double* d_b, double* d_x, bool fp32, cudaStream_t stream);
@@ -110,6 +115,8 @@ private:
     void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st);
     void launch_ainv(bool fp32, cudaStream_t st, const double* x_base = nullptr);  // d_vperm -> d_xraw
     void enqueue_pcg_iteration(bool fp32, cudaStream_t st);
+    void enqueue_contact_iteration(cudaStream_t st);
+    void build_contact(double dt);
     void enqueue_fwd_iteration(bool fp32, cudaStream_t st);
     void enqueue_bwd_iteration(cudaStream_t st);
     // mode 0 fwd64, 1 fwd mixed, 2 adjoint fixed point, 3 adjoint PCG (FP64 preconditioner), 4 PCG (FP32 precond.)
@@ -122,9 +129,11 @@ private:
     SFactor S;
     NodeMatrix A;
     int npad_ = 0, ntiles_ = 0, red_blocks_ = 1, gather_blocks_ = 1;
-    double graph_dt_ = -1;
-    cudaGraphExec_t graphs_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    size_t graph_nodes_[5] = {0, 0, 0, 0, 0};
+    double graph_dt_ = -1, graph_mu_ = 0;
+    cudaGraphExec_t graphs_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t graph_nodes_[6] = {0, 0, 0, 0, 0, 0};
+    ContactDev contact_;
+    bool has_contact_ = false;
     NodeCsr Acsr_;
     long long launches_ = 0;
     SpmvPlan<double> plan64_;
@@ -144,6 +153,8 @@ private:
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
     DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv;
+    DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
+        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_M, dc_ltmp, d_vcon, d_q0;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

@@ -195,7 +195,8 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
                                                          const unsigned char* __restrict__ fixed,
                                                          const int* __restrict__ iperm, T* __restrict__ v, int npad,
                                                          double* __restrict__ prev, double* __restrict__ part,
-                                                         NodeCsr A, const double* __restrict__ q, Ctrl* ctrl) {
+                                                         NodeCsr A, const double* __restrict__ q, int zero_dirichlet,
+                                                         Ctrl* ctrl) {
     if (ctrl->done) return;
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
             acc[0] += (p[d] - pr) * (p[d] - pr);
             acc[1] += pr * pr;
             prev[3 * i + d] = p[d];
-            v[(size_t)d * npad + j] = fx ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d] - aq[d]);
+            v[(size_t)d * npad + j] = (fx && zero_dirichlet) ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d] - aq[d]);
         }
     }
     block_sum<2>(acc, sh);
@@ -332,9 +333,15 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
         const T* o = p.ypart + (size_t)__ldg(p.row_items + k) * 3;
         s0 += o[0]; s1 += o[1]; s2 += o[2];
     }
-    y[i] = s0;
-    y[p.npad + i] = s1;
-    y[2 * (size_t)p.npad + i] = s2;
+    if (p.y_accumulate) {
+        y[i] += s0;
+        y[p.npad + i] += s1;
+        y[2 * (size_t)p.npad + i] += s2;
+    } else {
+        y[i] = s0;
+        y[p.npad + i] = s1;
+        y[2 * (size_t)p.npad + i] = s2;
+    }
 }
 
 // x = S^T y, stage 1: one CTA per (column tile, chunk of the tile's row list); partial tile sums are written
@@ -1180,10 +1187,10 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
 template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
-                       double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, Ctrl* ctrl,
-                       cudaStream_t st) {
+                       double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, int zero_dirichlet,
+                       Ctrl* ctrl, cudaStream_t st) {
     k_gather_fwd<T><<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
-                                                     v_perm, npad, prev_pd, part, A, q, ctrl);
+                                                     v_perm, npad, prev_pd, part, A, q, zero_dirichlet, ctrl);
 }
 
 template <typename T>
@@ -1256,10 +1263,10 @@ template void launch_elem_fwd<float>(int, int, int, const int*, const double*, c
                                      const double*, int, double, const EnergyPack&, double*, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<double>(int, const int*, const int*, const double*, const double*, double,
                                         const unsigned char*, const int*, double*, int, double*, double*, int, NodeCsr,
-                                        const double*, Ctrl*, cudaStream_t);
+                                        const double*, int, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<float>(int, const int*, const int*, const double*, const double*, double,
                                        const unsigned char*, const int*, float*, int, double*, double*, int, NodeCsr,
-                                       const double*, Ctrl*, cudaStream_t);
+                                       const double*, int, Ctrl*, cudaStream_t);
 
 void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
                        const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
@@ -1312,6 +1319,21 @@ void launch_param_reduce(int m, int ne, const int* np_k, const int* type_k, cons
                          cudaStream_t st) {
     if (ne > 0) k_param_reduce<<<ne, kThreads, 0, st>>>(m, np_k, type_k, off_k, gw, gmat, gnh, dl_dmat_w, dl_dparams);
 }
+
+template <typename T>
+void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st) {
+    k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
+    k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
+}
+template <typename T>
+void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
+    k_spmv_ST_part<T><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
+    k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
+}
+template void launch_s_only<double>(const SpmvPlan<double>&, const double*, double*, const Ctrl*, cudaStream_t);
+template void launch_s_only<float>(const SpmvPlan<float>&, const float*, float*, const Ctrl*, cudaStream_t);
+template void launch_st_only<double>(const SpmvPlan<double>&, const double*, double*, const Ctrl*, cudaStream_t);
+template void launch_st_only<float>(const SpmvPlan<float>&, const float*, double*, const Ctrl*, cudaStream_t);
 
 template void launch_sts<double>(const SpmvPlan<double>&, const double*, double*, double*, const Ctrl*,
                                  cudaStream_t);

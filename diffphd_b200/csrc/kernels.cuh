@@ -57,8 +57,8 @@ struct NodeCsr {
 template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
-                       double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, Ctrl* ctrl,
-                       cudaStream_t st);
+                       double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, int zero_dirichlet,
+                       Ctrl* ctrl, cudaStream_t st);
 // Sparse-inverse SpMV pair x = S^T (S v) (3 right-hand sides, permuted SoA v and y, x node-major FP64).
 // S row i: row_len[i] values from column row_a[i] (both multiples of 4) at vals[row_off[i]].
 template <typename T>
@@ -89,6 +89,7 @@ struct SpmvPlan {
     T* xpart = nullptr;
     const int* perm = nullptr;
     const double* x_base = nullptr;  // when set, x_out = x_base + S^T S v (refinement form)
+    int y_accumulate = 0;            // when set, y += S v instead of y = S v
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kChunkRows = 64;       // rows per S^T chunk CTA
@@ -145,6 +146,41 @@ void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStre
 template <typename T>
 void launch_pcg_init(int n, const double* gbar, const unsigned char* fixed_node, const int* iperm, double* r,
                      T* v_perm, int npad, cudaStream_t st);
+
+// Planar contact state on the device (see contact.cu).
+struct ContactDev {
+    int K = 0;                       // candidates (every listed boundary node, ascending)
+    const int* cand = nullptr;       // node of each candidate
+    double n[3] = {0, 0, 1}, t1[3] = {1, 0, 0}, t2[3] = {0, 1, 0};
+    double offset = 0, mu = 0;
+    const int64_t* off = nullptr;    // root-first S column paths of the candidates
+    const int* prow = nullptr;
+    const double* pval = nullptr;
+    const double* G = nullptr;       // K x K node block of A^-1
+    const double* rprec = nullptr;   // r_j = max(h^2 G_jj, 1e-10)
+    double* lam = nullptr;           // normal multipliers (warm-started across frames)
+    double* lt1 = nullptr;           // tangential multipliers (reset every frame)
+    double* lt2 = nullptr;
+    double* omega = nullptr;
+    double* Ediag = nullptr;
+    double* hvec = nullptr;
+    int* act = nullptr;              // ordered active candidate list
+    int* kact = nullptr;             // its length
+    double* ainvb = nullptr;         // 3 per active candidate
+    double* rhs = nullptr;
+    double* Mwork = nullptr;         // active system, K x K capacity
+    double* ltmp = nullptr;          // 2K
+};
+void launch_delassus(int K, const int64_t* off, const int* prow, const double* pval, double* G, cudaStream_t st);
+void launch_ncp_iteration(const ContactDev& c, const double* x, const double* y, int npad, const double* x_base,
+                          const double* q0, const int* iperm, double* vcon, Ctrl* ctrl, cudaStream_t st);
+void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,
+                        double slop, cudaStream_t st);
+// y (+)= S v only (first half of the pair), and x = S^T y only (second half).
+template <typename T>
+void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st);
+template <typename T>
+void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
 
 // Device-side adjoint routing (backward_gpu.cpp:881-917) and parameter-gradient reductions.
 // g_bar = dl_dq_next + dl_dv_next / h;  dl_dq = -dl_dv_next / h;  |g_bar| into norm_out[0].

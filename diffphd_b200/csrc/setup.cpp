@@ -425,4 +425,29 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
     }
 }
 
+ContactPaths build_contact_paths(const SFactor& S, const std::vector<int>& cand_nodes) {
+    ContactPaths P;
+    const int K = (int)cand_nodes.size();
+    P.off.assign(K + 1, 0);
+    std::vector<std::vector<int>> paths(K);
+    for (int c = 0; c < K; ++c) {
+        const int col = S.iperm[cand_nodes[c]];
+        for (int r = col; r != -1; r = S.parent[r]) paths[c].push_back(r);
+        std::reverse(paths[c].begin(), paths[c].end());
+        P.off[c + 1] = P.off[c] + (int64_t)paths[c].size();
+        P.max_depth = std::max(P.max_depth, (int)paths[c].size());
+    }
+    P.row.resize(P.off[K]);
+    P.val.resize(P.off[K]);
+    for (int c = 0; c < K; ++c) {
+        const int col = S.iperm[cand_nodes[c]];
+        for (size_t k = 0; k < paths[c].size(); ++k) {
+            const int r = paths[c][k];
+            P.row[P.off[c] + k] = r;
+            P.val[P.off[c] + k] = S.vals[S.row_ptr[r] + (col - S.lo[r])];
+        }
+    }
+    return P;
+}
+
 }  // namespace dphd

@@ -96,6 +96,10 @@ int dphd_backward_device(dphd_deformable* h, const char* method, const double* d
                          int nopts, double* d_dl_dq, double* d_dl_dv, double* d_dl_df_ext, double* d_dl_dmat_w,
                          double* d_dl_dparams, double* d_dl_dstate_p, void* stream);
 
+/* Clears the frame-to-frame warm start of the contact multipliers (the reference keeps them in
+ * alg_phd_prev_lambda_, forward_gpu.cpp:1074-1084, 1544-1545, across every later call). */
+int dphd_reset_warm_start(dphd_deformable* h);
+
 /* Number of kernels this library launched on the GPU since the handle was created (graph nodes included). */
 long long dphd_kernel_launches(const dphd_deformable* h);
 
