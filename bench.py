@@ -2,10 +2,17 @@
 """Benchmark: simulation steps/s of the projective-dynamics step + its adjoint on B200.
 
 One bench "step" is one forward PD time step (run to the dual gate) plus the adjoint of that step
-(backbone fixed point to the same tolerance, routing and per-element parameter gradients).  The
+(backbone solve to the same tolerance, routing and per-element parameter gradients).  The
 workload is the heterogeneous Neo-Hookean tet block (32x16x16 cells split into 5 tets: 40,960 tets,
 9,537 nodes, per-element (mu_e, lambda_e) from a seeded two-phase blob field, nu 0.45, dt 5e-3).
 Inputs are seeded synthetic meshes (no datasets).
+
+Headline (`value`): the learned-warm-start step: FP32 bulk + FP64 refinement, every PD loop started from
+the per-node MLP's prediction, every adjoint solve started from the previous (later) step's adjoint.  The
+network is trained before timing, on the GPU by the library's own kernels, on plain-solver rollouts of
+held-out material seeds (1..8; the timed scene is seed 0); its set-up time is reported, not timed.
+`plain_fp64_gpu` is the same step in FP64 with the reference's starts (q for the PD loop, 0 for the adjoint),
+both stopped by the same 1e-6 dual gate.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision f64|mixed]
 
@@ -117,13 +124,38 @@ def run_ainv_only(args):
                       "stored_values": d.s_padded_values()}))
 
 
-def options(sc, precision):
+def options(sc, precision, warm=False):
     o = dict(sc.options)
     o["thread_ct"] = os.cpu_count() or 8
     o["alg_phd_bwd_solver"] = 1   # conjugate-gradient adjoint, stopped by the reference's 1e-6 step rule
     if precision == "mixed":
         o["fp32_bulk"] = 1
+    if warm:
+        o["alg_phd_bwd_warm_start"] = 1
     return o
+
+
+def train_warm_start(dev, args):
+    """Trains the warm-start MLP on plain-solver rollouts of held-out material seeds (not the timed seed 0)."""
+    import torch
+    from diffphd_b200 import scenes
+    from diffphd_b200.warmstart import WarmStartMLP, fit, generate_dataset
+    seeds = list(range(1, 1 + args.ws_seeds))
+    sc0 = build_scene()
+    t0 = time.perf_counter()
+    X, Y = generate_dataset(lambda s: scenes.nh_tet_block(seed=s), seeds, args.ws_steps, dev,
+                            options=options(sc0, "mixed"))
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    mlp = WarmStartMLP(dev, seed=0)
+    hist = fit(mlp, X, Y, steps=args.ws_fit_steps, batch=65536, lr=2e-3, log_every=max(1, args.ws_fit_steps - 1))
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    info = {"train_seeds": f"{seeds[0]}..{seeds[-1]}", "rollout_steps_per_seed": args.ws_steps, "rows": int(X.shape[0]),
+            "data_gen_s": round(t1 - t0, 2), "fit_s": round(t2 - t1, 2), "fit_steps": args.ws_fit_steps,
+            "batch": 65536, "loss_first_last": [h[1] for h in hist]}
+    del X, Y
+    return mlp, info
 
 
 def cpu_baseline(sc, opts, steps=1):
@@ -136,6 +168,7 @@ def cpu_baseline(sc, opts, steps=1):
     copts = dict(opts)
     copts.pop("fp32_bulk", None)
     copts.pop("alg_phd_bwd_solver", None)
+    copts.pop("alg_phd_bwd_warm_start", None)
     copts["thread_ct"] = cores
     t_setup = time.perf_counter()
     o.ainv(np.zeros(sc.dofs), sc.dt)  # factorization, reported separately (not in the sample)
@@ -159,25 +192,39 @@ def cpu_baseline(sc, opts, steps=1):
 
 
 def run_ours(args, rank, world, local_rank):
-    line = _measure(args, rank, world, local_rank, args.precision, full=True)
-    if args.precision == "mixed" and not args.no_fp64_compare:
-        ref = _measure(args, rank, world, local_rank, "f64", full=False)
-        if line is not None and ref is not None:
-            line["plain_fp64_gpu"] = {"value": ref["value"], "unit": "steps/s", "ms_per_step": ref["ms_per_step"],
-                                      "pd_iters_per_step": ref["pd_iters_per_step"],
-                                      "adjoint_iters_per_step": ref["adjoint_iters_per_step"],
-                                      "speedup_of_mixed": line["value"] / ref["value"]}
-    return line
-
-
-def _measure(args, rank, world, local_rank, precision, full):
     import torch
     from diffphd_b200 import core
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     sc = build_scene()
-    opts = options(sc, precision)
     d = core.from_scene(sc)
+    learned = args.precision == "mixed" and not args.no_warm_start
+    mlp, ws_info = (train_warm_start(dev, args) if learned else (None, None))
+    line = _measure(args, rank, world, local_rank, args.precision, True, sc, d, mlp, warm=learned)
+    if args.precision == "mixed" and not args.no_fp64_compare:
+        ref = _measure(args, rank, world, local_rank, "f64", False, sc, d, None, warm=False)
+        abl = _measure(args, rank, world, local_rank, "mixed", False, sc, d, None, warm=False) if learned else None
+        if line is not None and ref is not None:
+            line["plain_fp64_gpu"] = {"value": ref["value"], "unit": "steps/s", "ms_per_step": ref["ms_per_step"],
+                                      "pd_iters_per_step": ref["pd_iters_per_step"],
+                                      "adjoint_iters_per_step": ref["adjoint_iters_per_step"],
+                                      "speedup_of_headline": line["value"] / ref["value"]}
+            if abl is not None:
+                line["mixed_without_warm_starts"] = {
+                    "value": abl["value"], "unit": "steps/s", "ms_per_step": abl["ms_per_step"],
+                    "pd_iters_per_step": abl["pd_iters_per_step"],
+                    "adjoint_iters_per_step": abl["adjoint_iters_per_step"]}
+    if line is not None and ws_info is not None:
+        line["warm_start_network"] = ws_info
+    return line
+
+
+def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    opts = options(sc, precision, warm=warm)
+    d.set_warm_start_network(mlp)
     n3 = sc.dofs
     method = "pd_eigen_alg_phd"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -198,6 +245,7 @@ def _measure(args, rank, world, local_rank, precision, full):
         return qs, vs
 
     # warm-up: W steps forward + adjoint (builds S, captures the iteration graphs)
+    d.reset_warm_start()
     with torch.cuda.stream(stream):
         qs, vs = roll(T(sc.q0), T(sc.v0), args.warmup)
         gq, gv = g_final.clone(), zeros.clone()
@@ -209,7 +257,8 @@ def _measure(args, rank, world, local_rank, precision, full):
     q_start, v_start = qs[-1], vs[-1]
     d.reset_frame_stats()
 
-    # timed region 1 (value): device-resident inputs
+    # timed region 1 (value): device-resident inputs; the warm starts carry state only within this rollout
+    d.reset_warm_start()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -260,8 +309,10 @@ def _measure(args, rank, world, local_rank, precision, full):
                 "pd_iters_per_step": float(np.mean(fwd_iters)) if len(fwd_iters) else None,
                 "adjoint_iters_per_step": float(np.mean(bwd_iters)) if bwd_iters else None}
 
-    # timed region 2 (e2e): host buffers through the C ABI
+    # timed region 2 (e2e): host buffers through the C ABI (PyForward / PyBackward; the attached network and
+    # the adjoint warm start act behind the same calls)
     qh, vh = q_start.cpu().numpy(), v_start.cpu().numpy()
+    d.reset_warm_start()
     fh = np.asarray(sc.f_ext)
     torch.cuda.synchronize()
     if world > 1:
@@ -328,6 +379,9 @@ def _measure(args, rank, world, local_rank, precision, full):
         "data": "synthetic (seeded two-phase blob material field, rest-state start)",
         "config": {"workload": WORKLOAD, "nodes": n, "elements": sc.m, "dt": sc.dt,
                    "precision": "fp32 bulk (projection, S/S^T) + fp64 gate/AA" if fp32 else "plain fp64",
+                   "pd_start": "learned warm start (per-node MLP, BF16 tensor cores)" if mlp is not None
+                   else "q (reference)",
+                   "adjoint_start": "previous step's adjoint" if warm else "0 (reference)",
                    "rel_tol": opts["rel_tol"], "abs_tol": opts["abs_tol"], "aa_window": opts["aa_window"],
                    "max_pd_iter": opts["max_pd_iter"], "step": "forward PD step + adjoint step",
                    "adjoint_solver": "PCG on (A - K_pd) preconditioned by S^T S, FP64 residual",
@@ -384,6 +438,10 @@ def main():
     ap.add_argument("--ainv-reps", type=int, default=0,
                     help="profiling mode: only apply the S^T S pair this many times on --scene")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-warm-start", action="store_true", help="headline without the learned / adjoint starts")
+    ap.add_argument("--ws-seeds", type=int, default=8, help="material seeds of the warm-start training rollouts")
+    ap.add_argument("--ws-steps", type=int, default=60, help="rollout steps per training seed")
+    ap.add_argument("--ws-fit-steps", type=int, default=1500, help="AdamW steps of warm-start training")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

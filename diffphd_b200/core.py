@@ -80,6 +80,17 @@ def load_library():
     L.dphd_debug_time_ainv.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, _dp]
     L.dphd_ainv_noalloc.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.dphd_debug_ainv.argtypes = [C.c_void_p, C.c_double, _dp, _dp, C.c_int]
+    L.dphd_forward_device_init.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_double] + kv + [C.c_void_p] * 4
+    L.dphd_mlp_sizes.argtypes = [_ip, _ip, _ip, _ip]
+    L.dphd_set_warm_start_network.argtypes = [C.c_void_p] * 3
+    L.dphd_mlp_pack.argtypes = [C.c_void_p] * 3
+    L.dphd_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.dphd_mlp_train_step.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_void_p] + [C.c_float] * 5 + \
+        [C.c_int] + [C.c_void_p] * 5
+    L.dphd_warmstart_features.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 8
+    L.dphd_warmstart_apply.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 4
+    L.dphd_warmstart_target.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 4
     L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     _lib = L
@@ -264,6 +275,40 @@ class Deformable:
                                                 C.c_void_p(v.data_ptr()), C.c_void_p(f_ext.data_ptr()), float(dt),
                                                 k, _ptr(vals), no, C.c_void_p(q_next.data_ptr()),
                                                 C.c_void_p(v_next.data_ptr()), C.c_void_p(int(stream))))
+
+    def forward_device_init(self, method, q, v, f_ext, dt, options, q_init, q_next, v_next, stream=0):
+        """forward_device whose PD loop starts from q_init (3n float64 CUDA tensor) instead of q."""
+        k, vals, no = _opts(options)
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        self._check(self._L.dphd_forward_device_init(self._h, method.encode(), ptr(q), ptr(v), ptr(f_ext), float(dt),
+                                                     k, _ptr(vals), no, ptr(q_init), ptr(q_next), ptr(v_next),
+                                                     C.c_void_p(int(stream))))
+
+    def set_warm_start_network(self, mlp):
+        """Attach a trained `warmstart.WarmStartMLP` (its weights are copied) or detach it (None): while
+        attached, PyForward / forward_device start each PD loop from the network's prediction."""
+        if mlp is None:
+            self._check(self._L.dphd_set_warm_start_network(self._h, None, None))
+        else:
+            import torch
+            torch.cuda.synchronize(mlp.device)  # the weights may still be in flight on a torch stream
+            self._check(self._L.dphd_set_warm_start_network(self._h, C.c_void_p(mlp.master.data_ptr()),
+                                                            C.c_void_p(mlp.packed.data_ptr())))
+
+    def warmstart_features(self, dt, q, q_prev, v, f_ext, prev_base, X, base, stream=0):
+        ptr = lambda t: C.c_void_p(t.data_ptr() if t is not None else 0)
+        self._check(self._L.dphd_warmstart_features(self._h, float(dt), ptr(q), ptr(q_prev), ptr(v), ptr(f_ext),
+                                                    ptr(prev_base), ptr(X), ptr(base), C.c_void_p(int(stream))))
+
+    def warmstart_apply(self, dt, base, out, q_init, stream=0):
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        self._check(self._L.dphd_warmstart_apply(self._h, float(dt), ptr(base), ptr(out), ptr(q_init),
+                                                 C.c_void_p(int(stream))))
+
+    def warmstart_target(self, dt, q_next, base, Y, stream=0):
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        self._check(self._L.dphd_warmstart_target(self._h, float(dt), ptr(q_next), ptr(base), ptr(Y),
+                                                  C.c_void_p(int(stream))))
 
     def backward_device(self, method, q_next, dl_dq_next, dl_dv_next, dt, options, dl_dq, dl_dv, dl_df_ext,
                         dl_dmat_w=None, dl_dparams=None, dl_dstate_p=None, stream=0):

@@ -250,6 +250,91 @@ int dphd_forward_device(dphd_deformable* h, const char* method, const double* d_
     });
 }
 
+int dphd_forward_device_init(dphd_deformable* h, const char* method, const double* d_q, const double* d_v,
+                             const double* d_f, double dt, const char** keys, const double* vals, int nopts,
+                             const double* d_q_init, double* d_qn, double* d_vn, void* stream) {
+    return guard([&] {
+        check_method(method);
+        DPHD_CHECK(d_q && d_v && d_f && d_q_init && d_qn && d_vn, "null device pointer");
+        DPHD_CHECK(dt > 0, "dt must be positive");
+        const dphd::Options o = dphd::Options::parse(to_map(keys, vals, nopts));
+        E(h).forward_device_init(d_q, d_v, d_f, dt, o, d_q_init, d_qn, d_vn, (cudaStream_t)stream);
+    });
+}
+
+int dphd_set_warm_start_network(dphd_deformable* h, const float* d_master, const void* d_packed) {
+    return guard([&] { E(h).set_ws_net(d_master, d_packed); });
+}
+
+int dphd_mlp_sizes(int* n_master, int* n_packed, int* part_floats_per_block, int* rows_per_block) {
+    return guard([&] {
+        if (n_master) *n_master = dphd::mlp_param_count();
+        if (n_packed) *n_packed = dphd::mlp_packed_count();
+        if (part_floats_per_block) *part_floats_per_block = dphd::mlp_part_size();
+        if (rows_per_block) *rows_per_block = dphd::mlp_rows_per_block();
+    });
+}
+
+int dphd_mlp_pack(float* d_master, void* d_packed, void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_master && d_packed, "null device pointer");
+        dphd::mlp_pack_flat(d_master, d_packed, (cudaStream_t)stream);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
+int dphd_mlp_forward(float* d_master, void* d_packed, const void* d_X, int n, float* d_out, void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_master && d_packed && d_X && d_out, "null device pointer");
+        DPHD_CHECK(n >= 0, "negative row count");
+        dphd::mlp_forward_flat(d_master, d_packed, d_X, n, d_out, (cudaStream_t)stream);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
+int dphd_mlp_train_step(float* d_master, void* d_packed, const void* d_X, const float* d_Y, int n, float* d_part,
+                        float lr, float beta1, float beta2, float eps, float weight_decay, int step, float* d_m,
+                        float* d_v, float* d_grad, float* d_loss, void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_master && d_packed && d_X && d_Y && d_part && d_m && d_v, "null device pointer");
+        DPHD_CHECK(n > 0, "empty training batch");
+        DPHD_CHECK(step >= 1, "AdamW step counter starts at 1");
+        const cudaStream_t st = (cudaStream_t)stream;
+        const int blocks = dphd::mlp_train_flat(d_master, d_packed, d_X, d_Y, n, d_part, st);
+        dphd::mlp_adamw_flat(d_master, d_packed, d_part, blocks, lr, beta1, beta2, eps, weight_decay, step, d_m, d_v,
+                             d_grad, d_loss, st);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
+int dphd_warmstart_features(dphd_deformable* h, double dt, const double* d_q, const double* d_q_prev,
+                            const double* d_v, const double* d_f, const double* d_prev_base, void* d_X,
+                            double* d_base, void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_q && d_q_prev && d_v && d_f && d_X && d_base, "null device pointer");
+        E(h).ws_features(dt, d_q, d_q_prev, d_v, d_f, d_prev_base, d_X, d_base, (cudaStream_t)stream);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
+int dphd_warmstart_apply(dphd_deformable* h, double dt, const double* d_base, const float* d_out, double* d_q_init,
+                         void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_base && d_out && d_q_init, "null device pointer");
+        E(h).ws_apply(dt, d_base, d_out, d_q_init, (cudaStream_t)stream);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
+int dphd_warmstart_target(dphd_deformable* h, double dt, const double* d_q_next, const double* d_base, float* d_Y,
+                          void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_q_next && d_base && d_Y, "null device pointer");
+        E(h).ws_target(dt, d_q_next, d_base, d_Y, (cudaStream_t)stream);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
 int dphd_backward_device(dphd_deformable* h, const char* method, const double* d_q_next, const double* d_dl_dq_next,
                          const double* d_dl_dv_next, double dt, const char** keys, const double* vals, int nopts,
                          double* d_dl_dq, double* d_dl_dv, double* d_dl_df_ext, double* d_dl_dmat_w,

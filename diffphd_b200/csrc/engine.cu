@@ -23,13 +23,6 @@
 
 namespace dphd {
 
-#define CUDA_OK(x)                                                                                    \
-    do {                                                                                              \
-        cudaError_t e__ = (x);                                                                        \
-        if (e__ != cudaSuccess) throw Error(std::string("CUDA error: ") + cudaGetErrorString(e__) +   \
-                                            " at " + __FILE__ + ":" + std::to_string(__LINE__));      \
-    } while (0)
-
 void DeviceBuffer::release() {
     if (p) cudaFree(p);
     p = nullptr;
@@ -64,6 +57,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.bwd_eigen_filter = (int)get("bwd_eigen_filter", 0);
     o.fp32_bulk = (int)get("fp32_bulk", 0);
     o.bwd_solver = (int)get("alg_phd_bwd_solver", 0);
+    o.bwd_warm_start = (int)get("alg_phd_bwd_warm_start", 0);
     o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
@@ -533,6 +527,8 @@ void Engine::build_contact(double dt) {
 
 void Engine::reset_warm_start() {
     if (has_contact_ && dc_lam.p) CUDA_OK(cudaMemset(dc_lam.p, 0, dc_lam.bytes));
+    mu_prev_valid_ = false;
+    ws_prev_valid_ = false;
 }
 
 std::vector<double> Engine::contact_lambda() {
@@ -723,10 +719,11 @@ void Engine::check_status(const char* where) {
     (void)where;
 }
 
-void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st) {
+void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st,
+                              const double* d_init) {
     const int n3 = 3 * M.n;
     Ctrl* c = d_ctrl.as<Ctrl>();
-    CUDA_OK(cudaMemcpyAsync(d_x.p, dq_in, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_x.p, d_init ? d_init : dq_in, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CUDA_OK(cudaMemsetAsync(d_prev_pd.p, 0, n3 * sizeof(double), st));
     init_ctrl(h_ctrl_, 0, o, o.max_pd_iter, 0.0);
     CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
@@ -757,12 +754,24 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
 
 void Engine::forward_device(const double* dq, const double* dv, const double* df, double dt, const Options& o,
                             double* dqn, double* dvn, cudaStream_t st) {
+    forward_device_init(dq, dv, df, dt, o, nullptr, dqn, dvn, st);
+}
+
+void Engine::forward_device_init(const double* dq, const double* dv, const double* df, double dt, const Options& o,
+                                 const double* d_init, double* dqn, double* dvn, cudaStream_t st) {
     ensure_built(dt, o.thread_ct);
     const int n3 = dofs();
     const double h2m = dt * dt / M.mass();
+    const bool learned = !d_init && ws_net_;
+    if (learned) d_init = ws_predict(dq, dv, df, dt, st);
     launch_qtilde(n3, dq, dv, df, dt, h2m, d_gravf.as<double>(), d_qt.as<double>(), st);
     CUDA_OK(cudaMemcpyAsync(d_q0.p, dq, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    run_forward_loop(dq, dt, o, st);
+    run_forward_loop(dq, dt, o, st, d_init);
+    if (learned) {
+        CUDA_OK(cudaMemcpyAsync(d_ws_qprev.p, dq, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        ws_which_ ^= 1;
+        ws_prev_valid_ = true;
+    }
     if (has_contact_ && o.restitution > 0) {
         launch_restitution(contact_, d_x.as<double>(), dq, dv, dt, o.restitution, o.contact_slop, st);
         launches_ += 1;
@@ -771,6 +780,90 @@ void Engine::forward_device(const double* dq, const double* dv, const double* df
     launch_velocity(n3, d_x.as<double>(), dq, 1.0 / dt, dvn, st);
     launches_ += 2;
     CUDA_OK(cudaGetLastError());
+}
+
+double Engine::ws_dx() const { return std::pow(M.vol, 1.0 / 3.0); }
+
+void Engine::set_ws_net(const float* d_master, const void* d_packed) {
+    if (!d_master) {
+        ws_net_ = false;
+        ws_prev_valid_ = false;
+        return;
+    }
+    DPHD_CHECK(d_packed, "warm-start network: null packed weights");
+    d_ws_master.alloc((size_t)mlp_param_count() * sizeof(float));
+    d_ws_packed.alloc((size_t)mlp_packed_count() * 2);
+    CUDA_OK(cudaMemcpy(d_ws_master.p, d_master, d_ws_master.bytes, cudaMemcpyDeviceToDevice));
+    CUDA_OK(cudaMemcpy(d_ws_packed.p, d_packed, d_ws_packed.bytes, cudaMemcpyDeviceToDevice));
+    ws_net_ = true;
+    ws_prev_valid_ = false;
+}
+
+const double* Engine::ws_predict(const double* dq, const double* dv, const double* df, double dt, cudaStream_t st) {
+    const int n = M.n, n3 = 3 * n;
+    d_ws_X.alloc((size_t)n * 16 * 2);
+    d_ws_out.alloc((size_t)n * 8 * sizeof(float));
+    d_ws_base0.alloc(n3 * sizeof(double));
+    d_ws_base1.alloc(n3 * sizeof(double));
+    d_ws_qprev.alloc(n3 * sizeof(double));
+    d_ws_qinit.alloc(n3 * sizeof(double));
+    double* base = (ws_which_ ? d_ws_base1 : d_ws_base0).as<double>();
+    const double* prev_base = ws_prev_valid_ ? (ws_which_ ? d_ws_base0 : d_ws_base1).as<double>() : nullptr;
+    const double* qp = ws_prev_valid_ ? d_ws_qprev.as<double>() : dq;
+    ws_features(dt, dq, qp, dv, df, prev_base, d_ws_X.p, base, st);
+    mlp_forward_flat(d_ws_master.as<float>(), d_ws_packed.p, d_ws_X.p, n, d_ws_out.as<float>(), st);
+    ws_apply(dt, base, d_ws_out.as<float>(), d_ws_qinit.as<double>(), st);
+    launches_ += 1;
+    return d_ws_qinit.as<double>();
+}
+
+void Engine::ws_features(double dt, const double* dq, const double* dqp, const double* dv, const double* df,
+                         const double* d_prev_base, void* X, double* d_base, cudaStream_t st) {
+    DPHD_CHECK(built_ && built_dt_ == dt && device_ready_, "warm start: make one forward call with this dt first");
+    if (!d_wlog.p) {
+        // log10 of each node's mean PD stiffness over its incident elements
+        std::vector<double> acc(M.n, 0.0);
+        std::vector<int> cnt(M.n, 0);
+        for (int e = 0; e < M.m; ++e) {
+            double w = 0;
+            for (const auto& en : M.energies)
+                if (en.all_elements || en.in_set[e]) w += en.elem_w(e);
+            for (int a = 0; a < M.k; ++a) {
+                acc[M.E[(size_t)e * M.k + a]] += w;
+                cnt[M.E[(size_t)e * M.k + a]]++;
+            }
+        }
+        std::vector<float> wl(M.n);
+        for (int i = 0; i < M.n; ++i) wl[i] = (float)std::log10(std::max(acc[i] / std::max(cnt[i], 1), 1.0)) / 7.0f;
+        d_wlog.upload(wl);
+    }
+    FeatureArgs a;
+    a.n = M.n;
+    a.X = dX.as<double>();
+    a.fixed = d_fixed_node.as<unsigned char>();
+    a.wlog = d_wlog.as<float>();
+    a.inv_dx = 1.0 / ws_dx();
+    a.h = dt;
+    a.h2m = dt * dt / M.mass();
+    for (int d = 0; d < 3; ++d) a.gforce[d] = M.has_gravity ? M.mass() * M.gravity[d] : 0.0;
+    a.plane = M.has_plane ? 1 : 0;
+    for (int d = 0; d < 3; ++d) a.pn[d] = M.plane_n[d];
+    a.poff = M.plane_off;
+    launch_mlp_features(a, dq, dqp, dv, df, d_prev_base, X, d_base, st);
+    launches_ += 1;
+}
+
+void Engine::ws_apply(double dt, const double* d_base, const float* out, double* d_q_init, cudaStream_t st) {
+    (void)dt;
+    launch_mlp_apply(dofs(), d_base, out, ws_dx(), d_fixed_dof.as<unsigned char>(), d_fixed_val.as<double>(), d_q_init,
+                     st);
+    launches_ += 1;
+}
+
+void Engine::ws_target(double dt, const double* d_q_next, const double* d_base, float* Y, cudaStream_t st) {
+    (void)dt;
+    launch_mlp_target(dofs(), d_q_next, d_base, 1.0 / ws_dx(), Y, st);
+    launches_ += 1;
 }
 
 void Engine::forward(const double* q, const double* v, const double* f_ext, double dt, const Options& o,
@@ -822,12 +915,26 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
         h_ctrl_->pcg_init = 1;
         CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemsetAsync(d_pp.p, 0, n3 * sizeof(double), st));
+        // warm start from the previous call's adjoint (the next time step of a reverse sweep): mu_0 = mu_prev,
+        // r_0 = g_bar - (A - K_pd) mu_0; the gate is unchanged, so only the iteration count moves
+        const bool warm = o.bwd_warm_start && mu_prev_valid_ && d_mu_prev.bytes == n3 * sizeof(double);
+        const double* w0 = nullptr;
+        if (warm) {
+            CUDA_OK(cudaMemcpyAsync(d_x.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
+                            d_J.as<double>(), d_elem_out64.as<double>(), c, st);
+            launch_pcg_gather(M.n, Acsr_, d_x.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
+                              d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
+                              d_part_gate.as<double>(), gather_blocks_, c, st);
+            w0 = d_wv.as<double>();
+            launches_ += 2;
+        }
         if (f32)
-            launch_pcg_init<float>(M.n, d_gbar.as<double>(), d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+            launch_pcg_init<float>(M.n, d_gbar.as<double>(), w0, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                    d_r.as<double>(), d_vperm32.as<float>(), npad_, st);
         else
-            launch_pcg_init<double>(M.n, d_gbar.as<double>(), d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
-                                    d_r.as<double>(), d_vperm64.as<double>(), npad_, st);
+            launch_pcg_init<double>(M.n, d_gbar.as<double>(), w0, d_fixed_node.as<unsigned char>(),
+                                    d_iperm.as<int>(), d_r.as<double>(), d_vperm64.as<double>(), npad_, st);
         launch_ainv(f32, st);
         launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
                            gather_blocks_, red_blocks_, c, st);
@@ -843,6 +950,8 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
             stats.bwd_fallbacks++;
         }
     } else {
+        if (o.bwd_warm_start && mu_prev_valid_ && d_mu_prev.bytes == n3 * sizeof(double))
+            CUDA_OK(cudaMemcpyAsync(d_x.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
         run_iterations(2, o, st);
     }
     stats.last_bwd_iters = h_ctrl_->iter;
@@ -856,6 +965,11 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
         if (d_dparams && np) CUDA_OK(cudaMemsetAsync(d_dparams, 0, np * sizeof(double), st));
         if (d_dstate_p && M.has_gravity) CUDA_OK(cudaMemsetAsync(d_dstate_p, 0, 3 * sizeof(double), st));
         return;
+    }
+    if (o.bwd_warm_start) {
+        d_mu_prev.alloc(n3 * sizeof(double));
+        CUDA_OK(cudaMemcpyAsync(d_mu_prev.p, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        mu_prev_valid_ = true;
     }
     launch_adj_route(n3, d_x.as<double>(), h_ctrl_->rn, d_adjnorm.as<double>(), inv_h2m, h, h2m, mass,
                      o.bwd_cascade_cap, M.has_gravity ? 1 : 0, d_dq, d_dv, d_df,

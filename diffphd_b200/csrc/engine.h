@@ -10,6 +10,14 @@
 #include "dphd_internal.h"
 #include "kernels.cuh"
 
+#define CUDA_OK(x)                                                                                    \
+    do {                                                                                              \
+        cudaError_t e__ = (x);                                                                        \
+        if (e__ != cudaSuccess)                                                                       \
+            throw ::dphd::Error(std::string("CUDA error: ") + cudaGetErrorString(e__) + " at " +      \
+                                __FILE__ + ":" + std::to_string(__LINE__));                           \
+    } while (0)
+
 namespace dphd {
 
 struct Options {
@@ -24,6 +32,7 @@ struct Options {
     int bwd_eigen_filter = 0;    // 0 off (exact adjoint), 1 clamp, 2 abs
     int fp32_bulk = 0;           // projection and S/S^T SpMVs in FP32
     int bwd_solver = 0;          // 0: Anderson-accelerated fixed point (reference), 1: preconditioned CG
+    int bwd_warm_start = 0;      // CG adjoint starts from the previous backward call's solution (reverse sweeps)
     int poll_chunk = 8;
     static Options parse(const std::map<std::string, double>& m);
 };
@@ -84,6 +93,21 @@ public:
     void forward_device(const double* d_q, const double* d_v, const double* d_f, double dt, const Options& o,
                         double* d_q_next, double* d_v_next, cudaStream_t stream);
 
+    // forward step whose PD iteration starts from d_q_init instead of q (the learned warm start)
+    void forward_device_init(const double* d_q, const double* d_v, const double* d_f, double dt, const Options& o,
+                             const double* d_q_init, double* d_q_next, double* d_v_next, cudaStream_t stream);
+    // warm-start features / application / training targets (see mlp.cu)
+    void ws_features(double dt, const double* d_q, const double* d_qp, const double* d_v, const double* d_f,
+                     const double* d_prev_base, void* X, double* d_base, cudaStream_t st);
+    void ws_apply(double dt, const double* d_base, const float* out, double* d_q_init, cudaStream_t st);
+    void ws_target(double dt, const double* d_q_next, const double* d_base, float* Y, cudaStream_t st);
+    double ws_dx() const;
+    // Attach a trained warm-start network (device pointers; copied into engine memory) or detach (null): while
+    // attached, every forward step whose caller gives no initial guess starts its PD loop from the network's
+    // prediction.  The previous step's q and q_tilde are engine state (reset by reset_warm_start).
+    void set_ws_net(const float* d_master, const void* d_packed);
+    bool ws_net_attached() const { return ws_net_; }
+
     void backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,
                          double* d_dq, double* d_dv, double* d_df, double* d_dmat_w, double* d_dparams,
                          double* d_dstate_p, cudaStream_t stream);
@@ -112,7 +136,8 @@ private:
     void ensure_built(double dt, int threads);
     void build_device(int threads);
     EnergyPack energy_pack() const;
-    void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st);
+    void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st,
+                          const double* d_init = nullptr);
     void launch_ainv(bool fp32, cudaStream_t st, const double* x_base = nullptr);  // d_vperm -> d_xraw
     void enqueue_pcg_iteration(bool fp32, cudaStream_t st);
     void enqueue_contact_iteration(cudaStream_t st);
@@ -152,7 +177,12 @@ private:
     DeviceBuffer d_elem_out64, d_elem_out32, d_vperm64, d_vperm32, d_y64, d_y32;
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
-    DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv;
+    DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv, d_wlog, d_mu_prev;
+    bool mu_prev_valid_ = false;
+    const double* ws_predict(const double* d_q, const double* d_v, const double* d_f, double dt, cudaStream_t st);
+    bool ws_net_ = false, ws_prev_valid_ = false;
+    int ws_which_ = 0;
+    DeviceBuffer d_ws_master, d_ws_packed, d_ws_X, d_ws_out, d_ws_base0, d_ws_base1, d_ws_qprev, d_ws_qinit;
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_M, dc_ltmp, d_vcon, d_q0;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror

@@ -1054,15 +1054,17 @@ __global__ void k_pcg_p(int n3, double* __restrict__ p, const double* __restrict
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x) p[k] = z[k] + beta * p[k];
 }
 
+// r = g_bar - w (w = (A - K_pd) mu_0 for a warm start, null for mu_0 = 0); v = r in the S ordering.
 template <typename T>
-__global__ void k_pcg_init(int n, const double* __restrict__ gbar, const unsigned char* __restrict__ fixed,
-                           const int* __restrict__ iperm, double* __restrict__ r, T* __restrict__ v, int npad) {
+__global__ void k_pcg_init(int n, const double* __restrict__ gbar, const double* __restrict__ w,
+                           const unsigned char* __restrict__ fixed, const int* __restrict__ iperm,
+                           double* __restrict__ r, T* __restrict__ v, int npad) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const bool fx = fixed[i] != 0;
     const int j = iperm[i];
     for (int d = 0; d < 3; ++d) {
-        const double g = fx ? 0.0 : gbar[3 * i + d];
+        const double g = fx ? 0.0 : gbar[3 * i + d] - (w ? w[3 * i + d] : 0.0);
         r[3 * i + d] = g;
         v[(size_t)d * npad + j] = (T)g;
     }
@@ -1287,18 +1289,18 @@ void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStre
     k_pcg_p<<<std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st>>>(n3, p, z, ctrl);
 }
 template <typename T>
-void launch_pcg_init(int n, const double* gbar, const unsigned char* fixed_node, const int* iperm, double* r,
-                     T* v_perm, int npad, cudaStream_t st) {
-    k_pcg_init<T><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, gbar, fixed_node, iperm, r, v_perm, npad);
+void launch_pcg_init(int n, const double* gbar, const double* w, const unsigned char* fixed_node, const int* iperm,
+                     double* r, T* v_perm, int npad, cudaStream_t st) {
+    k_pcg_init<T><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, gbar, w, fixed_node, iperm, r, v_perm, npad);
 }
 template void launch_pcg_update1<double>(int, double*, double*, const double*, const double*, const unsigned char*,
                                          const int*, double*, int, double*, int, Ctrl*, cudaStream_t);
 template void launch_pcg_update1<float>(int, double*, double*, const double*, const double*, const unsigned char*,
                                         const int*, float*, int, double*, int, Ctrl*, cudaStream_t);
-template void launch_pcg_init<double>(int, const double*, const unsigned char*, const int*, double*, double*, int,
-                                      cudaStream_t);
-template void launch_pcg_init<float>(int, const double*, const unsigned char*, const int*, double*, float*, int,
-                                     cudaStream_t);
+template void launch_pcg_init<double>(int, const double*, const double*, const unsigned char*, const int*, double*,
+                                      double*, int, cudaStream_t);
+template void launch_pcg_init<float>(int, const double*, const double*, const unsigned char*, const int*, double*,
+                                     float*, int, cudaStream_t);
 void launch_adj_prepare(int n3, const double* gq, const double* gv, double inv_h, double* gbar, double* dq,
                         double* part, double* norm_out, cudaStream_t st) {
     // norm_out[1] doubles as the arrival counter of this kernel (zeroed by the caller)

@@ -142,10 +142,11 @@ void launch_pcg_update1(int n, double* mu, double* r, const double* p, const dou
 void launch_pcg_update2(int n3, const double* r, const double* z, double* part, const double* mu_part, int mu_blocks,
                         int blocks, Ctrl* ctrl, cudaStream_t st);
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st);
-// r = g_bar on free DoFs (0 on Dirichlet), permuted right-hand side for the first preconditioner apply.
+// r = g_bar - w on free DoFs (0 on Dirichlet; w = (A - K_pd) mu_0 or null for mu_0 = 0), permuted right-hand
+// side for the first preconditioner apply.
 template <typename T>
-void launch_pcg_init(int n, const double* gbar, const unsigned char* fixed_node, const int* iperm, double* r,
-                     T* v_perm, int npad, cudaStream_t st);
+void launch_pcg_init(int n, const double* gbar, const double* w, const unsigned char* fixed_node, const int* iperm,
+                     double* r, T* v_perm, int npad, cudaStream_t st);
 
 // Planar contact state on the device (see contact.cu).
 struct ContactDev {
@@ -181,6 +182,35 @@ template <typename T>
 void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st);
 template <typename T>
 void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
+
+// Learned warm start (mlp.cu) -----------------------------------------------------------------------
+struct FeatureArgs {
+    int n = 0;
+    const double* X = nullptr;             // rest positions
+    const unsigned char* fixed = nullptr;  // per node
+    const float* wlog = nullptr;           // log10 of the node's mean PD stiffness
+    double inv_dx = 1, h = 0, h2m = 0;
+    double gforce[3] = {0, 0, 0};          // m g
+    int plane = 0;
+    double pn[3] = {0, 0, 1}, poff = 0;
+};
+// Per-node MLP 15 -> 128 -> 128 -> 3 (mlp.cu).  `master` holds the FP32 weights in one flat array
+// (W1 [16][128], W2 [128][128], W3 [128][8], b1 [128], b2 [128], b3 [8]); `packed` the BF16 operand copies.
+int mlp_param_count();    // floats in `master` (= gradient length)
+int mlp_packed_count();   // bf16 values in `packed`
+int mlp_part_size();      // floats of one CTA's gradient partial
+int mlp_rows_per_block(); // rows (nodes) per CTA
+void mlp_pack_flat(float* master, void* packed, cudaStream_t st);
+void mlp_forward_flat(float* master, void* packed, const void* X, int n, float* out, cudaStream_t st);
+int mlp_train_flat(float* master, void* packed, const void* X, const float* Y, int n, float* part, cudaStream_t st);
+void mlp_adamw_flat(float* master, void* packed, const float* part, int nblocks, float lr, float b1, float b2,
+                    float eps, float wd, int step, float* m, float* v, float* grad_out, float* loss_out,
+                    cudaStream_t st);
+void launch_mlp_features(const FeatureArgs& a, const double* q, const double* qp, const double* v, const double* f,
+                         const double* prev_base, void* X, double* base, cudaStream_t st);
+void launch_mlp_apply(int n3, const double* base, const float* out, double dx, const unsigned char* fixed_dof,
+                      const double* fval, double* q_init, cudaStream_t st);
+void launch_mlp_target(int n3, const double* q_next, const double* base, double inv_dx, float* Y, cudaStream_t st);
 
 // Device-side adjoint routing (backward_gpu.cpp:881-917) and parameter-gradient reductions.
 // g_bar = dl_dq_next + dl_dv_next / h;  dl_dq = -dl_dv_next / h;  |g_bar| into norm_out[0].

@@ -125,6 +125,50 @@ long long dphd_s_padded_values(const dphd_deformable* h);
  * device looks up the array's address; make it before any stream capture. */
 int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream);
 
+/* ---- Learned warm start (no counterpart in the reference: the reference starts every PD loop from q). ----
+ * A forward step whose PD loop starts from d_q_init (3n FP64) instead of q.  The loop still runs to the same
+ * dual gate, so the start only changes the iteration count, never the accepted fixed point's tolerance. */
+int dphd_forward_device_init(dphd_deformable* h, const char* method, const double* d_q, const double* d_v,
+                             const double* d_f, double dt, const char** keys, const double* vals, int nopts,
+                             const double* d_q_init, double* d_q_next, double* d_v_next, void* stream);
+/* Attach a trained warm-start network to the deformable (device pointers in the dphd_mlp_* layout below;
+ * copied, so the caller may free them), or detach it (d_master = null).  While attached, dphd_forward and
+ * dphd_forward_device start every PD loop from q_tilde + dx * MLP(features) (features from this and the
+ * previous forward call's state, kept by the handle and cleared by dphd_reset_warm_start) instead of q, and
+ * still run it to the same dual gate: drop-in for the reference's PyForward, with only the iteration count
+ * changed. */
+int dphd_set_warm_start_network(dphd_deformable* h, const float* d_master, const void* d_packed);
+/* Per-node MLP 15 -> 128 -> 128 -> 3 (GELU), BF16 tensor-core kernels with FP32 accumulation.
+ * d_master: FP32 weights in one flat array (W1 [16][128], W2 [128][128], W3 [128][8], b1 [128], b2 [128],
+ * b3 [8]; row 15 of W1 and columns 3..7 of W3/b3 are unused and kept at zero by training);
+ * d_packed: the BF16 operand copies (dphd_mlp_pack writes them).  Inputs X are BF16 [n][16]; outputs FP32
+ * [n][8] (columns 0..2 used). */
+int dphd_mlp_sizes(int* n_master, int* n_packed, int* part_floats_per_block, int* rows_per_block);
+int dphd_mlp_pack(float* d_master, void* d_packed, void* stream);
+int dphd_mlp_forward(float* d_master, void* d_packed, const void* d_X, int n, float* d_out, void* stream);
+/* One training step on rows [0, n): loss = sum over rows and the 3 outputs of (pred - Y)^2 / n (Y: FP32
+ * [n][3]); d_part holds ceil(n / rows_per_block) * part_floats_per_block floats of per-block gradient
+ * partials, summed in a fixed order (deterministic); AdamW (bias-corrected, decoupled decay on weights only)
+ * updates d_master and re-packs d_packed.  lr = 0 computes the gradient only.  d_grad (n_master floats) and
+ * d_loss (1 float) may be null. */
+int dphd_mlp_train_step(float* d_master, void* d_packed, const void* d_X, const float* d_Y, int n, float* d_part,
+                        float lr, float beta1, float beta2, float eps, float weight_decay, int step, float* d_m,
+                        float* d_v, float* d_grad, float* d_loss, void* stream);
+/* Features of every node for one step (BF16 [n][16]: (q - X)/dx, (q - q_prev)/dx, the previous step's
+ * correction (q - q_tilde_prev)/dx (zero when d_prev_base is null), h^2 f_ext/(m dx), signed height above the
+ * contact plane / dx, log10(mean stiffness)/7, Dirichlet flag, 0) and the inertial prediction
+ * q_tilde = q + h v + h^2/m (f_ext + m g) (3n FP64, d_base).  dx = cube root of the mean element volume.  The
+ * handle must have made one forward call with this dt. */
+int dphd_warmstart_features(dphd_deformable* h, double dt, const double* d_q, const double* d_q_prev,
+                            const double* d_v, const double* d_f, const double* d_prev_base, void* d_X,
+                            double* d_base, void* stream);
+/* q_init = q_tilde + dx * out[:, :3] (Dirichlet dofs take their fixed values). */
+int dphd_warmstart_apply(dphd_deformable* h, double dt, const double* d_base, const float* d_out, double* d_q_init,
+                         void* stream);
+/* Training target Y = (q_next - q_tilde) / dx (FP32 [n][3]). */
+int dphd_warmstart_target(dphd_deformable* h, double dt, const double* d_q_next, const double* d_base, float* d_Y,
+                          void* stream);
+
 /* Diagnostics used by the tests: x = A^-1 b through the GPU S^T S pair (fp32 = 0 or 1), the same product
  * with the host copy of S (the set-up self-check of forward_gpu.cpp:653-670), and the GPU local step
  * (ProjectiveDynamicsLocalStep, deformable_projective_dynamics_forward.cpp:186-292). */
