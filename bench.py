@@ -28,7 +28,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -51,47 +50,82 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _clock_worker(pci, index, period, stop, ready, out):
+    """Clock sampler process: NVML read-only queries of one GPU until `stop` is set."""
+    rows = []
+    try:
+        import pynvml as nv
+        nv.nvmlInit()
+        try:
+            h = nv.nvmlDeviceGetHandleByPciBusId(pci.encode()) if pci else nv.nvmlDeviceGetHandleByIndex(index)
+        except Exception:
+            h = nv.nvmlDeviceGetHandleByIndex(index)
+        names = [("hw_slowdown", nv.nvmlClocksEventReasonHwSlowdown),
+                 ("hw_thermal_slowdown", nv.nvmlClocksEventReasonHwThermalSlowdown),
+                 ("sw_thermal_slowdown", nv.nvmlClocksEventReasonSwThermalSlowdown),
+                 ("sw_power_cap", nv.nvmlClocksEventReasonSwPowerCap)]
+        first = True
+        while True:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            rows.append((sm, mx, [n for n, bit in names if r & bit]))
+            if first:
+                ready.set()
+                first = False
+            if stop.wait(period):
+                break
+    except Exception:
+        ready.set()
+    out.put(rows)
+
+
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples SM clocks and throttle reasons of this rank's GPU every 50 ms while the timed region runs, from a
+    separate process (NVML, read-only).  A sampler thread in this process would contend for the interpreter
+    lock with the thread that issues the library calls; an nvidia-smi subprocess per sample would cost tens of
+    milliseconds each."""
 
-    def __init__(self, index=0):
-        self.index = index
+    def __init__(self, local_rank=0, period=0.05):
+        self.local_rank = local_rank
+        self.period = period
         self.rows = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.rows.append([x.strip() for x in line.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._p = None
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        import multiprocessing as mp
+        pci = ""
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.local_rank)
+            pci = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        except Exception:
+            pass
+        ctx = mp.get_context("spawn")
+        self._stop, ready, self._q = ctx.Event(), ctx.Event(), ctx.Queue()
+        self._p = ctx.Process(target=_clock_worker,
+                              args=(pci, self.local_rank, self.period, self._stop, ready, self._q), daemon=True)
+        self._p.start()
+        ready.wait(30)
         return self
 
     def __exit__(self, *a):
+        if self._p is None:
+            return
         self._stop.set()
-        self._t.join(timeout=10)
+        try:
+            self.rows = self._q.get(timeout=30)
+        except Exception:
+            self.rows = []
+        self._p.join(timeout=10)
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        sm = [r[0] for r in self.rows]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted({n for r in self.rows for n in r[2]}), "samples": len(self.rows),
+                "source": "NVML, 50 ms period, separate process"}
 
 
 SCENE = "nh_tet_block"
@@ -216,6 +250,9 @@ def run_ours(args, rank, world, local_rank):
                     "adjoint_iters_per_step": abl["adjoint_iters_per_step"]}
     if line is not None and ws_info is not None:
         line["warm_start_network"] = ws_info
+    if line is not None and not args.no_cpu_baseline:
+        # last: the oracle's OpenMP threads would otherwise compete with the host side of the GPU timings
+        line["cpu_baseline"] = cpu_baseline(sc, options(sc, "f64"), steps=1)
     return line
 
 
@@ -398,8 +435,6 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
         "adjoint_iters_per_step": float(np.mean(bwd_iters)) if bwd_iters else None,
         "forward_converged_frac": float(np.mean(conv)) if len(conv) else None,
     }
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sc, opts, steps=1)
     return line
 
 

@@ -59,6 +59,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.bwd_solver = (int)get("alg_phd_bwd_solver", 0);
     o.bwd_warm_start = (int)get("alg_phd_bwd_warm_start", 0);
     o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
+    o.graph_while = (int)get("graph_while", 1);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -291,6 +292,30 @@ void Engine::build_device(int threads) {
         }
         t_cptr[t + 1] = (int)c_tile.size();
     }
+    // Packed descriptors (one 16-byte load per work item / S^T row instead of a chain of dependent loads).
+    // Item partial sums go to row-contiguous slots so that the S^T pass can sum a row's items itself.
+    std::vector<int> slot(it_row.size());
+    {
+        std::vector<int> pos(r_ptr.begin(), r_ptr.end() - 1);
+        for (size_t t = 0; t < it_row.size(); ++t) slot[t] = pos[it_row[t]]++;
+    }
+    std::vector<int4> idesc(it_row.size());
+    for (size_t t = 0; t < it_row.size(); ++t) {
+        const int r = it_row[t];
+        const int64_t off = ro[r] + it_c0[t];
+        idesc[t] = make_int4((int)(uint32_t)(off & 0xffffffffll), (int)(off >> 32), ra[r] + it_c0[t], it_nc[t]);
+    }
+    std::vector<int4> tdesc(trows.size());
+    std::vector<int64_t> toff(trows.size());
+    for (size_t q = 0; q < trows.size(); ++q) {
+        const int r = trows[q];
+        tdesc[q] = make_int4(ra[r], rl[r], r_ptr[r], r_ptr[r + 1]);
+        toff[q] = ro[r];
+    }
+    d_item_desc.upload(idesc);
+    d_item_slot.upload(slot);
+    d_trow_desc.upload(tdesc);
+    d_trow_off.upload(toff);
     d_short_rows.upload(it_row);
     d_grp_row0.upload(it_c0);
     d_grp_g.upload(it_nc);
@@ -322,6 +347,11 @@ void Engine::build_device(int threads) {
         P.row_a = d_row_a.as<int>();
         P.row_len = d_row_len.as<int>();
         P.n_items = (int)it_row.size();
+        P.item_desc = d_item_desc.as<int4>();
+        P.item_slot = d_item_slot.as<int>();
+        P.row_yptr = d_row_item_ptr.as<int>();
+        P.trow_desc = d_trow_desc.as<int4>();
+        P.trow_off = d_trow_off.as<int64_t>();
         P.item_row = d_short_rows.as<int>();
         P.item_c0 = d_grp_row0.as<int>();
         P.item_nc = d_grp_g.as<int>();
@@ -345,6 +375,9 @@ void Engine::build_device(int threads) {
     plan32_.ypart = d_ypart32.as<float>();
     plan32_.vals = d_vals32.as<float>();
     plan32_.xpart = d_xpart32.as<float>();
+    // the factor stays in L2 across PD iterations when it takes at most about half of it (126 MB on B200)
+    plan64_.keep_in_l2 = d_vals64.bytes <= (64ull << 20) ? 1 : 0;
+    plan32_.keep_in_l2 = d_vals32.bytes <= (64ull << 20) ? 1 : 0;
     // mesh, samples, constraints
     dE.upload(M.E);
     dX.upload(M.X);
@@ -396,7 +429,7 @@ void Engine::build_device(int threads) {
     d_dG.alloc(ld * kMaxWindow * sizeof(double));
     d_dX.alloc(ld * kMaxWindow * sizeof(double));
     red_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256));
-    gather_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n + 255) / 256));
+    gather_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n * kGatherLanes + 255) / 256));
     d_part_gate.alloc(kMaxRedBlocks * 2 * sizeof(double));
     d_part_aa.alloc(kMaxRedBlocks * 64 * sizeof(double));
     d_part_upd.alloc(kMaxRedBlocks * 3 * sizeof(double));
@@ -673,23 +706,98 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st) {
 
 // Runs iterations until the device-side gate sets `done`: one iteration is captured once as a CUDA graph and
 // replayed; the control block is read back every few iterations (doubling up to poll_chunk).
+// Runs iterations until the device-side gate sets `done`.  Default: one launch of a graph whose WHILE node
+// replays the captured iteration until k_loop_cond clears its condition (no host round trip inside a solve).
+// Fallback (graph_while = 0, or a driver without conditional nodes): the iteration graph is replayed from the
+// host and the control block polled every few iterations (doubling up to poll_chunk).
+void Engine::enqueue_iteration(int mode, cudaStream_t cap) {
+    if (mode == 2) enqueue_bwd_iteration(cap);
+    else if (mode == 5) enqueue_contact_iteration(cap);
+    else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
+    else enqueue_fwd_iteration(mode == 1, cap);
+}
+
+bool Engine::build_while_graph(int mode, int cap_iters) {
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    cudaGraph_t graph = nullptr;
+    if (cudaGraphCreate(&graph, 0) != cudaSuccess) return false;
+    cudaGraphConditionalHandle handle;
+    bool ok = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t node;
+    cudaGraphNodeParams cp = {};
+    if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+    }
+    if (ok) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        cudaStream_t cs;
+        CUDA_OK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+             cudaSuccess;
+        if (ok) {
+            enqueue_iteration(mode, cs);
+            launch_loop_cond(handle, c, cap_iters, cs);
+            cudaGraph_t out = body;
+            ok = cudaStreamEndCapture(cs, &out) == cudaSuccess;
+            size_t nn = 0;
+            if (ok) ok = cudaGraphGetNodes(body, nullptr, &nn) == cudaSuccess;
+            graph_nodes_[mode] = nn;
+        }
+        CUDA_OK(cudaStreamDestroy(cs));
+    }
+    if (ok) ok = cudaGraphInstantiate(&graphs_[mode], graph, 0) == cudaSuccess;
+    cudaGraphDestroy(graph);
+    if (!ok) {
+        graphs_[mode] = nullptr;
+        (void)cudaGetLastError();
+    }
+    return ok;
+}
+
 void Engine::run_iterations(int mode, const Options& o, cudaStream_t st) {
     Ctrl* c = d_ctrl.as<Ctrl>();
     cudaGraphExec_t& g = graphs_[mode];
+    const bool use_while = o.graph_while && while_ok_;
+    if (g && graph_is_while_[mode] != use_while) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    const int cap_iters = o.max_pd_iter + 8;
+    if (g && graph_is_while_[mode] && graph_cap_[mode] != cap_iters) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    if (!g && use_while) {
+        if (build_while_graph(mode, cap_iters)) {
+            graph_is_while_[mode] = true;
+            graph_cap_[mode] = cap_iters;
+        } else {
+            while_ok_ = false;
+        }
+    }
+    if (g && graph_is_while_[mode]) {
+        CUDA_OK(cudaGraphLaunch(g, st));
+        CUDA_OK(cudaMemcpyAsync(h_ctrl_, c, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        launches_ += (long long)h_ctrl_->loops * (long long)graph_nodes_[mode];
+        return;
+    }
     if (!g) {
         cudaStream_t cap;
         CUDA_OK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         cudaGraph_t graph;
         CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        if (mode == 2) enqueue_bwd_iteration(cap);
-        else if (mode == 5) enqueue_contact_iteration(cap);
-        else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
-        else enqueue_fwd_iteration(mode == 1, cap);
+        enqueue_iteration(mode, cap);
         CUDA_OK(cudaStreamEndCapture(cap, &graph));
         CUDA_OK(cudaGraphGetNodes(graph, nullptr, &graph_nodes_[mode]));
         CUDA_OK(cudaGraphInstantiate(&g, graph, 0));
         CUDA_OK(cudaGraphDestroy(graph));
         CUDA_OK(cudaStreamDestroy(cap));
+        graph_is_while_[mode] = false;
     }
     int launched = 0, chunk = std::min(o.poll_chunk, 4);
     while (launched < o.max_pd_iter) {
@@ -819,7 +927,7 @@ const double* Engine::ws_predict(const double* dq, const double* dv, const doubl
 
 void Engine::ws_features(double dt, const double* dq, const double* dqp, const double* dv, const double* df,
                          const double* d_prev_base, void* X, double* d_base, cudaStream_t st) {
-    DPHD_CHECK(built_ && built_dt_ == dt && device_ready_, "warm start: make one forward call with this dt first");
+    ensure_built(dt, 0);
     if (!d_wlog.p) {
         // log10 of each node's mean PD stiffness over its incident elements
         std::vector<double> acc(M.n, 0.0);
@@ -854,14 +962,14 @@ void Engine::ws_features(double dt, const double* dq, const double* dqp, const d
 }
 
 void Engine::ws_apply(double dt, const double* d_base, const float* out, double* d_q_init, cudaStream_t st) {
-    (void)dt;
+    ensure_built(dt, 0);
     launch_mlp_apply(dofs(), d_base, out, ws_dx(), d_fixed_dof.as<unsigned char>(), d_fixed_val.as<double>(), d_q_init,
                      st);
     launches_ += 1;
 }
 
 void Engine::ws_target(double dt, const double* d_q_next, const double* d_base, float* Y, cudaStream_t st) {
-    (void)dt;
+    ensure_built(dt, 0);
     launch_mlp_target(dofs(), d_q_next, d_base, 1.0 / ws_dx(), Y, st);
     launches_ += 1;
 }

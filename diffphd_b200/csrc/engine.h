@@ -34,6 +34,7 @@ struct Options {
     int bwd_solver = 0;          // 0: Anderson-accelerated fixed point (reference), 1: preconditioned CG
     int bwd_warm_start = 0;      // CG adjoint starts from the previous backward call's solution (reverse sweeps)
     int poll_chunk = 8;
+    int graph_while = 1;         // device-side WHILE graph per solve (0: host polling every poll_chunk iterations)
     static Options parse(const std::map<std::string, double>& m);
 };
 
@@ -157,6 +158,11 @@ private:
     double graph_dt_ = -1, graph_mu_ = 0;
     cudaGraphExec_t graphs_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     size_t graph_nodes_[6] = {0, 0, 0, 0, 0, 0};
+    bool graph_is_while_[6] = {false, false, false, false, false, false};
+    int graph_cap_[6] = {0, 0, 0, 0, 0, 0};
+    bool while_ok_ = true;
+    void enqueue_iteration(int mode, cudaStream_t cap);
+    bool build_while_graph(int mode, int cap_iters);
     ContactDev contact_;
     bool has_contact_ = false;
     NodeCsr Acsr_;
@@ -177,6 +183,7 @@ private:
     DeviceBuffer d_elem_out64, d_elem_out32, d_vperm64, d_vperm32, d_y64, d_y32;
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
+    DeviceBuffer d_item_desc, d_item_slot, d_trow_desc, d_trow_off;
     DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv, d_wlog, d_mu_prev;
     bool mu_prev_valid_ = false;
     const double* ws_predict(const double* d_q, const double* d_v, const double* d_f, double dt, cudaStream_t st);

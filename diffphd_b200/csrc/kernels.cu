@@ -188,6 +188,16 @@ __global__ void __launch_bounds__(kThreads) k_elem_fwd(int m, const int* __restr
     }
 }
 
+// Node gathers run kGatherLanes lanes per node (strided over the node's incident element outputs and its CSR
+// row of A) and combine them with xor shuffles in a fixed order: deterministic, and eight times the memory
+// parallelism of one thread per node on meshes of a few thousand nodes.
+
+template <typename T>
+__device__ __forceinline__ void group_sum(T& a) {
+#pragma unroll
+    for (int o = kGatherLanes / 2; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __restrict__ node_ptr,
                                                          const int* __restrict__ node_inc, const double* __restrict__ eo,
@@ -200,33 +210,45 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
     if (ctrl->done) return;
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double p0 = 0, p1 = 0, p2 = 0;
-        const int b = node_ptr[i], e = node_ptr[i + 1];
-        for (int idx = b; idx < e; ++idx) {
-            const double* c = eo + (size_t)node_inc[idx] * 3;
-            p0 += c[0]; p1 += c[1]; p2 += c[2];
-        }
-        const double p[3] = {p0, p1, p2};
-        const int j = iperm[i];
-        const bool fx = fixed[i] != 0;
-        double aq[3] = {0.0, 0.0, 0.0};
-        if (A.rp && !fx) {
-            for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-                const int c = A.ci[k];
-                const double a = A.v[k];
-                aq[0] += a * q[3 * c];
-                aq[1] += a * q[3 * c + 1];
-                aq[2] += a * q[3 * c + 2];
+    const int lane = threadIdx.x & (kGatherLanes - 1);
+    constexpr int per_block = kThreads / kGatherLanes;
+    for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
+        const int i = base + (int)threadIdx.x / kGatherLanes;
+        const bool valid = i < n;
+        const bool fx = valid ? fixed[i] != 0 : true;
+        double p[3] = {0.0, 0.0, 0.0}, aq[3] = {0.0, 0.0, 0.0};
+        if (valid) {
+            const int b = node_ptr[i], e = node_ptr[i + 1];
+            for (int idx = b + lane; idx < e; idx += kGatherLanes) {
+                const double* c = eo + (size_t)node_inc[idx] * 3;
+                p[0] += c[0]; p[1] += c[1]; p[2] += c[2];
+            }
+            if (A.rp && !fx) {
+                for (int k = A.rp[i] + lane; k < A.rp[i + 1]; k += kGatherLanes) {
+                    const int c = A.ci[k];
+                    const double a = A.v[k];
+                    aq[0] += a * q[3 * c];
+                    aq[1] += a * q[3 * c + 1];
+                    aq[2] += a * q[3 * c + 2];
+                }
             }
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const double pr = prev[3 * i + d];
-            acc[0] += (p[d] - pr) * (p[d] - pr);
-            acc[1] += pr * pr;
-            prev[3 * i + d] = p[d];
-            v[(size_t)d * npad + j] = (fx && zero_dirichlet) ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d] - aq[d]);
+            group_sum(p[d]);
+            group_sum(aq[d]);
+        }
+        if (valid && lane == 0) {
+            const int j = iperm[i];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double pr = prev[3 * i + d];
+                acc[0] += (p[d] - pr) * (p[d] - pr);
+                acc[1] += pr * pr;
+                prev[3 * i + d] = p[d];
+                v[(size_t)d * npad + j] =
+                    (fx && zero_dirichlet) ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d] - aq[d]);
+            }
         }
     }
     block_sum<2>(acc, sh);
@@ -251,6 +273,11 @@ template <> struct Vec4<float> {
         const float4 x = __ldcs(reinterpret_cast<const float4*>(p));
         v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
     }
+    // S values: kept in L2 across iterations when the factor fits there, streamed (evict-first) otherwise
+    __device__ __forceinline__ void load_s(const float* p, int keep) {
+        if (keep) load(p);
+        else load_stream(p);
+    }
 };
 template <> struct Vec4<double> {
     double v[4];
@@ -264,6 +291,10 @@ template <> struct Vec4<double> {
         const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
     }
+    __device__ __forceinline__ void load_s(const double* p, int keep) {
+        if (keep) load(p);
+        else load_stream(p);
+    }
 };
 
 // y = S v, stage 1: one warp per work item (a row segment of <= kSegCols columns), four 16-byte loads of S
@@ -273,9 +304,10 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
     if (ctrl->done) return;
     const int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (it >= p.n_items) return;
-    const int i = __ldg(p.item_row + it), c0 = __ldg(p.item_c0 + it), nc = __ldg(p.item_nc + it);
-    const T* __restrict__ sv = p.vals + __ldg(p.row_off + i) + c0;
-    const int a = __ldg(p.row_a + i) + c0;
+    const int4 dsc = __ldg(p.item_desc + it);
+    const int slot = __ldg(p.item_slot + it);
+    const T* __restrict__ sv = p.vals + ((int64_t)(uint32_t)dsc.x | ((int64_t)dsc.y << 32));
+    const int a = dsc.z, nc = dsc.w;
     const T* __restrict__ v0 = v + a;
     const T* __restrict__ v1 = v + p.npad + a;
     const T* __restrict__ v2 = v + 2 * (size_t)p.npad + a;
@@ -284,7 +316,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
     for (; c + 384 < nc; c += 512) {
         Vec4<T> s[4], x0[4], x1[4], x2[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) s[u].load_stream(sv + c + 128 * u);
+        for (int u = 0; u < 4; ++u) s[u].load_s(sv + c + 128 * u, p.keep_in_l2);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             x0[u].load(v0 + c + 128 * u);
@@ -302,7 +334,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
     }
     for (; c < nc; c += 128) {
         Vec4<T> s, x0, x1, x2;
-        s.load_stream(sv + c);
+        s.load_s(sv + c, p.keep_in_l2);
         x0.load(v0 + c);
         x1.load(v1 + c);
         x2.load(v2 + c);
@@ -317,7 +349,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
     s1 = warp_sum(s1);
     s2 = warp_sum(s2);
     if (lane == 0) {
-        T* o = p.ypart + (size_t)it * 3;
+        T* o = p.ypart + (size_t)slot * 3;
         o[0] = s0; o[1] = s1; o[2] = s2;
     }
 }
@@ -329,8 +361,8 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     T s0 = T(0), s1 = T(0), s2 = T(0);
-    for (int k = __ldg(p.row_item_ptr + i); k < __ldg(p.row_item_ptr + i + 1); ++k) {
-        const T* o = p.ypart + (size_t)__ldg(p.row_items + k) * 3;
+    for (int k = __ldg(p.row_yptr + i); k < __ldg(p.row_yptr + i + 1); ++k) {
+        const T* o = p.ypart + (size_t)k * 3;
         s0 += o[0]; s1 += o[1]; s2 += o[2];
     }
     if (p.y_accumulate) {
@@ -345,8 +377,12 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
 }
 
 // x = S^T y, stage 1: one CTA per (column tile, chunk of the tile's row list); partial tile sums are written
-// to xpart[chunk] and summed in chunk order by stage 2.
-template <typename T>
+// to xpart[chunk] and summed in chunk order by stage 2.  Each warp takes every 8th row of the chunk and keeps
+// kStRows rows in flight.  FROM_ITEMS: y_r is summed here from the S pass's row-contiguous item partials (in
+// slot order, as the S fix-up kernel would), so the pair needs no separate fix-up launch.
+constexpr int kStRows = 4;
+
+template <typename T, bool FROM_ITEMS>
 __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
     if (ctrl->done) return;
     __shared__ T red[8][3][kTileCols];
@@ -360,48 +396,50 @@ __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[d][q] = T(0);
     const int pe = __ldg(p.chunk_p1 + ch);
-    int pp = __ldg(p.chunk_p0 + ch) + wid;
-    for (; pp + 8 < pe; pp += 16) {
-        const int i0 = __ldg(p.tile_rows + pp), i1 = __ldg(p.tile_rows + pp + 8);
-        const int a0 = __ldg(p.row_a + i0), l0 = __ldg(p.row_len + i0);
-        const int a1 = __ldg(p.row_a + i1), l1 = __ldg(p.row_len + i1);
-        const bool in0 = c >= a0 && c + 4 <= a0 + l0, in1 = c >= a1 && c + 4 <= a1 + l1;
-        Vec4<T> s0, s1;
-        if (in0) s0.load_stream(p.vals + __ldg(p.row_off + i0) + (c - a0));
-        if (in1) s1.load_stream(p.vals + __ldg(p.row_off + i1) + (c - a1));
-        const T y00 = __ldg(y + i0), y01 = __ldg(y + npad + i0), y02 = __ldg(y + 2 * (size_t)npad + i0);
-        const T y10 = __ldg(y + i1), y11 = __ldg(y + npad + i1), y12 = __ldg(y + 2 * (size_t)npad + i1);
-        if (in0) {
+    for (int pp = __ldg(p.chunk_p0 + ch) + wid; pp < pe; pp += 8 * kStRows) {
+        int4 dsc[kStRows];
+        int64_t off[kStRows];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                acc[0][q] += s0.v[q] * y00;
-                acc[1][q] += s0.v[q] * y01;
-                acc[2][q] += s0.v[q] * y02;
+        for (int u = 0; u < kStRows; ++u) {
+            const int q = pp + 8 * u;
+            dsc[u] = make_int4(0, 0, 0, 0);
+            off[u] = 0;
+            if (q < pe) {
+                dsc[u] = __ldg(p.trow_desc + q);
+                off[u] = __ldg(p.trow_off + q);
             }
         }
-        if (in1) {
+        Vec4<T> sv[kStRows];
+        T yv[kStRows][3];
+        bool in[kStRows];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                acc[0][q] += s1.v[q] * y10;
-                acc[1][q] += s1.v[q] * y11;
-                acc[2][q] += s1.v[q] * y12;
+        for (int u = 0; u < kStRows; ++u) {
+            in[u] = dsc[u].y > 0 && c >= dsc[u].x && c + 4 <= dsc[u].x + dsc[u].y;
+            if (in[u]) sv[u].load_s(p.vals + off[u] + (c - dsc[u].x), p.keep_in_l2);
+            yv[u][0] = yv[u][1] = yv[u][2] = T(0);
+            if (FROM_ITEMS) {
+                for (int k = dsc[u].z; k < dsc[u].w; ++k) {
+                    yv[u][0] += __ldg(p.ypart + 3 * (size_t)k);
+                    yv[u][1] += __ldg(p.ypart + 3 * (size_t)k + 1);
+                    yv[u][2] += __ldg(p.ypart + 3 * (size_t)k + 2);
+                }
+            } else if (pp + 8 * u < pe) {
+                const int i = __ldg(p.tile_rows + pp + 8 * u);
+                yv[u][0] = __ldg(y + i);
+                yv[u][1] = __ldg(y + npad + i);
+                yv[u][2] = __ldg(y + 2 * (size_t)npad + i);
             }
         }
-    }
-    for (; pp < pe; pp += 8) {
-        const int i = __ldg(p.tile_rows + pp);
-        const int a = __ldg(p.row_a + i), len = __ldg(p.row_len + i);
-        if (c >= a && c + 4 <= a + len) {
-            Vec4<T> sv;
-            sv.load_stream(p.vals + __ldg(p.row_off + i) + (c - a));
-            const T y0 = __ldg(y + i), y1 = __ldg(y + npad + i), y2 = __ldg(y + 2 * (size_t)npad + i);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                acc[0][q] += sv.v[q] * y0;
-                acc[1][q] += sv.v[q] * y1;
-                acc[2][q] += sv.v[q] * y2;
+        for (int u = 0; u < kStRows; ++u)
+            if (in[u]) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    acc[0][q] += sv[u].v[q] * yv[u][0];
+                    acc[1][q] += sv[u].v[q] * yv[u][1];
+                    acc[2][q] += sv[u].v[q] * yv[u][2];
+                }
             }
-        }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d)
@@ -503,52 +541,86 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
         return;
     }
     if (m < 1) return;
-    // extend the stored Gram matrix by the new difference's column
+    // Extend the stored Gram matrix by the new difference's column, then solve
+    // (dG^T dG + reg I) gamma = dG^T g, reg = max(1e-6 |dG|_F^2 / m, 1e-12), by Cholesky.  All loops run to
+    // kMaxWindow with guards so that the small arrays stay in registers; the stored entries are loaded
+    // independently (one round trip) rather than inside the factorisation.
     const int snew = (head + m - 1) % W;
-    for (int j = 0; j < m; ++j) {
-        const int sj = (head + j) % W;
-        ctrl->gram[snew][sj] = tot[j];
-        ctrl->gram[sj][snew] = tot[j];
-    }
-    // (dG^T dG + reg I) gamma = dG^T g, reg = max(1e-6 |dG|_F^2 / m, 1e-12); Cholesky solve.
-    double A[kMaxWindow * kMaxWindow], b[kMaxWindow];
+    double A[kMaxWindow][kMaxWindow], b[kMaxWindow];
+#pragma unroll
+    for (int i = 0; i < kMaxWindow; ++i)
+#pragma unroll
+        for (int j = 0; j < kMaxWindow; ++j)
+            if (i < m && j < m)
+                A[i][j] = (i == m - 1) ? tot[j] : (j == m - 1) ? tot[i] : ctrl->gram[(head + i) % W][(head + j) % W];
+#pragma unroll
+    for (int j = 0; j < kMaxWindow; ++j)
+        if (j < m) {
+            const int sj = (head + j) % W;
+            ctrl->gram[snew][sj] = tot[j];
+            ctrl->gram[sj][snew] = tot[j];
+        }
     double fro = 0;
-    for (int j = 0; j < m; ++j) fro += ctrl->gram[(head + j) % W][(head + j) % W];
+#pragma unroll
+    for (int j = 0; j < kMaxWindow; ++j)
+        if (j < m) fro += A[j][j];
     const double reg = fmax(1e-6 * fro / m, 1e-12);
-    for (int i = 0; i < m; ++i) {
-        for (int j = 0; j < m; ++j) A[i * m + j] = ctrl->gram[(head + i) % W][(head + j) % W];
-        A[i * m + i] += reg;
-        b[i] = tot[kMaxWindow + i];
-    }
-    for (int j = 0; j < m; ++j) {
-        double d = A[j * m + j];
-        for (int k = 0; k < j; ++k) d -= A[j * m + k] * A[j * m + k];
-        d = sqrt(fmax(d, 1e-300));
-        A[j * m + j] = d;
-        for (int i = j + 1; i < m; ++i) {
-            double s = A[i * m + j];
-            for (int k = 0; k < j; ++k) s -= A[i * m + k] * A[j * m + k];
-            A[i * m + j] = s / d;
+#pragma unroll
+    for (int i = 0; i < kMaxWindow; ++i)
+        if (i < m) {
+            A[i][i] += reg;
+            b[i] = tot[kMaxWindow + i];
+        }
+#pragma unroll
+    for (int j = 0; j < kMaxWindow; ++j) {
+        if (j < m) {
+            double d = A[j][j];
+#pragma unroll
+            for (int k = 0; k < kMaxWindow; ++k)
+                if (k < j) d -= A[j][k] * A[j][k];
+            d = sqrt(fmax(d, 1e-300));
+            A[j][j] = d;
+#pragma unroll
+            for (int i = 0; i < kMaxWindow; ++i)
+                if (i > j && i < m) {
+                    double t = A[i][j];
+#pragma unroll
+                    for (int k = 0; k < kMaxWindow; ++k)
+                        if (k < j) t -= A[i][k] * A[j][k];
+                    A[i][j] = t / d;
+                }
         }
     }
-    for (int i = 0; i < m; ++i) {
-        double s = b[i];
-        for (int k = 0; k < i; ++k) s -= A[i * m + k] * b[k];
-        b[i] = s / A[i * m + i];
-    }
-    for (int i = m - 1; i >= 0; --i) {
-        double s = b[i];
-        for (int k = i + 1; k < m; ++k) s -= A[k * m + i] * b[k];
-        b[i] = s / A[i * m + i];
-    }
+#pragma unroll
+    for (int i = 0; i < kMaxWindow; ++i)
+        if (i < m) {
+            double t = b[i];
+#pragma unroll
+            for (int k = 0; k < kMaxWindow; ++k)
+                if (k < i) t -= A[i][k] * b[k];
+            b[i] = t / A[i][i];
+        }
+#pragma unroll
+    for (int i = kMaxWindow - 1; i >= 0; --i)
+        if (i < m) {
+            double t = b[i];
+#pragma unroll
+            for (int k = 0; k < kMaxWindow; ++k)
+                if (k > i && k < m) t -= A[k][i] * b[k];
+            b[i] = t / A[i][i];
+        }
     double gn = 0;
-    for (int i = 0; i < m; ++i) gn += b[i] * b[i];
+#pragma unroll
+    for (int i = 0; i < kMaxWindow; ++i)
+        if (i < m) gn += b[i] * b[i];
     gn = sqrt(gn);
     if (!(gn < 10.0)) {
         ctrl->restart = 1;
     } else {
         ctrl->accept = 1;
-        for (int i = 0; i < m; ++i) ctrl->gamma[i] = b[i];
+#pragma unroll
+        for (int i = 0; i < kMaxWindow; ++i)
+            if (i < m) ctrl->gamma[i] = b[i];
     }
 }
 
@@ -811,17 +883,27 @@ __global__ void __launch_bounds__(kThreads) k_gather_bwd(int n, const int* __res
                                                          const int* __restrict__ iperm, double* __restrict__ v,
                                                          int npad, const Ctrl* ctrl) {
     if (ctrl->done) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & (kGatherLanes - 1);
+    constexpr int per_block = kThreads / kGatherLanes;
+    for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
+        const int i = base + (int)threadIdx.x / kGatherLanes;
+        const bool valid = i < n;
         double p0 = 0, p1 = 0, p2 = 0;
-        for (int idx = node_ptr[i]; idx < node_ptr[i + 1]; ++idx) {
-            const double* c = eo + (size_t)node_inc[idx] * 3;
-            p0 += c[0]; p1 += c[1]; p2 += c[2];
+        if (valid)
+            for (int idx = node_ptr[i] + lane; idx < node_ptr[i + 1]; idx += kGatherLanes) {
+                const double* c = eo + (size_t)node_inc[idx] * 3;
+                p0 += c[0]; p1 += c[1]; p2 += c[2];
+            }
+        group_sum(p0);
+        group_sum(p1);
+        group_sum(p2);
+        if (valid && lane == 0) {
+            const int j = iperm[i];
+            const bool fx = fixed[i] != 0;
+            v[j] = fx ? 0.0 : gbar[3 * i] + p0;
+            v[npad + j] = fx ? 0.0 : gbar[3 * i + 1] + p1;
+            v[2 * (size_t)npad + j] = fx ? 0.0 : gbar[3 * i + 2] + p2;
         }
-        const int j = iperm[i];
-        const bool fx = fixed[i] != 0;
-        v[j] = fx ? 0.0 : gbar[3 * i] + p0;
-        v[npad + j] = fx ? 0.0 : gbar[3 * i + 1] + p1;
-        v[2 * (size_t)npad + j] = fx ? 0.0 : gbar[3 * i + 2] + p2;
     }
 }
 
@@ -940,25 +1022,33 @@ __global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const
     if (ctrl->done) return;
     __shared__ double sh[32];
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (fixed[i]) {
-            w[3 * i] = w[3 * i + 1] = w[3 * i + 2] = 0.0;
-            continue;
-        }
+    const int lane = threadIdx.x & (kGatherLanes - 1);
+    constexpr int per_block = kThreads / kGatherLanes;
+    for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
+        const int i = base + (int)threadIdx.x / kGatherLanes;
+        const bool valid = i < n;
+        const bool fx = valid ? fixed[i] != 0 : true;
         double a0 = 0, a1 = 0, a2 = 0;
-        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-            const int c = A.ci[k];
-            const double a = A.v[k];
-            a0 += a * p[3 * c];
-            a1 += a * p[3 * c + 1];
-            a2 += a * p[3 * c + 2];
+        if (valid && !fx) {
+            for (int k = A.rp[i] + lane; k < A.rp[i + 1]; k += kGatherLanes) {
+                const int c = A.ci[k];
+                const double a = A.v[k];
+                a0 += a * p[3 * c];
+                a1 += a * p[3 * c + 1];
+                a2 += a * p[3 * c + 2];
+            }
+            for (int idx = node_ptr[i] + lane; idx < node_ptr[i + 1]; idx += kGatherLanes) {
+                const double* c = eo + (size_t)node_inc[idx] * 3;
+                a0 -= c[0]; a1 -= c[1]; a2 -= c[2];
+            }
         }
-        for (int idx = node_ptr[i]; idx < node_ptr[i + 1]; ++idx) {
-            const double* c = eo + (size_t)node_inc[idx] * 3;
-            a0 -= c[0]; a1 -= c[1]; a2 -= c[2];
+        group_sum(a0);
+        group_sum(a1);
+        group_sum(a2);
+        if (valid && lane == 0) {
+            w[3 * i] = a0; w[3 * i + 1] = a1; w[3 * i + 2] = a2;  // zero on Dirichlet nodes
+            acc[0] += a0 * p[3 * i] + a1 * p[3 * i + 1] + a2 * p[3 * i + 2];
         }
-        w[3 * i] = a0; w[3 * i + 1] = a1; w[3 * i + 2] = a2;
-        acc[0] += a0 * p[3 * i] + a1 * p[3 * i + 1] + a2 * p[3 * i + 2];
     }
     block_sum<1>(acc, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
@@ -1198,8 +1288,12 @@ void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const do
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
     k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
-    k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
-    k_spmv_ST_part<T><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
+    if (p.y_accumulate) {
+        k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
+        k_spmv_ST_part<T, false><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
+    } else {
+        k_spmv_ST_part<T, true><<<p.n_chunks, 256, 0, st>>>(p, nullptr, ctrl);
+    }
     k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
 }
 
@@ -1246,8 +1340,9 @@ void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const d
 void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* gbar,
                        const unsigned char* fixed_node, const int* iperm, double* v_perm, int npad, const Ctrl* ctrl,
                        cudaStream_t st) {
-    k_gather_bwd<<<kRedBlocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm,
-                                                 npad, ctrl);
+    const int blocks = std::max(1, std::min(kMaxRedBlocks, (n * kGatherLanes + kThreads - 1) / kThreads));
+    k_gather_bwd<<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm, npad,
+                                              ctrl);
 }
 
 void launch_param_grad(int m, int k, int s, const int* E, const double* q, const double* mu, const double* grad,
@@ -1329,13 +1424,23 @@ void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cud
 }
 template <typename T>
 void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
-    k_spmv_ST_part<T><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
+    k_spmv_ST_part<T, false><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
     k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
 }
 template void launch_s_only<double>(const SpmvPlan<double>&, const double*, double*, const Ctrl*, cudaStream_t);
 template void launch_s_only<float>(const SpmvPlan<float>&, const float*, float*, const Ctrl*, cudaStream_t);
 template void launch_st_only<double>(const SpmvPlan<double>&, const double*, double*, const Ctrl*, cudaStream_t);
 template void launch_st_only<float>(const SpmvPlan<float>&, const float*, double*, const Ctrl*, cudaStream_t);
+
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap) {
+    const int loops = ctrl->loops + 1;
+    ctrl->loops = loops;
+    cudaGraphSetConditional(h, (!ctrl->done && loops < cap) ? 1u : 0u);
+}
+
+void launch_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap, cudaStream_t st) {
+    k_loop_cond<<<1, 1, 0, st>>>(h, ctrl, cap);
+}
 
 template void launch_sts<double>(const SpmvPlan<double>&, const double*, double*, double*, const Ctrl*,
                                  cudaStream_t);

@@ -33,6 +33,7 @@ struct Ctrl {
     double rz, alpha, beta;              // conjugate-gradient scalars of the adjoint solve
     int pcg_init;
     unsigned int arrive[4];
+    int loops;  // iterations run by the device-side while loop (k_loop_cond)
 };
 
 struct EnergyPack {
@@ -68,11 +69,17 @@ struct SpmvPlan {
     const int* row_a = nullptr;
     const int* row_len = nullptr;
     const T* vals = nullptr;
+    int keep_in_l2 = 0;  // S fits comfortably in L2: ordinary cached loads instead of evict-first streaming
     // y = S v: work items (row, first column, column count) of at most kSegCols columns, one warp each;
     // items of the same nested-dissection separator and column segment are adjacent so that the warps of
     // one CTA read the same slice of v (L1 reuse).  Partial sums ypart[item][3] are summed per row in item
     // order by the fix-up kernel (rows own items [row_item_ptr[r], row_item_ptr[r+1]) via row_items).
     int n_items = 0;
+    const int4* item_desc = nullptr;    // per item: S offset of its first value (lo, hi words), first column, count
+    const int* item_slot = nullptr;     // per item: its slot in ypart; row r owns slots [row_yptr[r], row_yptr[r+1])
+    const int* row_yptr = nullptr;
+    const int4* trow_desc = nullptr;    // per S^T tile-row position: first column, length, slot range of the row
+    const int64_t* trow_off = nullptr;  // per S^T tile-row position: S offset of the row's first value
     const int* item_row = nullptr;
     const int* item_c0 = nullptr;
     const int* item_nc = nullptr;
@@ -93,6 +100,7 @@ struct SpmvPlan {
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kChunkRows = 64;       // rows per S^T chunk CTA
+constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
@@ -182,6 +190,10 @@ template <typename T>
 void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st);
 template <typename T>
 void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
+
+// Device-side loop control of a graph WHILE node: counts the iteration and keeps looping while the gate has
+// not set `done` and fewer than `cap` iterations ran (cap > max_iter: a bound even if a gate kernel is skipped).
+void launch_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap, cudaStream_t st);
 
 // Learned warm start (mlp.cu) -----------------------------------------------------------------------
 struct FeatureArgs {

@@ -157,8 +157,8 @@ int dphd_mlp_train_step(float* d_master, void* d_packed, const void* d_X, const 
 /* Features of every node for one step (BF16 [n][16]: (q - X)/dx, (q - q_prev)/dx, the previous step's
  * correction (q - q_tilde_prev)/dx (zero when d_prev_base is null), h^2 f_ext/(m dx), signed height above the
  * contact plane / dx, log10(mean stiffness)/7, Dirichlet flag, 0) and the inertial prediction
- * q_tilde = q + h v + h^2/m (f_ext + m g) (3n FP64, d_base).  dx = cube root of the mean element volume.  The
- * handle must have made one forward call with this dt. */
+ * q_tilde = q + h v + h^2/m (f_ext + m g) (3n FP64, d_base).  dx = cube root of the mean element volume.  Builds
+ * the handle's factor for this dt first if no forward call has. */
 int dphd_warmstart_features(dphd_deformable* h, double dt, const double* d_q, const double* d_q_prev,
                             const double* d_v, const double* d_f, const double* d_prev_base, void* d_X,
                             double* d_base, void* stream);
