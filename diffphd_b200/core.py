@@ -84,6 +84,7 @@ def load_library():
                                            C.c_double] + kv + [C.c_void_p] * 4
     L.dphd_mlp_sizes.argtypes = [_ip, _ip, _ip, _ip]
     L.dphd_set_warm_start_network.argtypes = [C.c_void_p] * 3
+    L.dphd_contact_adjoint_stats.argtypes = [C.c_void_p, _ip, _ip, _ip]
     L.dphd_mlp_pack.argtypes = [C.c_void_p] * 3
     L.dphd_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.dphd_mlp_train_step.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_void_p] + [C.c_float] * 5 + \
@@ -342,6 +343,13 @@ class Deformable:
         cv = np.zeros(max(nf, 1), np.int32)
         self._check(self._L.dphd_frame_stats(self._h, _iptr(it), _iptr(cv)))
         return it[:nf].copy(), cv[:nf].copy()
+
+    def contact_adjoint_stats(self):
+        """(source, constraints, cg_iters) of the last backward's contact-aware material adjoint: source 0 none,
+        1 forward tape, 2 replayed forward step, 3 tape miss without replay inputs."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(self._L.dphd_contact_adjoint_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def reset_frame_stats(self):
         self._check(self._L.dphd_reset_frame_stats(self._h))

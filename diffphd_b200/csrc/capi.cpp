@@ -388,6 +388,15 @@ int dphd_reset_frame_stats(dphd_deformable* h) {
     });
 }
 int dphd_last_backward_iters(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.last_bwd_iters : -1; }
+int dphd_contact_adjoint_stats(const dphd_deformable* h, int* source, int* constraints, int* iters) {
+    return guard([&] {
+        DPHD_CHECK(h && h->eng, "null handle");
+        const auto& st = h->eng->stats;
+        if (source) *source = st.contact_source;
+        if (constraints) *constraints = st.contact_constraints;
+        if (iters) *iters = st.contact_iters;
+    });
+}
 long long dphd_s_memory_bytes(const dphd_deformable* h) { return h && h->eng ? h->eng->s_memory_bytes() : -1; }
 long long dphd_s_nnz(const dphd_deformable* h) { return h && h->eng ? h->eng->s_nnz() : -1; }
 

@@ -58,6 +58,12 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.fp32_bulk = (int)get("fp32_bulk", 0);
     o.bwd_solver = (int)get("alg_phd_bwd_solver", 0);
     o.bwd_warm_start = (int)get("alg_phd_bwd_warm_start", 0);
+    o.skip_woodbury = get("skip_contact_woodbury", 0) > 0.5;
+    o.skip_material_grad = get("skip_material_grad", 0) > 0.5;
+    o.tangent_lambda_min = get("alg_phd_bwd_tangent_lambda_min", 1e-8);
+    o.rhs_prune_rel = get("alg_phd_bwd_rhs_prune_rel", 1e-3);
+    o.rhs_prune_abs = get("alg_phd_bwd_rhs_prune_abs", 1e-12);
+    o.basis_topk = (int)get("alg_phd_bwd_basis_topk", 0);
     o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
     o.graph_while = (int)get("graph_while", 1);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
@@ -682,14 +688,18 @@ void Engine::enqueue_bwd_iteration(cudaStream_t st) {
 }
 
 // One conjugate-gradient iteration of the adjoint (A - K_pd) mu = g_bar, preconditioned by S^T S.
-void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st) {
+void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected) {
     const int n = M.n, n3 = 3 * n;
     Ctrl* c = d_ctrl.as<Ctrl>();
+    const int capK = has_contact_ ? contact_.K : 0;
     launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_pp.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
                     d_elem_out64.as<double>(), c, st);
     launch_pcg_gather(n, Acsr_, d_pp.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
                       d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
                       d_part_gate.as<double>(), gather_blocks_, c, st);
+    if (projected)  // w = P (A - K_pd) p  (p lies in range(P), so p.w above is unchanged)
+        launch_wb_project<double>(capK, d_wb_count.as<int>(), d_wb_nodes.as<int>(), d_wb_dirs.as<double>(),
+                                  d_wb_ndir.as<int>(), d_wv.as<double>(), nullptr, nullptr, npad_, c, st);
     if (f32)
         launch_pcg_update1<float>(n, d_x.as<double>(), d_r.as<double>(), d_pp.as<double>(), d_wv.as<double>(),
                                   d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm32.as<float>(), npad_,
@@ -699,6 +709,9 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st) {
                                    d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_,
                                    d_part_upd.as<double>(), gather_blocks_, c, st);
     launch_ainv(f32, st);
+    if (projected)  // z = P A^-1 P r
+        launch_wb_project<double>(capK, d_wb_count.as<int>(), d_wb_nodes.as<int>(), d_wb_dirs.as<double>(),
+                                  d_wb_ndir.as<int>(), d_xraw.as<double>(), nullptr, nullptr, npad_, c, st);
     launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
                        gather_blocks_, red_blocks_, c, st);
     launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
@@ -713,6 +726,7 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st) {
 void Engine::enqueue_iteration(int mode, cudaStream_t cap) {
     if (mode == 2) enqueue_bwd_iteration(cap);
     else if (mode == 5) enqueue_contact_iteration(cap);
+    else if (mode == 6 || mode == 7) enqueue_pcg_iteration(mode == 7, cap, true);
     else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
     else enqueue_fwd_iteration(mode == 1, cap);
 }
@@ -884,6 +898,7 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
         launch_restitution(contact_, d_x.as<double>(), dq, dv, dt, o.restitution, o.contact_slop, st);
         launches_ += 1;
     }
+    if (has_contact_) tape_push(d_x.as<double>(), st);
     CUDA_OK(cudaMemcpyAsync(dqn, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     launch_velocity(n3, d_x.as<double>(), dq, 1.0 / dt, dvn, st);
     launches_ += 2;
@@ -995,11 +1010,243 @@ void Engine::forward(const double* q, const double* v, const double* f_ext, doub
     }
 }
 
+// ---- forward contact tape (forward_gpu.cpp:1547-1593; backward_gpu.cpp:716-742) -----------------------------
+void Engine::tape_push(const double* d_qn, cudaStream_t st) {
+    const int n3 = 3 * M.n, K = contact_.K;
+    std::unique_ptr<TapeFrame> fr;
+    if (!tape_free_.empty()) {
+        fr = std::move(tape_free_.back());
+        tape_free_.pop_back();
+    } else {
+        fr.reset(new TapeFrame());
+    }
+    fr->q_sol.alloc(n3 * sizeof(double));
+    fr->lam.alloc((size_t)K * sizeof(double));
+    fr->omega.alloc((size_t)K * sizeof(double));
+    CUDA_OK(cudaMemcpyAsync(fr->q_sol.p, d_qn, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(fr->lam.p, dc_lam.p, K * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(fr->omega.p, dc_omega.p, K * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    tape_.push_back(std::move(fr));
+    if (tape_.size() > 8192) {
+        tape_free_.push_back(std::move(tape_.front()));
+        tape_.pop_front();
+    }
+}
+
+// Pops the newest frame when its q_sol matches q_next (relative 1e-8); clears the tape on a clear mismatch
+// (relative > 1e-6), as the reference does.
+bool Engine::tape_take(const double* d_qn, std::unique_ptr<TapeFrame>& out, cudaStream_t st) {
+    if (tape_.empty()) return false;
+    const int n3 = 3 * M.n;
+    d_cmp.alloc(4 * sizeof(double));
+    if (!h_cmp_) CUDA_OK(cudaMallocHost(&h_cmp_, 4 * sizeof(double)));
+    launch_diff_norms(n3, tape_.back()->q_sol.as<double>(), d_qn, d_cmp.as<double>(), st);
+    CUDA_OK(cudaMemcpyAsync(h_cmp_, d_cmp.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double denom = std::max(1.0, std::max(std::sqrt(h_cmp_[1]), std::sqrt(h_cmp_[2])));
+    const double rel = std::sqrt(h_cmp_[0]) / denom;
+    if (rel <= 1e-8) {
+        out = std::move(tape_.back());
+        tape_.pop_back();
+        return true;
+    }
+    if (rel > 1e-6) {
+        while (!tape_.empty()) {
+            tape_free_.push_back(std::move(tape_.back()));
+            tape_.pop_back();
+        }
+    }
+    return false;
+}
+
+// Replays the forward step from (q, v, f_ext) to regenerate the contact frame of a tape miss.  The lambda warm
+// start, the frame statistics and the learned-start state are left as they were.
+void Engine::replay_step(const double* dq, const double* dv, const double* df, double dt, const Options& o,
+                         cudaStream_t st) {
+    const int n3 = 3 * M.n, K = contact_.K;
+    std::vector<double> lam(K);
+    CUDA_OK(cudaMemcpyAsync(lam.data(), dc_lam.p, K * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const size_t nf = stats.frame_iters.size();
+    const bool net = ws_net_;
+    ws_net_ = false;
+    d_rq.alloc(n3 * sizeof(double));
+    d_rv.alloc(n3 * sizeof(double));
+    forward_device_init(dq, dv, df, dt, o, nullptr, d_rq.as<double>(), d_rv.as<double>(), st);
+    ws_net_ = net;
+    stats.frame_iters.resize(nf);
+    stats.frame_converged.resize(nf);
+    CUDA_OK(cudaMemcpyAsync(dc_lam.p, lam.data(), K * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+}
+
+// Contact-aware adjoint for the material gradients (backward_gpu.cpp:937-1208).  The reference forms
+// z_q = mu - W_T G_T^-1 J mu with W_T[k] = (A - K_pd)^-1 j_k from one fixed-point solve per basis vector.  That is
+// the (A - K_pd)-orthogonal projection of mu onto {z : J z = 0}, i.e. the adjoint system solved with the selected
+// contact directions held at zero:  P (A - K_pd) P z = P g_bar,  z in range(P),  P = I - sum_k d_k d_k^T per node.
+// It is solved here by one conjugate-gradient run (preconditioner P S^T S P, started from P mu) instead of one
+// solve per constraint.  Selection (omega >= 0.5, tangents when friction_mu > 0 and lambda above the threshold,
+// right-hand-side pruning, top-k) follows the reference.  d_x holds mu on entry and z_q on exit.
+void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t st) {
+    const int K = contact_.K, n = M.n, n3 = 3 * n;
+    stats.contact_constraints = 0;
+    stats.contact_iters = 0;
+    d_wb_gath.alloc((size_t)3 * K * sizeof(double));
+    launch_gather_nodes(K, dc_cand.as<int>(), d_x.as<double>(), d_wb_gath.as<double>(), st);
+    std::vector<double> muc(3 * (size_t)K), lam(K), om(K);
+    CUDA_OK(cudaMemcpyAsync(muc.data(), d_wb_gath.p, muc.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(lam.data(), fr.lam.p, K * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(om.data(), fr.omega.p, K * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double* nrm = M.plane_n;
+    // tangent basis of the backward (backward_gpu.cpp:958-981)
+    int axis = 0;
+    for (int d = 1; d < 3; ++d)
+        if (std::fabs(nrm[d]) < std::fabs(nrm[axis])) axis = d;
+    double e[3] = {0, 0, 0};
+    e[axis] = 1;
+    const double ne = nrm[0] * e[0] + nrm[1] * e[1] + nrm[2] * e[2];
+    double t1[3] = {e[0] - ne * nrm[0], e[1] - ne * nrm[1], e[2] - ne * nrm[2]};
+    const double l1 = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    if (l1 > 1e-12) for (double& x : t1) x /= l1;
+    else { t1[0] = 1; t1[1] = 0; t1[2] = 0; }
+    double t2[3] = {nrm[1] * t1[2] - nrm[2] * t1[1], nrm[2] * t1[0] - nrm[0] * t1[2], nrm[0] * t1[1] - nrm[1] * t1[0]};
+    const double l2 = std::sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+    if (l2 > 1e-12) for (double& x : t2) x /= l2;
+    else { t2[0] = 0; t2[1] = 1; t2[2] = 0; }
+    const double* dirs3[3] = {nrm, t1, t2};
+    const bool tang = o.friction_mu > 0;
+    struct Basis { int k, b; };
+    std::vector<Basis> full;
+    for (int k = 0; k < K; ++k) {  // the frame's active set: lambda > 0
+        if (!(lam[k] > 0) || om[k] < 0.5) continue;
+        full.push_back({k, 0});
+        if (tang && lam[k] > o.tangent_lambda_min) {
+            full.push_back({k, 1});
+            full.push_back({k, 2});
+        }
+    }
+    const int nbf = (int)full.size();
+    std::vector<double> rfull(nbf);
+    double rmax = 0;
+    for (int i = 0; i < nbf; ++i) {
+        const double* d = dirs3[full[i].b];
+        const double sc = full[i].b == 0 ? om[full[i].k] : 1.0;
+        const double* u = &muc[3 * (size_t)full[i].k];
+        rfull[i] = sc * (d[0] * u[0] + d[1] * u[1] + d[2] * u[2]);
+        rmax = std::max(rmax, std::fabs(rfull[i]));
+    }
+    const double gate = std::max(o.rhs_prune_abs, o.rhs_prune_rel * rmax);
+    std::vector<int> sel;
+    for (int i = 0; i < nbf; ++i)
+        if (std::fabs(rfull[i]) >= gate) sel.push_back(i);
+    if (o.basis_topk > 0 && (int)sel.size() > o.basis_topk) {
+        std::nth_element(sel.begin(), sel.begin() + o.basis_topk, sel.end(),
+                         [&](int a, int b) { return std::fabs(rfull[a]) > std::fabs(rfull[b]); });
+        sel.resize(o.basis_topk);
+    }
+    if (sel.empty()) return;
+    // per constrained node: its selected directions (orthonormal: n, t1, t2)
+    std::map<int, std::vector<int>> per;
+    for (int i : sel) per[full[i].k].push_back(full[i].b);
+    std::vector<int> nodes, ndir;
+    std::vector<double> dirs;
+    for (const auto& kv : per) {
+        if (M.dirichlet.count(3 * M.contact_nodes[kv.first])) continue;  // a fixed node has no free direction
+        nodes.push_back(M.contact_nodes[kv.first]);
+        ndir.push_back((int)kv.second.size());
+        for (int j = 0; j < 3; ++j)
+            for (int d = 0; d < 3; ++d)
+                dirs.push_back(j < (int)kv.second.size() ? dirs3[kv.second[j]][d] : 0.0);
+    }
+    const int count = (int)nodes.size();
+    stats.contact_constraints = (int)sel.size();
+    if (count == 0) return;
+    d_wb_nodes.alloc((size_t)K * sizeof(int));
+    d_wb_ndir.alloc((size_t)K * sizeof(int));
+    d_wb_dirs.alloc((size_t)9 * K * sizeof(double));
+    d_wb_count.alloc(sizeof(int));
+    CUDA_OK(cudaMemcpyAsync(d_wb_nodes.p, nodes.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_wb_ndir.p, ndir.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_wb_dirs.p, dirs.data(), dirs.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d_wb_count.p, &count, sizeof(int), cudaMemcpyHostToDevice, st));
+    // keep mu: the fallback when the projected system shows negative curvature
+    d_wb_mu.alloc(n3 * sizeof(double));
+    CUDA_OK(cudaMemcpyAsync(d_wb_mu.p, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    const bool f32 = o.fp32_bulk != 0;
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
+    h_ctrl_->pcg_init = 1;
+    CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemsetAsync(d_pp.p, 0, n3 * sizeof(double), st));
+    auto proj = [&](double* u, void* vperm) {
+        if (f32)
+            launch_wb_project<float>(K, d_wb_count.as<int>(), d_wb_nodes.as<int>(), d_wb_dirs.as<double>(),
+                                     d_wb_ndir.as<int>(), u, reinterpret_cast<float*>(vperm), d_iperm.as<int>(),
+                                     npad_, c, st);
+        else
+            launch_wb_project<double>(K, d_wb_count.as<int>(), d_wb_nodes.as<int>(), d_wb_dirs.as<double>(),
+                                      d_wb_ndir.as<int>(), u, reinterpret_cast<double*>(vperm), d_iperm.as<int>(),
+                                      npad_, c, st);
+    };
+    proj(d_x.as<double>(), nullptr);  // z_0 = P mu
+    launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
+                    d_elem_out64.as<double>(), c, st);
+    launch_pcg_gather(n, Acsr_, d_x.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
+                      d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
+                      d_part_gate.as<double>(), gather_blocks_, c, st, 1);
+    proj(d_wv.as<double>(), nullptr);
+    void* vp = f32 ? d_vperm32.p : d_vperm64.p;
+    if (f32)
+        launch_pcg_init<float>(n, d_gbar.as<double>(), d_wv.as<double>(), d_fixed_node.as<unsigned char>(),
+                               d_iperm.as<int>(), d_r.as<double>(), d_vperm32.as<float>(), npad_, st);
+    else
+        launch_pcg_init<double>(n, d_gbar.as<double>(), d_wv.as<double>(), d_fixed_node.as<unsigned char>(),
+                                d_iperm.as<int>(), d_r.as<double>(), d_vperm64.as<double>(), npad_, st);
+    proj(d_r.as<double>(), vp);  // r_0 = P (g_bar - (A - K_pd) z_0)
+    launch_ainv(f32, st);
+    proj(d_xraw.as<double>(), nullptr);
+    launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
+                       gather_blocks_, red_blocks_, c, st);
+    launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
+    launches_ += 12;
+    run_iterations(f32 ? 7 : 6, o, st);
+    stats.contact_iters = h_ctrl_->iter;
+    if (h_ctrl_->status & (kStatusIndefinite | kStatusNonFinite | kStatusDiverged)) {
+        CUDA_OK(cudaMemcpyAsync(d_x.p, d_wb_mu.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        stats.bwd_fallbacks++;
+    }
+}
+
 void Engine::backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt,
                              const Options& o, double* d_dq, double* d_dv, double* d_df, double* d_dmat_w,
                              double* d_dparams, double* d_dstate_p, cudaStream_t st) {
+    backward_core(d_q_next, d_gq, d_gv, dt, o, d_dq, d_dv, d_df, d_dmat_w, d_dparams, d_dstate_p, st, nullptr,
+                  nullptr, nullptr);
+}
+
+void Engine::backward_core(const double* d_q_next, const double* d_gq, const double* d_gv, double dt,
+                           const Options& o, double* d_dq, double* d_dv, double* d_df, double* d_dmat_w,
+                           double* d_dparams, double* d_dstate_p, cudaStream_t st, const double* d_q,
+                           const double* d_v, const double* d_f) {
     ensure_built(dt, o.thread_ct);
     const int n3 = 3 * M.n, m = M.m;
+    // the contact frame of this step (tape, or a replayed forward step), before anything below uses d_x
+    std::unique_ptr<TapeFrame> frame;
+    stats.contact_source = 0;
+    stats.contact_constraints = stats.contact_iters = 0;
+    if (has_contact_ && !o.skip_material_grad && !o.skip_woodbury) {
+        if (tape_take(d_q_next, frame, st)) {
+            stats.contact_source = 1;
+        } else if (d_q && d_v && d_f) {
+            replay_step(d_q, d_v, d_f, dt, o, st);
+            frame = std::move(tape_.back());
+            tape_.pop_back();
+            stats.contact_source = 2;
+        } else {
+            stats.contact_source = 3;
+        }
+    }
     const double h = dt, mass = M.mass(), inv_h2m = mass / (h * h), h2m = h * h / mass;
     const EnergyPack ep = energy_pack();
     const double vol_over_s = M.vol / M.s;
@@ -1033,7 +1280,7 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
                             d_J.as<double>(), d_elem_out64.as<double>(), c, st);
             launch_pcg_gather(M.n, Acsr_, d_x.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
                               d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
-                              d_part_gate.as<double>(), gather_blocks_, c, st);
+                              d_part_gate.as<double>(), gather_blocks_, c, st, 1);
             w0 = d_wv.as<double>();
             launches_ += 2;
         }
@@ -1067,6 +1314,7 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
     const int ne = (int)M.energies.size(), np = num_pd_params();
     const bool diverged = (h_ctrl_->status & (kStatusDiverged | kStatusNonFinite)) != 0;
     if (diverged) {  // reference: a diverged backbone contributes nothing downstream (backward_gpu.cpp:873-880)
+        if (frame) tape_free_.push_back(std::move(frame));
         CUDA_OK(cudaMemsetAsync(d_dv, 0, n3 * sizeof(double), st));
         CUDA_OK(cudaMemsetAsync(d_df, 0, n3 * sizeof(double), st));
         if (d_dmat_w && ne) CUDA_OK(cudaMemsetAsync(d_dmat_w, 0, ne * sizeof(double), st));
@@ -1083,6 +1331,17 @@ void Engine::backward_device(const double* d_q_next, const double* d_gq, const d
                      o.bwd_cascade_cap, M.has_gravity ? 1 : 0, d_dq, d_dv, d_df,
                      d_dstate_p ? d_dstate_p : d_dstate_dev.as<double>(), d_part_adj.as<double>(),
                      reinterpret_cast<unsigned int*>(d_adjnorm.as<double>() + 1), st);
+    if (o.skip_material_grad) {
+        if (frame) tape_free_.push_back(std::move(frame));
+        if (d_dmat_w && ne) CUDA_OK(cudaMemsetAsync(d_dmat_w, 0, ne * sizeof(double), st));
+        if (d_dparams && np) CUDA_OK(cudaMemsetAsync(d_dparams, 0, np * sizeof(double), st));
+        CUDA_OK(cudaGetLastError());
+        return;
+    }
+    if (frame) {  // d_x: mu -> z_q (the routing above already read mu, in stream order)
+        contact_adjoint(o, *frame, st);
+        tape_free_.push_back(std::move(frame));
+    }
     d_gw.alloc((size_t)kMaxEnergies * m * sizeof(double));
     d_gmat.alloc((size_t)kMaxEnergies * m * sizeof(double));
     d_gnh.alloc((size_t)kMaxEnergies * m * 2 * sizeof(double));
@@ -1099,16 +1358,23 @@ void Engine::backward(const double* q, const double* v, const double* f_ext, dou
                       const double* v_next, const double* dl_dq_next, const double* dl_dv_next, const Options& o,
                       double* dl_dq, double* dl_dv, double* dl_df, double* dl_dmat_w, double* dl_dparams,
                       double* dl_dstate_p) {
-    (void)q; (void)v; (void)f_ext; (void)v_next;
+    (void)v_next;
     ensure_built(dt, o.thread_ct);
     const int n3 = dofs();
     cudaStream_t st = stream_;
     CUDA_OK(cudaMemcpyAsync(d_qn.p, q_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
     CUDA_OK(cudaMemcpyAsync(d_gq.p, dl_dq_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
     CUDA_OK(cudaMemcpyAsync(d_gv.p, dl_dv_next, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
-    backward_device(d_qn.as<double>(), d_gq.as<double>(), d_gv.as<double>(), dt, o, d_dq.as<double>(),
-                    d_dv.as<double>(), d_df.as<double>(), d_dmat_dev.as<double>(), d_dpar_dev.as<double>(),
-                    d_dstate_dev.as<double>(), st);
+    const bool replayable = has_contact_ && q && v && f_ext;
+    if (replayable) {  // inputs of a possible replay of the forward step (a tape miss)
+        CUDA_OK(cudaMemcpyAsync(d_q.p, q, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d_v.p, v, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d_f.p, f_ext, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    backward_core(d_qn.as<double>(), d_gq.as<double>(), d_gv.as<double>(), dt, o, d_dq.as<double>(),
+                  d_dv.as<double>(), d_df.as<double>(), d_dmat_dev.as<double>(), d_dpar_dev.as<double>(),
+                  d_dstate_dev.as<double>(), st, replayable ? d_q.as<double>() : nullptr,
+                  replayable ? d_v.as<double>() : nullptr, replayable ? d_f.as<double>() : nullptr);
     const int ne = (int)M.energies.size(), np = num_pd_params();
     CUDA_OK(cudaMemcpyAsync(dl_dq, d_dq.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaMemcpyAsync(dl_dv, d_dv.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));

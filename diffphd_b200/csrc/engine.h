@@ -3,7 +3,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <deque>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -33,6 +35,9 @@ struct Options {
     int fp32_bulk = 0;           // projection and S/S^T SpMVs in FP32
     int bwd_solver = 0;          // 0: Anderson-accelerated fixed point (reference), 1: preconditioned CG
     int bwd_warm_start = 0;      // CG adjoint starts from the previous backward call's solution (reverse sweeps)
+    // contact-aware material adjoint (backward_gpu.cpp:937-1208)
+    int skip_woodbury = 0, skip_material_grad = 0, basis_topk = 0;
+    double tangent_lambda_min = 1e-8, rhs_prune_rel = 1e-3, rhs_prune_abs = 1e-12;
     int poll_chunk = 8;
     int graph_while = 1;         // device-side WHILE graph per solve (0: host polling every poll_chunk iterations)
     static Options parse(const std::map<std::string, double>& m);
@@ -58,6 +63,15 @@ struct DeviceBuffer {
 struct StepStats {
     std::vector<int> frame_iters, frame_converged;
     int last_bwd_iters = 0, last_filtered = 0, bwd_fallbacks = 0;
+    // last backward's contact-aware material adjoint: frame source (0 no contact / skipped by option,
+    // 1 forward tape, 2 replayed forward step, 3 tape miss without replay inputs), constraints, CG iterations
+    int contact_source = 0, contact_constraints = 0, contact_iters = 0;
+};
+
+// One forward contact frame kept for the adjoint (the reference's AlgPhdReplayCache): the step's output and,
+// per candidate, the final normal multiplier and the last NCP iteration's omega.
+struct TapeFrame {
+    DeviceBuffer q_sol, lam, omega;
 };
 
 class Engine {
@@ -140,7 +154,20 @@ private:
     void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st,
                           const double* d_init = nullptr);
     void launch_ainv(bool fp32, cudaStream_t st, const double* x_base = nullptr);  // d_vperm -> d_xraw
-    void enqueue_pcg_iteration(bool fp32, cudaStream_t st);
+    void enqueue_pcg_iteration(bool fp32, cudaStream_t st, bool projected = false);
+    void backward_core(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,
+                       double* d_dq, double* d_dv, double* d_df, double* d_dmat_w, double* d_dparams,
+                       double* d_dstate_p, cudaStream_t st, const double* d_q, const double* d_v, const double* d_f);
+    // forward contact tape
+    std::deque<std::unique_ptr<TapeFrame>> tape_;
+    std::vector<std::unique_ptr<TapeFrame>> tape_free_;
+    void tape_push(const double* d_q_next, cudaStream_t st);
+    bool tape_take(const double* d_q_next, std::unique_ptr<TapeFrame>& out, cudaStream_t st);
+    void replay_step(const double* d_q, const double* d_v, const double* d_f, double dt, const Options& o,
+                     cudaStream_t st);
+    void contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t st);
+    DeviceBuffer d_wb_nodes, d_wb_dirs, d_wb_ndir, d_wb_count, d_wb_gath, d_wb_mu, d_cmp, d_rq, d_rv;
+    double* h_cmp_ = nullptr;
     void enqueue_contact_iteration(cudaStream_t st);
     void build_contact(double dt);
     void enqueue_fwd_iteration(bool fp32, cudaStream_t st);
@@ -156,10 +183,12 @@ private:
     NodeMatrix A;
     int npad_ = 0, ntiles_ = 0, red_blocks_ = 1, gather_blocks_ = 1;
     double graph_dt_ = -1, graph_mu_ = 0;
-    cudaGraphExec_t graphs_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    size_t graph_nodes_[6] = {0, 0, 0, 0, 0, 0};
-    bool graph_is_while_[6] = {false, false, false, false, false, false};
-    int graph_cap_[6] = {0, 0, 0, 0, 0, 0};
+    // 0 fwd64, 1 fwd mixed, 2 adjoint fixed point, 3/4 CG adjoint f64/f32, 5 contact, 6/7 projected CG f64/f32
+    static constexpr int kModes = 8;
+    cudaGraphExec_t graphs_[kModes] = {};
+    size_t graph_nodes_[kModes] = {};
+    bool graph_is_while_[kModes] = {};
+    int graph_cap_[kModes] = {};
     bool while_ok_ = true;
     void enqueue_iteration(int mode, cudaStream_t cap);
     bool build_while_graph(int mode, int cap_iters);

@@ -1018,7 +1018,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const
                                                          const double* __restrict__ eo,
                                                          const unsigned char* __restrict__ fixed,
                                                          double* __restrict__ w, double* __restrict__ part,
-                                                         Ctrl* ctrl) {
+                                                         Ctrl* ctrl, int init) {
     if (ctrl->done) return;
     __shared__ double sh[32];
     double acc[1] = {0.0};
@@ -1050,6 +1050,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const
             acc[0] += a0 * p[3 * i] + a1 * p[3 * i + 1] + a2 * p[3 * i + 2];
         }
     }
+    if (init) return;  // w = (A - K_pd) x0 for a start vector: no step length, no curvature test
     block_sum<1>(acc, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
     if (!arrive_last(&ctrl->arrive[2])) return;
@@ -1367,8 +1368,86 @@ template void launch_gather_fwd<float>(int, const int*, const int*, const double
 
 void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
                        const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
-                       Ctrl* ctrl, cudaStream_t st) {
-    k_pcg_gather<<<blocks, kThreads, 0, st>>>(n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl);
+                       Ctrl* ctrl, cudaStream_t st, int init) {
+    k_pcg_gather<<<blocks, kThreads, 0, st>>>(n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl,
+                                              init);
+}
+
+// ---- contact-aware material adjoint ------------------------------------------------------------------
+// u_c <- (I - sum_k d_k d_k^T) u_c at the constrained nodes (orthonormal directions d_k, at most 3 per node);
+// with vperm, the projected values are also written to the S-ordered copy.
+template <typename T>
+__global__ void k_wb_project(const int* __restrict__ count, const int* __restrict__ nodes,
+                             const double* __restrict__ dirs, const int* __restrict__ ndir, double* __restrict__ u,
+                             T* __restrict__ vperm, const int* __restrict__ iperm, int npad, const Ctrl* ctrl) {
+    if (ctrl && ctrl->done) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *count) return;
+    const int node = nodes[k];
+    double x[3] = {u[3 * node], u[3 * node + 1], u[3 * node + 2]};
+    for (int j = 0; j < ndir[k]; ++j) {
+        const double* d = dirs + 9 * (size_t)k + 3 * j;
+        const double t = d[0] * x[0] + d[1] * x[1] + d[2] * x[2];
+        x[0] -= t * d[0];
+        x[1] -= t * d[1];
+        x[2] -= t * d[2];
+    }
+    u[3 * node] = x[0];
+    u[3 * node + 1] = x[1];
+    u[3 * node + 2] = x[2];
+    if (vperm) {
+        const int j = iperm[node];
+        vperm[j] = (T)x[0];
+        vperm[npad + j] = (T)x[1];
+        vperm[2 * (size_t)npad + j] = (T)x[2];
+    }
+}
+
+template <typename T>
+void launch_wb_project(int capacity, const int* count, const int* nodes, const double* dirs, const int* ndir,
+                       double* u, T* vperm, const int* iperm, int npad, const Ctrl* ctrl, cudaStream_t st) {
+    k_wb_project<T><<<blocks_for(std::max(capacity, 1), kThreads), kThreads, 0, st>>>(count, nodes, dirs, ndir, u,
+                                                                                     vperm, iperm, npad, ctrl);
+}
+template void launch_wb_project<double>(int, const int*, const int*, const double*, const int*, double*, double*,
+                                        const int*, int, const Ctrl*, cudaStream_t);
+template void launch_wb_project<float>(int, const int*, const int*, const double*, const int*, double*, float*,
+                                       const int*, int, const Ctrl*, cudaStream_t);
+
+// out[k] = u at node cand[k] (3 values per candidate)
+__global__ void k_gather_nodes(int K, const int* __restrict__ cand, const double* __restrict__ u,
+                               double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const int node = cand[k];
+    out[3 * k] = u[3 * node];
+    out[3 * k + 1] = u[3 * node + 1];
+    out[3 * k + 2] = u[3 * node + 2];
+}
+void launch_gather_nodes(int K, const int* cand, const double* u, double* out, cudaStream_t st) {
+    if (K > 0) k_gather_nodes<<<blocks_for(K, kThreads), kThreads, 0, st>>>(K, cand, u, out);
+}
+
+// res = {|a - b|^2, |a|^2, |b|^2} (one CTA: a tape comparison per backward call, off the iteration path)
+__global__ void __launch_bounds__(1024) k_diff_norms(int n, const double* __restrict__ a,
+                                                     const double* __restrict__ b, double* __restrict__ res) {
+    __shared__ double sh[3 * 32];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = a[i], y = b[i];
+        acc[0] += (x - y) * (x - y);
+        acc[1] += x * x;
+        acc[2] += y * y;
+    }
+    block_sum<3>(acc, sh);
+    if (threadIdx.x == 0) {
+        res[0] = acc[0];
+        res[1] = acc[1];
+        res[2] = acc[2];
+    }
+}
+void launch_diff_norms(int n, const double* a, const double* b, double* res, cudaStream_t st) {
+    k_diff_norms<<<1, 1024, 0, st>>>(n, a, b, res);
 }
 template <typename T>
 void launch_pcg_update1(int n, double* mu, double* r, const double* p, const double* w,

@@ -142,7 +142,7 @@ void launch_param_grad(int m, int k, int s, const int* E, const double* q, const
 // stop rule |z| < rtol |mu| + atol, p = z + beta p.
 void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
                        const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
-                       Ctrl* ctrl, cudaStream_t st);
+                       Ctrl* ctrl, cudaStream_t st, int init = 0);
 template <typename T>
 void launch_pcg_update1(int n, double* mu, double* r, const double* p, const double* w,
                         const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad, double* part,
@@ -190,6 +190,14 @@ template <typename T>
 void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st);
 template <typename T>
 void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
+
+// Contact-aware material adjoint: projection of node vectors onto the complement of the constrained contact
+// directions, candidate-node gather, and the |a - b|, |a|, |b| norms of a tape comparison.
+template <typename T>
+void launch_wb_project(int capacity, const int* count, const int* nodes, const double* dirs, const int* ndir,
+                       double* u, T* vperm, const int* iperm, int npad, const Ctrl* ctrl, cudaStream_t st);
+void launch_gather_nodes(int K, const int* cand, const double* u, double* out, cudaStream_t st);
+void launch_diff_norms(int n, const double* a, const double* b, double* res, cudaStream_t st);
 
 // Device-side loop control of a graph WHILE node: counts the iteration and keeps looping while the gate has
 // not set `done` and fewer than `cap` iterations ran (cap > max_iter: a bound even if a gate kernel is skipped).

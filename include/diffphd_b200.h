@@ -109,6 +109,11 @@ int dphd_num_frames(const dphd_deformable* h);
 int dphd_frame_stats(const dphd_deformable* h, int* frame_iters, int* frame_converged);
 int dphd_reset_frame_stats(dphd_deformable* h);
 int dphd_last_backward_iters(const dphd_deformable* h);
+/* The last backward call's contact-aware material adjoint (backward_gpu.cpp:937-1208): where its contact frame
+ * came from (0 none / skipped by option, 1 the forward tape, 2 a replayed forward step, 3 a tape miss on the
+ * device-pointer entry, which has no q, v to replay from: material gradients then use the plain adjoint),
+ * the number of contact basis constraints kept, and the conjugate-gradient iterations of the constrained solve. */
+int dphd_contact_adjoint_stats(const dphd_deformable* h, int* source, int* constraints, int* iters);
 /* AlgPhdSMemoryBytes / AlgPhdSNnz (forward_gpu.cpp:302-315): bytes of the S factor in HBM and its nnz. */
 long long dphd_s_memory_bytes(const dphd_deformable* h);
 long long dphd_s_nnz(const dphd_deformable* h);

@@ -651,6 +651,14 @@ struct Model {
     // lambda warm start (forward_gpu.cpp:1074-1084, 1544-1545)
     std::vector<int> prev_cand;
     std::vector<real> prev_lambda;
+    // forward tape of contact frames (AlgPhdReplayCache, deformable.h:336-355; pushed forward_gpu.cpp:1547-1593,
+    // popped backward_gpu.cpp:716-742): active candidates (lambda > 0), their last-iteration omega and lambda
+    struct TapeFrame {
+        std::vector<real> q_sol;
+        std::vector<int> active;
+        std::vector<real> omega, lambda;
+    };
+    std::vector<TapeFrame> tape;
     // statistics of the last forward call
     int last_iters = 0, last_converged = 0;
 
@@ -870,6 +878,10 @@ struct Options {
     int mean_stiffness_bwd = 0;  // reference backward semantics: mean stiffness in K_pd
     int cascade_cap = 1;
     int verbose = 0;
+    // contact-aware material adjoint (backward_gpu.cpp:937-1208)
+    int skip_woodbury = 0, skip_material_grad = 0;
+    real tangent_lambda_min = 1e-8, rhs_prune_rel = 1e-3, rhs_prune_abs = 1e-12;
+    int basis_topk = 0, wt_max_iter = 120;
 };
 
 // Type-II Anderson acceleration with the reference's regularisation and restart rule
@@ -1031,6 +1043,7 @@ static void forward(Model& M, const real* q, const real* v, const real* f_ext, r
     Anderson aa{opt.aa_window, {}, {}};
     bool converged = false;
     int iters = 0;
+    std::vector<real> om_last(K, 0);
     for (int it = 0; it < opt.max_pd_iter; ++it) {
         local_step(M, qs.data(), pd.data());
         for (int i = 0; i < n3; ++i) b[i] = inv_h2m * qt[i] + pd[i];
@@ -1045,6 +1058,7 @@ static void forward(Model& M, const real* q, const real* v, const real* f_ext, r
                 om[ci] = 1.0 - dn[ci] / den;
                 Ed[ci] = (1.0 - rp[ci] * lam[ci] / den) * rp[ci];
             }
+            om_last = om;
             std::vector<real> Ms((size_t)K * K);
             for (int i = 0; i < K; ++i)
                 for (int j = 0; j < K; ++j) Ms[(size_t)i * K + j] = om[i] * W[(size_t)i * K + j] * om[j];
@@ -1180,6 +1194,18 @@ static void forward(Model& M, const real* q, const real* v, const real* f_ext, r
         if (lam[ci] > 0) active.push_back(cand[ci]);
     M.prev_cand = cand;
     M.prev_lambda = lam;
+    if (K > 0) {
+        Model::TapeFrame fr;
+        fr.q_sol.assign(q_next, q_next + n3);
+        for (int ci = 0; ci < K; ++ci)
+            if (lam[ci] > 0) {
+                fr.active.push_back(cand[ci]);
+                fr.omega.push_back(om_last[ci]);
+                fr.lambda.push_back(lam[ci]);
+            }
+        M.tape.push_back(std::move(fr));
+        if (M.tape.size() > 8192) M.tape.erase(M.tape.begin());
+    }
 }
 
 // K_pd u: sum_e (vol/s) sum_s A_s^T [w dBp/dF](A_s u)  (deformable_projective_dynamics_backward.cpp:10-139)
@@ -1221,7 +1247,6 @@ static void backward(Model& M, const real* q, const real* v, const real* f_ext, 
                      const real* dl_dq_next, const real* dl_dv_next, const Options& opt, real* dl_dq, real* dl_dv,
                      real* dl_df, real* dl_dmat_w, real* dl_dparams, real* dl_dstate_p, int* iters_out) {
     setup_solver(M, h);
-    (void)v; (void)f_ext;
     const int n3 = 3 * M.n;
     const real inv_h2m = M.mass() / (h * h), h2m = h * h / M.mass();
     std::vector<real> gbar(n3);
@@ -1284,6 +1309,137 @@ static void backward(Model& M, const real* q, const real* v, const real* f_ext, 
     }
     if (!M.gravity.empty())
         for (int i = 0; i < n3; ++i) dl_dstate_p[i % 3] += h2m * inj[i] * M.mass();
+    if (opt.skip_material_grad) return;
+    // Contact-aware adjoint for the material gradients (backward_gpu.cpp:937-1208):
+    // z_q = mu - W_T G_T^-1 (J_basis mu), W_T[k] = (A - K_pd)^-1 j_k by the Anderson fixed point.
+    std::vector<real> zq = mu;
+    Model::TapeFrame fr;
+    bool have = false;
+    if (M.has_plane) {
+        if (!M.tape.empty()) {  // tape pop (backward_gpu.cpp:716-742)
+            const Model::TapeFrame& tail = M.tape.back();
+            std::vector<real> dd(n3);
+            for (int i = 0; i < n3; ++i) dd[i] = tail.q_sol[i] - q_next[i];
+            const real denom = std::max<real>(1, std::max(norm(tail.q_sol), norm(std::vector<real>(q_next, q_next + n3))));
+            const real rel = norm(dd) / denom;
+            if (rel <= 1e-8) {
+                fr = tail;
+                M.tape.pop_back();
+                have = true;
+            } else if (rel > 1e-6) {
+                M.tape.clear();
+            }
+        }
+        if (!have) {  // replay: the forward step again from (q, v, f_ext), lambda warm start preserved
+            const std::vector<int> pc = M.prev_cand;
+            const std::vector<real> pl = M.prev_lambda;
+            std::vector<real> tq(n3), tv(n3);
+            std::vector<int> act;
+            forward(M, q, v, f_ext, h, opt, tq.data(), tv.data(), act);
+            fr = M.tape.back();
+            M.tape.pop_back();
+            M.prev_cand = pc;
+            M.prev_lambda = pl;
+            have = true;
+        }
+    }
+    if (have && !opt.skip_woodbury && !fr.active.empty()) {
+        const real* nrm = M.pn;
+        // tangent basis of the backward (backward_gpu.cpp:958-981): axis of the smallest |n_d|
+        int axis = 0;
+        for (int d = 1; d < 3; ++d)
+            if (std::fabs(nrm[d]) < std::fabs(nrm[axis])) axis = d;
+        real e[3] = {0, 0, 0};
+        e[axis] = 1;
+        const real ne = nrm[0] * e[0] + nrm[1] * e[1] + nrm[2] * e[2];
+        real t1[3] = {e[0] - ne * nrm[0], e[1] - ne * nrm[1], e[2] - ne * nrm[2]};
+        real l1 = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+        if (l1 > 1e-12) for (auto& x : t1) x /= l1;
+        else { t1[0] = 1; t1[1] = 0; t1[2] = 0; }
+        real t2[3] = {nrm[1] * t1[2] - nrm[2] * t1[1], nrm[2] * t1[0] - nrm[0] * t1[2], nrm[0] * t1[1] - nrm[1] * t1[0]};
+        const real l2 = std::sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+        if (l2 > 1e-12) for (auto& x : t2) x /= l2;
+        else { t2[0] = 0; t2[1] = 1; t2[2] = 0; }
+        const bool tang = opt.friction_mu > 0;
+        struct Basis { int ai, b; };
+        std::vector<Basis> full;
+        for (int ai = 0; ai < (int)fr.active.size(); ++ai) {
+            if (fr.omega[ai] < 0.5) continue;
+            full.push_back({ai, 0});
+            if (tang && fr.lambda[ai] > opt.tangent_lambda_min) {
+                full.push_back({ai, 1});
+                full.push_back({ai, 2});
+            }
+        }
+        auto basis_dir = [&](const Basis& bc, real* dir, real& scale) {
+            const real* src = bc.b == 0 ? nrm : (bc.b == 1 ? t1 : t2);
+            for (int d = 0; d < 3; ++d) dir[d] = src[d];
+            scale = bc.b == 0 ? fr.omega[bc.ai] : 1.0;
+        };
+        auto project = [&](const Basis& bc, const std::vector<real>& x) {
+            real dir[3], sc;
+            basis_dir(bc, dir, sc);
+            const int node = fr.active[bc.ai];
+            return sc * (dir[0] * x[3 * node] + dir[1] * x[3 * node + 1] + dir[2] * x[3 * node + 2]);
+        };
+        const int nbf = (int)full.size();
+        std::vector<real> rfull(nbf);
+        real rmax = 0;
+        for (int i = 0; i < nbf; ++i) {
+            rfull[i] = project(full[i], zq);
+            rmax = std::max(rmax, std::fabs(rfull[i]));
+        }
+        const real gate = std::max(opt.rhs_prune_abs, opt.rhs_prune_rel * rmax);
+        std::vector<int> sel;
+        for (int i = 0; i < nbf; ++i)
+            if (std::fabs(rfull[i]) >= gate) sel.push_back(i);
+        if (opt.basis_topk > 0 && (int)sel.size() > opt.basis_topk) {
+            std::nth_element(sel.begin(), sel.begin() + opt.basis_topk, sel.end(),
+                             [&](int a, int b) { return std::fabs(rfull[a]) > std::fabs(rfull[b]); });
+            sel.resize(opt.basis_topk);
+        }
+        const int nb = (int)sel.size();
+        if (nb > 0) {
+            const int wmax = std::min(opt.max_pd_iter, std::max(1, opt.wt_max_iter));
+            std::vector<std::vector<real>> WT(nb);
+            for (int k = 0; k < nb; ++k) {
+                const Basis bc = full[sel[k]];
+                real dir[3], sc;
+                basis_dir(bc, dir, sc);
+                std::vector<real> j(n3, 0), sv(n3, 0), kp(n3), rh(n3), sn(n3);
+                const int node = fr.active[bc.ai];
+                for (int d = 0; d < 3; ++d) j[3 * node + d] = sc * dir[d];
+                Anderson wa{opt.aa_window, {}, {}};
+                for (int it = 0; it < wmax; ++it) {
+                    apply_kpd(M, svd, sv.data(), kp.data(), opt.mean_stiffness_bwd != 0);
+                    for (int i = 0; i < n3; ++i) rh[i] = j[i] + kp[i];
+                    apply_ainv(M, rh.data(), sn.data());
+                    for (const auto& kv : M.dirichlet) sn[kv.first] = 0;
+                    clip(sn);
+                    std::vector<real> dd(n3);
+                    for (int i = 0; i < n3; ++i) dd[i] = sn[i] - sv[i];
+                    const real err = norm(dd);
+                    std::vector<real> cx;
+                    if (wa.step(sv, dd, cx)) {
+                        sn = cx;
+                        clip(sn);
+                    }
+                    sv = sn;
+                    if (it > 0 && err < opt.rel_tol * norm(sv) + opt.abs_tol) break;
+                }
+                WT[k] = sv;
+            }
+            std::vector<real> GT((size_t)nb * nb), al(nb);
+            for (int k = 0; k < nb; ++k)
+                for (int l = 0; l < nb; ++l) GT[(size_t)l * nb + k] = project(full[sel[l]], WT[k]);
+            for (int i = 0; i < nb; ++i) al[i] = rfull[sel[i]];
+            dense_solve(nb, GT, al);
+            for (int k = 0; k < nb; ++k)
+                for (int i = 0; i < n3; ++i) zq[i] -= al[k] * WT[k][i];
+            clip(zq);
+        }
+    }
+    mu = zq;  // the material gradients below use the contact-aware adjoint
     // parameter gradients: dl/dw_e = -(vol/s) sum_s mu_e^T A_s^T (F_s - Bp_s); reference-style dl_dmat_w
     // uses the stress over the energy's mean stiffness (deformable_pd_energy.cpp:368-403).
     int off = 0;
@@ -1398,6 +1554,13 @@ Options parse_opts(const char** keys, const double* vals, int n) {
     if (m.count("alg_phd_bwd_clip_norm")) o.clip = m["alg_phd_bwd_clip_norm"];
     if (m.count("bwd_mean_stiffness")) o.mean_stiffness_bwd = (int)m["bwd_mean_stiffness"];
     if (m.count("bwd_cascade_cap")) o.cascade_cap = (int)m["bwd_cascade_cap"];
+    if (m.count("skip_contact_woodbury")) o.skip_woodbury = m["skip_contact_woodbury"] > 0.5;
+    if (m.count("skip_material_grad")) o.skip_material_grad = m["skip_material_grad"] > 0.5;
+    if (m.count("alg_phd_bwd_tangent_lambda_min")) o.tangent_lambda_min = m["alg_phd_bwd_tangent_lambda_min"];
+    if (m.count("alg_phd_bwd_rhs_prune_rel")) o.rhs_prune_rel = m["alg_phd_bwd_rhs_prune_rel"];
+    if (m.count("alg_phd_bwd_rhs_prune_abs")) o.rhs_prune_abs = m["alg_phd_bwd_rhs_prune_abs"];
+    if (m.count("alg_phd_bwd_basis_topk")) o.basis_topk = (int)m["alg_phd_bwd_basis_topk"];
+    if (m.count("alg_phd_bwd_wt_max_iter")) o.wt_max_iter = (int)m["alg_phd_bwd_wt_max_iter"];
 #ifdef _OPENMP
     if ((int)m["thread_ct"] > 0) omp_set_num_threads((int)m["thread_ct"]);
 #endif
