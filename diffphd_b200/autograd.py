@@ -8,8 +8,9 @@ stale (it passes 5 outputs to the 7-output PyBackward).  `Rollout` replaces it f
 * `sim` is a `DiffSim` (scene + options); `params` is the concatenation of every AddPdEnergy parameter
   array (per-element stiffnesses or interleaved [mu_e, la_e]); changing it rebuilds the deformable.
 * `f_ext` is one (3n,) external force applied at every step.
-* Forward runs on the device entry points and stores (q, v) every `checkpoint_every` steps; backward
-  recomputes each segment from its checkpoint and runs the adjoint through it in reverse
+* Forward runs on the device entry points and stores (q, v, contact multipliers) every `checkpoint_every`
+  steps; backward recomputes each segment from its checkpoint and runs the adjoint through it in reverse
+  (the recomputed frames also refill the contact tape that the adjoint pops)
   (forward checkpointing with recomputation; memory is O(T / k + k) states instead of O(T)).
 Gradients: q0, v0, params (summed over steps) and f_ext (summed over steps).
 """
@@ -71,11 +72,12 @@ class Rollout(torch.autograd.Function):
         q, v = q0.detach().contiguous(), v0.detach().contiguous()
         f = f_ext.detach().contiguous()
         k = max(1, int(checkpoint_every))
-        ckpts = {0: (q.clone(), v.clone())}
+        # a checkpoint holds (q, v) and the contact multipliers that warm-start the next frame's NCP
+        ckpts = {0: (q.clone(), v.clone(), d.contact_lambda(stream=stream).clone())}
         for t in range(steps):
             q, v = _step(d, sim, q, v, f, stream)
             if (t + 1) % k == 0 and t + 1 < steps:
-                ckpts[t + 1] = (q.clone(), v.clone())
+                ckpts[t + 1] = (q.clone(), v.clone(), d.contact_lambda(stream=stream).clone())
         ctx.sim, ctx.steps, ctx.k, ctx.p_np = sim, steps, k, p_np
         ctx.ckpts = ckpts
         ctx.save_for_backward(f)
@@ -97,8 +99,9 @@ class Rollout(torch.autograd.Function):
         starts = sorted(ctx.ckpts)
         for s in reversed(starts):
             e = min(s + k, steps)
-            # recompute the segment's states from its checkpoint
-            q, v = ctx.ckpts[s]
+            # recompute the segment's states from its checkpoint (and its contact multipliers)
+            q, v, lam = ctx.ckpts[s]
+            d.set_contact_lambda(lam, stream=stream)
             qs = [q]
             for _ in range(s, e):
                 q, v = _step(d, sim, q, v, f, stream)

@@ -85,6 +85,9 @@ def load_library():
     L.dphd_mlp_sizes.argtypes = [_ip, _ip, _ip, _ip]
     L.dphd_set_warm_start_network.argtypes = [C.c_void_p] * 3
     L.dphd_contact_adjoint_stats.argtypes = [C.c_void_p, _ip, _ip, _ip]
+    L.dphd_last_filtered_samples.argtypes = [C.c_void_p]
+    L.dphd_num_contact_candidates.argtypes = [C.c_void_p]
+    L.dphd_contact_lambda_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.dphd_mlp_pack.argtypes = [C.c_void_p] * 3
     L.dphd_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.dphd_mlp_train_step.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_void_p] + [C.c_float] * 5 + \
@@ -343,6 +346,32 @@ class Deformable:
         cv = np.zeros(max(nf, 1), np.int32)
         self._check(self._L.dphd_frame_stats(self._h, _iptr(it), _iptr(cv)))
         return it[:nf].copy(), cv[:nf].copy()
+
+    def num_contact_candidates(self):
+        return int(self._L.dphd_num_contact_candidates(self._h))
+
+    def contact_lambda(self, out=None, stream=0):
+        """The contact multipliers (lambda warm start) as a float64 CUDA tensor (copied into `out` if given)."""
+        import torch
+        k = self.num_contact_candidates()
+        if out is None:
+            out = torch.empty(max(k, 0), dtype=torch.float64, device="cuda")
+        if k > 0:
+            self._check(self._L.dphd_contact_lambda_device(self._h, C.c_void_p(out.data_ptr()), 0,
+                                                           C.c_void_p(int(stream))))
+        return out
+
+    def set_contact_lambda(self, lam, stream=0):
+        k = self.num_contact_candidates()
+        if k > 0:
+            if lam.numel() != k or lam.dtype.itemsize != 8 or not lam.is_cuda:
+                raise RuntimeError(f"contact multipliers: expected {k} float64 values on the GPU")
+            self._check(self._L.dphd_contact_lambda_device(self._h, C.c_void_p(lam.data_ptr()), 1,
+                                                           C.c_void_p(int(stream))))
+
+    def last_filtered_samples(self):
+        """Samples whose local Hessian the last backward eigen-filtered (option bwd_eigen_filter)."""
+        return int(self._L.dphd_last_filtered_samples(self._h))
 
     def contact_adjoint_stats(self):
         """(source, constraints, cg_iters) of the last backward's contact-aware material adjoint: source 0 none,

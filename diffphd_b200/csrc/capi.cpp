@@ -266,6 +266,17 @@ int dphd_set_warm_start_network(dphd_deformable* h, const float* d_master, const
     return guard([&] { E(h).set_ws_net(d_master, d_packed); });
 }
 
+int dphd_num_contact_candidates(const dphd_deformable* h) {
+    return h && h->eng ? h->eng->contact_candidates() : -1;
+}
+
+int dphd_contact_lambda_device(dphd_deformable* h, double* d_lambda, int set, void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_lambda || E(h).contact_candidates() == 0, "null device pointer");
+        E(h).contact_lambda_device(d_lambda, set != 0, (cudaStream_t)stream);
+    });
+}
+
 int dphd_mlp_sizes(int* n_master, int* n_packed, int* part_floats_per_block, int* rows_per_block) {
     return guard([&] {
         if (n_master) *n_master = dphd::mlp_param_count();
@@ -388,6 +399,9 @@ int dphd_reset_frame_stats(dphd_deformable* h) {
     });
 }
 int dphd_last_backward_iters(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.last_bwd_iters : -1; }
+int dphd_last_filtered_samples(const dphd_deformable* h) {
+    return h && h->eng ? h->eng->stats.last_filtered : -1;
+}
 int dphd_contact_adjoint_stats(const dphd_deformable* h, int* source, int* constraints, int* iters) {
     return guard([&] {
         DPHD_CHECK(h && h->eng, "null handle");

@@ -570,6 +570,21 @@ void Engine::reset_warm_start() {
     ws_prev_valid_ = false;
 }
 
+int Engine::contact_candidates() const { return M.has_plane ? (int)M.contact_nodes.size() : 0; }
+
+void Engine::contact_lambda_device(double* d_out, bool set, cudaStream_t st) {
+    const int K = contact_candidates();
+    if (K == 0) return;
+    const size_t b = (size_t)K * sizeof(double);
+    if (!has_contact_ || !dc_lam.p) {  // before the first forward call: the multipliers are zero
+        DPHD_CHECK(!set, "contact multipliers: make one forward call before setting them");
+        CUDA_OK(cudaMemsetAsync(d_out, 0, b, st));
+        return;
+    }
+    if (set) CUDA_OK(cudaMemcpyAsync(dc_lam.p, d_out, b, cudaMemcpyDeviceToDevice, st));
+    else CUDA_OK(cudaMemcpyAsync(d_out, dc_lam.p, b, cudaMemcpyDeviceToDevice, st));
+}
+
 std::vector<double> Engine::contact_lambda() {
     std::vector<double> l(has_contact_ ? contact_.K : 0);
     if (!l.empty()) CUDA_OK(cudaMemcpy(l.data(), dc_lam.p, l.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -886,6 +901,15 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     const double h2m = dt * dt / M.mass();
     const bool learned = !d_init && ws_net_;
     if (learned) d_init = ws_predict(dq, dv, df, dt, st);
+    // new-rollout detection of the contact tape (forward_gpu.cpp:437-449): the input must continue the last
+    // frame; the comparison is read after the solve's own synchronisation
+    const bool check_tape = has_contact_ && !tape_.empty();
+    if (check_tape) {
+        d_cmp.alloc(4 * sizeof(double));
+        if (!h_cmp_) CUDA_OK(cudaMallocHost(&h_cmp_, 4 * sizeof(double)));
+        launch_diff_norms(n3, tape_.back()->q_sol.as<double>(), dq, d_cmp.as<double>(), st);
+        CUDA_OK(cudaMemcpyAsync(h_cmp_, d_cmp.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
     launch_qtilde(n3, dq, dv, df, dt, h2m, d_gravf.as<double>(), d_qt.as<double>(), st);
     CUDA_OK(cudaMemcpyAsync(d_q0.p, dq, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     run_forward_loop(dq, dt, o, st, d_init);
@@ -897,6 +921,14 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     if (has_contact_ && o.restitution > 0) {
         launch_restitution(contact_, d_x.as<double>(), dq, dv, dt, o.restitution, o.contact_slop, st);
         launches_ += 1;
+    }
+    if (check_tape) {
+        const double denom = std::max(1.0, std::max(std::sqrt(h_cmp_[1]), std::sqrt(h_cmp_[2])));
+        if (!(std::sqrt(h_cmp_[0]) <= 1e-8 * denom))
+            while (!tape_.empty()) {
+                tape_free_.push_back(std::move(tape_.back()));
+                tape_.pop_back();
+            }
     }
     if (has_contact_) tape_push(d_x.as<double>(), st);
     CUDA_OK(cudaMemcpyAsync(dqn, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));

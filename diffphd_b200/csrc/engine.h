@@ -121,6 +121,9 @@ public:
     // attached, every forward step whose caller gives no initial guess starts its PD loop from the network's
     // prediction.  The previous step's q and q_tilde are engine state (reset by reset_warm_start).
     void set_ws_net(const float* d_master, const void* d_packed);
+    // contact candidates and their normal multipliers (the lambda warm start carried across frames)
+    int contact_candidates() const;
+    void contact_lambda_device(double* d_buf, bool set, cudaStream_t st);
     bool ws_net_attached() const { return ws_net_; }
 
     void backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,

@@ -789,10 +789,10 @@ __global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict_
         for (int i = 0; i < 9; ++i) Jt[col * 9 + i] = out[i];  // column col (column-major 9x9)
     }
     if (filter == 0) return;
-    // State-adaptive filter of the local Hessian H = wsum I - J (the PD energy's per-sample Hessian):
-    // kept as is when symmetric diagonally dominant with a non-negative diagonal (hence PSD); otherwise
-    // eigen-decomposed and its eigenvalues clamped at 0 (filter 1) or replaced by |lambda| (filter 2),
-    // following ProjectedNewtonMatrix (cpp/core/src/fem/deformable_newton_forward.cpp:394-434).
+    // State-adaptive filter of the local Hessian H = wsum I - J (the PD energy's per-sample Hessian), with the
+    // rule of ProjectedNewtonMatrix (cpp/core/src/fem/deformable_newton_forward.cpp:394-434): kept as is when
+    // diagonally dominant (|H_kk| >= sum_j |H_kj| + 1e-5 in every row); otherwise eigen-decomposed and its
+    // eigenvalues clamped at 0 (filter 1) or replaced by |lambda| (filter 2).
     double H[81];
     for (int i = 0; i < 9; ++i)
         for (int j = 0; j < 9; ++j) H[i * 9 + j] = (i == j ? wsum : 0.0) - 0.5 * (Jt[j * 9 + i] + Jt[i * 9 + j]);
@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict_
         double off = 0;
         for (int j = 0; j < 9; ++j)
             if (j != i) off += fabs(H[i * 9 + j]);
-        dd = H[i * 9 + i] >= off;
+        dd = !(fabs(H[i * 9 + i]) < off + 1e-5);
     }
     if (dd) return;
     double Q[81];

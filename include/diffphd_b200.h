@@ -109,6 +109,9 @@ int dphd_num_frames(const dphd_deformable* h);
 int dphd_frame_stats(const dphd_deformable* h, int* frame_iters, int* frame_converged);
 int dphd_reset_frame_stats(dphd_deformable* h);
 int dphd_last_backward_iters(const dphd_deformable* h);
+/* Samples whose 9x9 local Hessian the last backward call eigen-filtered (option bwd_eigen_filter 1 clamp /
+ * 2 absolute value; the diagonal-dominance test of ProjectedNewtonMatrix, deformable_newton_forward.cpp:394-434). */
+int dphd_last_filtered_samples(const dphd_deformable* h);
 /* The last backward call's contact-aware material adjoint (backward_gpu.cpp:937-1208): where its contact frame
  * came from (0 none / skipped by option, 1 the forward tape, 2 a replayed forward step, 3 a tape miss on the
  * device-pointer entry, which has no q, v to replay from: material gradients then use the plain adjoint),
@@ -129,6 +132,13 @@ long long dphd_s_padded_values(const dphd_deformable* h);
  * array: calls that overlap on the GPU race and must be serialised by the caller.  The first call on a
  * device looks up the array's address; make it before any stream capture. */
 int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream);
+
+/* Contact candidates of the frictional boundary (0 without one; -1 before the first forward call builds them)
+ * and their normal multipliers lambda, the warm start the reference carries across frames
+ * (forward_gpu.cpp:1074-1084): copied to (set = 0) or from (set = 1) a device array of that length.  A
+ * checkpointed rollout saves them with each checkpoint so that recomputing a segment repeats the forward. */
+int dphd_num_contact_candidates(const dphd_deformable* h);
+int dphd_contact_lambda_device(dphd_deformable* h, double* d_lambda, int set, void* stream);
 
 /* ---- Learned warm start (no counterpart in the reference: the reference starts every PD loop from q). ----
  * A forward step whose PD loop starts from d_q_init (3n FP64) instead of q.  The loop still runs to the same

@@ -52,6 +52,7 @@ def lib():
         L.orc_mass.restype = C.c_double
         L.orc_last_iters.argtypes = [C.c_void_p]
         L.orc_last_converged.argtypes = [C.c_void_p]
+        L.orc_last_filtered.argtypes = [C.c_void_p]
         L.orc_reset_warm_start.argtypes = [C.c_void_p]
         L.orc_forward.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, C.POINTER(C.c_char_p), _dp, C.c_int,
                                   _dp, _dp, _ip, _ip]
@@ -173,6 +174,11 @@ class OracleDeformable:
     @property
     def last_iters(self):
         return lib().orc_last_iters(self.h)
+
+    @property
+    def last_filtered(self):
+        """Samples whose Hessian the last backward eigen-filtered (option bwd_eigen_filter)."""
+        return lib().orc_last_filtered(self.h)
 
     def reset_warm_start(self):
         lib().orc_reset_warm_start(self.h)

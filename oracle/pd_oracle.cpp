@@ -661,6 +661,7 @@ struct Model {
     std::vector<TapeFrame> tape;
     // statistics of the last forward call
     int last_iters = 0, last_converged = 0;
+    int last_filtered = 0;  // samples whose Hessian the last backward filtered
 
     const real* g(int e, int smp) const { return &grad[((size_t)(hex ? 0 : e) * s + smp) * k * 3]; }
     real mass() const { return density * vol; }
@@ -882,6 +883,7 @@ struct Options {
     int skip_woodbury = 0, skip_material_grad = 0;
     real tangent_lambda_min = 1e-8, rhs_prune_rel = 1e-3, rhs_prune_abs = 1e-12;
     int basis_topk = 0, wt_max_iter = 120;
+    int eigen_filter = 0;  // 0 off, 1 clamp at 0, 2 absolute value (deformable_newton_forward.cpp:394-434)
 };
 
 // Type-II Anderson acceleration with the reference's regularisation and restart rule
@@ -1233,6 +1235,114 @@ static void apply_kpd(const Model& M, const std::vector<std::vector<SvdData>>& s
             for (int i = 0; i < 3; ++i) out[3 * M.E[(size_t)e * M.k + a] + i] += per[((size_t)e * M.k + a) * 3 + i];
 }
 
+// Symmetric eigen-decomposition A = Q diag(A') Q^T by cyclic Jacobi rotations (n x n, row-major, in place).
+static void sym_eig(int n, std::vector<real>& A, std::vector<real>& Q) {
+    Q.assign((size_t)n * n, 0);
+    for (int i = 0; i < n; ++i) Q[(size_t)i * n + i] = 1;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        real off = 0, tot = 0;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const real a = A[(size_t)i * n + j];
+                tot += a * a;
+                if (i != j) off += a * a;
+            }
+        if (off <= 1e-32 * tot) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const real apq = A[(size_t)p * n + q];
+                if (apq == 0) continue;
+                const real theta = 0.5 * std::atan2(2 * apq, A[(size_t)q * n + q] - A[(size_t)p * n + p]);
+                const real c = std::cos(theta), s = std::sin(theta);
+                for (int k = 0; k < n; ++k) {
+                    const real akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - s * akq;
+                    A[(size_t)k * n + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const real apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - s * aqk;
+                    A[(size_t)q * n + k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const real qkp = Q[(size_t)k * n + p], qkq = Q[(size_t)k * n + q];
+                    Q[(size_t)k * n + p] = c * qkp - s * qkq;
+                    Q[(size_t)k * n + q] = s * qkp + c * qkq;
+                }
+            }
+    }
+}
+
+// Per-sample 9x9 Jacobian of the weighted projections, J[col * 9 + i] = d(sum_en w Bp)_i / dF_col, with the
+// state-adaptive eigen filter of H = (sum w) I - sym(J) applied when `filter` is set (the diagonal-dominance
+// test and eigenvalue clamp / absolute value of ProjectedNewtonMatrix, deformable_newton_forward.cpp:394-434).
+static int build_filtered_jacobians(const Model& M, const std::vector<std::vector<SvdData>>& svd, bool mean_w,
+                                    int filter, std::vector<real>& Jall) {
+    Jall.assign((size_t)M.m * M.s * 81, 0);
+    int nfilt = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nfilt)
+    for (int e = 0; e < M.m; ++e)
+        for (int smp = 0; smp < M.s; ++smp) {
+            real* J = &Jall[((size_t)e * M.s + smp) * 81];
+            real wsum = 0;
+            for (const auto& en : M.energies)
+                if (en.in_set[e]) wsum += (mean_w ? en.w_mean : en.elem_w(e)) * M.vol / M.s;
+            for (int col = 0; col < 9; ++col) {
+                M3 dF = zero3();
+                dF.a[col] = 1;
+                for (const auto& en : M.energies) {
+                    if (!en.in_set[e]) continue;
+                    const real w = (mean_w ? en.w_mean : en.elem_w(e)) * M.vol / M.s;
+                    const M3 dB = project_diff(en, svd[e][smp], dF);
+                    for (int i = 0; i < 9; ++i) J[col * 9 + i] += w * dB.a[i];
+                }
+            }
+            if (!filter) continue;
+            std::vector<real> H(81), Q;
+            for (int i = 0; i < 9; ++i)
+                for (int j = 0; j < 9; ++j) H[i * 9 + j] = (i == j ? wsum : 0.0) - 0.5 * (J[j * 9 + i] + J[i * 9 + j]);
+            bool dd = true;
+            for (int i = 0; i < 9 && dd; ++i) {
+                real off = 0;
+                for (int j = 0; j < 9; ++j)
+                    if (j != i) off += std::fabs(H[i * 9 + j]);
+                if (std::fabs(H[i * 9 + i]) < off + 1e-5) dd = false;
+            }
+            if (dd) continue;
+            sym_eig(9, H, Q);
+            real lam[9];
+            for (int k = 0; k < 9; ++k) lam[k] = filter == 1 ? std::max(H[k * 9 + k], real(0)) : std::fabs(H[k * 9 + k]);
+            for (int i = 0; i < 9; ++i)
+                for (int j = 0; j < 9; ++j) {
+                    real h = 0;
+                    for (int k = 0; k < 9; ++k) h += Q[i * 9 + k] * lam[k] * Q[j * 9 + k];
+                    J[j * 9 + i] = (i == j ? wsum : 0.0) - h;
+                }
+            ++nfilt;
+        }
+    return nfilt;
+}
+
+// K_pd u from the per-sample Jacobians of build_filtered_jacobians.
+static void apply_kpd_J(const Model& M, const std::vector<real>& Jall, const real* u, real* out) {
+    const int n3 = 3 * M.n;
+    std::vector<real> per((size_t)M.m * M.k * 3, 0);
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < M.m; ++e)
+        for (int smp = 0; smp < M.s; ++smp) {
+            const M3 dF = def_grad(M, e, smp, u);
+            const real* J = &Jall[((size_t)e * M.s + smp) * 81];
+            M3 P = zero3();
+            for (int col = 0; col < 9; ++col)
+                for (int i = 0; i < 9; ++i) P.a[i] += J[col * 9 + i] * dF.a[col];
+            add_At(M, e, smp, P, 1.0, &per[(size_t)e * M.k * 3]);
+        }
+    std::fill(out, out + n3, 0.0);
+    for (int e = 0; e < M.m; ++e)
+        for (int a = 0; a < M.k; ++a)
+            for (int i = 0; i < 3; ++i) out[3 * M.E[(size_t)e * M.k + a] + i] += per[((size_t)e * M.k + a) * 3 + i];
+}
+
 static int count_params(const Model& M) {
     int t = 0;
     for (const auto& en : M.energies) t += (int)en.params.size();
@@ -1260,6 +1370,14 @@ static void backward(Model& M, const real* q, const real* v, const real* f_ext, 
 #pragma omp parallel for
     for (int e = 0; e < M.m; ++e)
         for (int smp = 0; smp < M.s; ++smp) svd[e][smp] = make_svd(def_grad(M, e, smp, q_next));
+    std::vector<real> Jf;
+    int nfilt = 0;
+    if (opt.eigen_filter) nfilt = build_filtered_jacobians(M, svd, opt.mean_stiffness_bwd != 0, opt.eigen_filter, Jf);
+    M.last_filtered = nfilt;
+    auto kpd_apply = [&](const real* u, real* out) {
+        if (opt.eigen_filter) apply_kpd_J(M, Jf, u, out);
+        else apply_kpd(M, svd, u, out, opt.mean_stiffness_bwd != 0);
+    };
     std::vector<real> mu(n3, 0), kpd(n3), rhs(n3), nx(n3);
     auto clip = [&](std::vector<real>& x) {
         for (auto& val : x)
@@ -1271,7 +1389,7 @@ static void backward(Model& M, const real* q, const real* v, const real* f_ext, 
     Anderson aa{opt.aa_window, {}, {}};
     int iters = 0;
     for (int it = 0; it < opt.max_pd_iter; ++it) {
-        apply_kpd(M, svd, mu.data(), kpd.data(), opt.mean_stiffness_bwd != 0);
+        kpd_apply(mu.data(), kpd.data());
         for (int i = 0; i < n3; ++i) rhs[i] = gbar[i] + kpd[i];
         apply_ainv(M, rhs.data(), nx.data());
         for (const auto& kv : M.dirichlet) nx[kv.first] = 0;
@@ -1411,7 +1529,7 @@ static void backward(Model& M, const real* q, const real* v, const real* f_ext, 
                 for (int d = 0; d < 3; ++d) j[3 * node + d] = sc * dir[d];
                 Anderson wa{opt.aa_window, {}, {}};
                 for (int it = 0; it < wmax; ++it) {
-                    apply_kpd(M, svd, sv.data(), kp.data(), opt.mean_stiffness_bwd != 0);
+                    kpd_apply(sv.data(), kp.data());
                     for (int i = 0; i < n3; ++i) rh[i] = j[i] + kp[i];
                     apply_ainv(M, rh.data(), sn.data());
                     for (const auto& kv : M.dirichlet) sn[kv.first] = 0;
@@ -1561,6 +1679,7 @@ Options parse_opts(const char** keys, const double* vals, int n) {
     if (m.count("alg_phd_bwd_rhs_prune_abs")) o.rhs_prune_abs = m["alg_phd_bwd_rhs_prune_abs"];
     if (m.count("alg_phd_bwd_basis_topk")) o.basis_topk = (int)m["alg_phd_bwd_basis_topk"];
     if (m.count("alg_phd_bwd_wt_max_iter")) o.wt_max_iter = (int)m["alg_phd_bwd_wt_max_iter"];
+    if (m.count("bwd_eigen_filter")) o.eigen_filter = (int)m["bwd_eigen_filter"];
 #ifdef _OPENMP
     if ((int)m["thread_ct"] > 0) omp_set_num_threads((int)m["thread_ct"]);
 #endif
@@ -1681,6 +1800,7 @@ ORC_API int orc_set_planar_boundary(void* h, const double* p4, const int* idx, i
 ORC_API int orc_num_params(void* h) { return count_params(((Handle*)h)->M); }
 ORC_API double orc_mass(void* h) { return ((Handle*)h)->M.mass(); }
 ORC_API int orc_last_iters(void* h) { return ((Handle*)h)->M.last_iters; }
+ORC_API int orc_last_filtered(void* h) { return ((Handle*)h)->M.last_filtered; }
 ORC_API int orc_last_converged(void* h) { return ((Handle*)h)->M.last_converged; }
 ORC_API void orc_reset_warm_start(void* h) {
     ((Handle*)h)->M.prev_cand.clear();
