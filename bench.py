@@ -158,9 +158,14 @@ def run_ainv_only(args):
                       "stored_values": d.s_padded_values()}))
 
 
+HOST_LOOP = False  # --host-loop: iteration loops replayed from the host (profilers see each kernel launch)
+
+
 def options(sc, precision, warm=False):
     o = dict(sc.options)
     o["thread_ct"] = os.cpu_count() or 8
+    if HOST_LOOP:
+        o["graph_while"] = 0
     o["alg_phd_bwd_solver"] = 1   # conjugate-gradient adjoint, stopped by the reference's 1e-6 step rule
     if precision == "mixed":
         o["fp32_bulk"] = 1
@@ -303,6 +308,7 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
     ev = []
     bwd_iters = []
     with ClockSampler(local_rank) as clk, torch.cuda.stream(stream):
+        torch.cuda.nvtx.range_push("timed_value")  # lets a profiler restrict itself to the timed steps
         q, v = q_start, v_start
         qs, vs = [q], [v]
         for _ in range(args.steps):
@@ -328,6 +334,7 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
             bwd_iters.append(d._L.dphd_last_backward_iters(d._h))
             gq, gv = dq, dv
         stream.synchronize()
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -474,10 +481,15 @@ def main():
                     help="profiling mode: only apply the S^T S pair this many times on --scene")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true", help="headline without the learned / adjoint starts")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="profiling: replay each iteration graph from the host instead of one device-side WHILE "
+                         "graph per solve (same kernels; ncu does not profile kernels inside conditional nodes)")
     ap.add_argument("--ws-seeds", type=int, default=8, help="material seeds of the warm-start training rollouts")
     ap.add_argument("--ws-steps", type=int, default=60, help="rollout steps per training seed")
     ap.add_argument("--ws-fit-steps", type=int, default=1500, help="AdamW steps of warm-start training")
     args = ap.parse_args()
+    global HOST_LOOP
+    HOST_LOOP = args.host_loop
     if args.warmup < 3:
         args.warmup = 3
     if args.ainv_reps > 0:

@@ -96,6 +96,7 @@ def load_library():
     L.dphd_warmstart_apply.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 4
     L.dphd_warmstart_target.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 4
     L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+    L.dphd_debug_s_rows.argtypes = [C.c_void_p, C.c_double, _ip, _ip]
     L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     _lib = L
     return L
@@ -390,6 +391,13 @@ class Deformable:
         return int(self._L.dphd_s_nnz(self._h))
 
     # ---- diagnostics -----------------------------------------------------------------------------
+    def debug_s_rows(self, dt):
+        """(lo, perm): first column of each row of the sparse inverse factor S and the permutation (host only)."""
+        n = self.dofs() // 3
+        lo, perm = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self._check(self._L.dphd_debug_s_rows(self._h, float(dt), _iptr(lo), _iptr(perm)))
+        return lo, perm
+
     def debug_ainv(self, b, dt, fp32=False):
         b = _arr(b, self.dofs())
         x = np.zeros_like(b)

@@ -414,6 +414,22 @@ int dphd_contact_adjoint_stats(const dphd_deformable* h, int* source, int* const
 long long dphd_s_memory_bytes(const dphd_deformable* h) { return h && h->eng ? h->eng->s_memory_bytes() : -1; }
 long long dphd_s_nnz(const dphd_deformable* h) { return h && h->eng ? h->eng->s_nnz() : -1; }
 
+int dphd_debug_s_rows(dphd_deformable* h, double dt, int* row_lo, int* perm) {
+    return guard([&] {
+        dphd::Engine& e = E(h);
+        DPHD_CHECK(e.M.n > 0, "Deformable is not initialized.");
+        dphd::init_samples(e.M);
+        const dphd::NodeMatrix A = dphd::assemble_A(e.M, dt);
+        const std::vector<int> order = dphd::nested_dissection(e.M, A);
+        dphd::SFactor S;
+        dphd::build_sfactor(A, order, S, 0);
+        for (int i = 0; i < S.n; ++i) {
+            if (row_lo) row_lo[i] = S.lo[i];
+            if (perm) perm[i] = S.perm[i];
+        }
+    });
+}
+
 int dphd_debug_ainv(dphd_deformable* h, double dt, const double* b, double* x, int fp32) {
     return guard([&] { E(h).apply_ainv(dt, b, x, fp32 != 0); });
 }

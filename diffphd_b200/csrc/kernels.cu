@@ -198,6 +198,47 @@ __device__ __forceinline__ void group_sum(T& a) {
     for (int o = kGatherLanes / 2; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
 }
 
+
+// Sum of a node's incident element contributions eo[node_inc[idx]] (3 doubles each) over idx in [b, e), this
+// lane taking idx = b + lane, b + lane + kGatherLanes, ...; four indices are loaded before their values so
+// that a lane has several independent loads in flight instead of a chain of dependent ones.
+__device__ __forceinline__ void sum_incident(const int* __restrict__ node_inc, const double* __restrict__ eo, int b,
+                                             int e, int lane, double* p) {
+    for (int idx = b + lane; idx < e; idx += 4 * kGatherLanes) {
+        int k[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) k[u] = idx + u * kGatherLanes < e ? __ldg(node_inc + idx + u * kGatherLanes) : -1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k[u] >= 0) {
+                const double* c = eo + (size_t)k[u] * 3;
+                p[0] += c[0]; p[1] += c[1]; p[2] += c[2];
+            }
+    }
+}
+
+// sum_k A.v[k] x[3 A.ci[k] + d] over this lane's share of the row [r0, r1), batched like sum_incident
+__device__ __forceinline__ void csr_row_product(const NodeCsr& A, const double* __restrict__ x, int r0, int r1, int lane,
+                                                double* acc) {
+    for (int k0 = r0 + lane; k0 < r1; k0 += 4 * kGatherLanes) {
+        int c[4];
+        double a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * kGatherLanes;
+            c[u] = k < r1 ? __ldg(A.ci + k) : -1;
+            a[u] = k < r1 ? __ldg(A.v + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (c[u] >= 0) {
+                acc[0] += a[u] * x[3 * c[u]];
+                acc[1] += a[u] * x[3 * c[u] + 1];
+                acc[2] += a[u] * x[3 * c[u] + 2];
+            }
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __restrict__ node_ptr,
                                                          const int* __restrict__ node_inc, const double* __restrict__ eo,
@@ -218,20 +259,8 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
         const bool fx = valid ? fixed[i] != 0 : true;
         double p[3] = {0.0, 0.0, 0.0}, aq[3] = {0.0, 0.0, 0.0};
         if (valid) {
-            const int b = node_ptr[i], e = node_ptr[i + 1];
-            for (int idx = b + lane; idx < e; idx += kGatherLanes) {
-                const double* c = eo + (size_t)node_inc[idx] * 3;
-                p[0] += c[0]; p[1] += c[1]; p[2] += c[2];
-            }
-            if (A.rp && !fx) {
-                for (int k = A.rp[i] + lane; k < A.rp[i + 1]; k += kGatherLanes) {
-                    const int c = A.ci[k];
-                    const double a = A.v[k];
-                    aq[0] += a * q[3 * c];
-                    aq[1] += a * q[3 * c + 1];
-                    aq[2] += a * q[3 * c + 2];
-                }
-            }
+            sum_incident(node_inc, eo, node_ptr[i], node_ptr[i + 1], lane, p);
+            if (A.rp && !fx) csr_row_product(A, q, A.rp[i], A.rp[i + 1], lane, aq);
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -300,9 +329,8 @@ template <> struct Vec4<double> {
 // y = S v, stage 1: one warp per work item (a row segment of <= kSegCols columns), four 16-byte loads of S
 // in flight per lane, v through L1 (the CTA's warps share the segment's columns).
 template <typename T>
-__global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __restrict__ v, const Ctrl* ctrl) {
-    if (ctrl->done) return;
-    const int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+__device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __restrict__ v, int vb) {
+    const int it = (vb * (int)blockDim.x + (int)threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (it >= p.n_items) return;
     const int4 dsc = __ldg(p.item_desc + it);
     const int slot = __ldg(p.item_slot + it);
@@ -354,6 +382,12 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __restrict__ v, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    s_items_body(p, v, blockIdx.x);
+}
+
 // y = S v, stage 2: per row, the item partials in item order.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __restrict__ y, const Ctrl* ctrl) {
@@ -383,10 +417,9 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
 constexpr int kStRows = 4;
 
 template <typename T, bool FROM_ITEMS>
-__global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
-    if (ctrl->done) return;
+__device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __restrict__ y, int ch) {
     __shared__ T red[8][3][kTileCols];
-    const int ch = blockIdx.x, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tile = __ldg(p.chunk_tile + ch);
     const int c = tile * kTileCols + lane * 4;
     const int npad = p.npad;
@@ -453,25 +486,44 @@ __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __
         for (int w = 0; w < 8; ++w) s += red[w][d][col];
         p.xpart[(size_t)ch * 3 * kTileCols + t] = s;
     }
+    __syncthreads();  // `red` is reused by the next chunk of a persistent CTA
+}
+
+template <typename T, bool FROM_ITEMS>
+__global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    st_part_body<T, FROM_ITEMS>(p, y, blockIdx.x);
 }
 
 // x = S^T y, stage 2: per tile column, sum the chunk partials in order and scatter to node-major x.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double* __restrict__ x_out,
-                                                          const Ctrl* ctrl) {
-    if (ctrl->done) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void st_fin_body(const SpmvPlan<T>& p, double* __restrict__ x_out, int vb) {
+    const int t = vb * (int)blockDim.x + (int)threadIdx.x;
     if (t >= p.ntiles * 3 * kTileCols) return;
     const int tile = t / (3 * kTileCols), r = t % (3 * kTileCols);
     const int d = r / kTileCols, col = r % kTileCols;
     const int j = tile * kTileCols + col;
     if (j >= p.n) return;
     double s = 0.0;
-    for (int ch = __ldg(p.tile_chunk_ptr + tile); ch < __ldg(p.tile_chunk_ptr + tile + 1); ++ch)
-        s += (double)p.xpart[(size_t)ch * 3 * kTileCols + r];
+    const int c0 = __ldg(p.tile_chunk_ptr + tile), c1 = __ldg(p.tile_chunk_ptr + tile + 1);
+    for (int ch = c0; ch < c1; ch += 8) {  // eight independent loads in flight, summed in chunk order
+        T t8[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t8[u] = ch + u < c1 ? p.xpart[(size_t)(ch + u) * 3 * kTileCols + r] : T(0);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += (double)t8[u];
+    }
     const size_t o = 3 * (size_t)__ldg(p.perm + j) + d;
     x_out[o] = p.x_base ? p.x_base[o] + s : s;
 }
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double* __restrict__ x_out,
+                                                          const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    st_fin_body(p, x_out, blockIdx.x);
+}
+
 
 // ------------------------------------------------------------------------------------------------
 // Type-II Anderson acceleration (forward_gpu.cpp:1340-1379; backward_gpu.cpp:825-859) and the gate.
@@ -888,12 +940,9 @@ __global__ void __launch_bounds__(kThreads) k_gather_bwd(int n, const int* __res
     for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
         const int i = base + (int)threadIdx.x / kGatherLanes;
         const bool valid = i < n;
-        double p0 = 0, p1 = 0, p2 = 0;
-        if (valid)
-            for (int idx = node_ptr[i] + lane; idx < node_ptr[i + 1]; idx += kGatherLanes) {
-                const double* c = eo + (size_t)node_inc[idx] * 3;
-                p0 += c[0]; p1 += c[1]; p2 += c[2];
-            }
+        double pp[3] = {0.0, 0.0, 0.0};
+        if (valid) sum_incident(node_inc, eo, node_ptr[i], node_ptr[i + 1], lane, pp);
+        double p0 = pp[0], p1 = pp[1], p2 = pp[2];
         group_sum(p0);
         group_sum(p1);
         group_sum(p2);
@@ -1030,17 +1079,12 @@ __global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const
         const bool fx = valid ? fixed[i] != 0 : true;
         double a0 = 0, a1 = 0, a2 = 0;
         if (valid && !fx) {
-            for (int k = A.rp[i] + lane; k < A.rp[i + 1]; k += kGatherLanes) {
-                const int c = A.ci[k];
-                const double a = A.v[k];
-                a0 += a * p[3 * c];
-                a1 += a * p[3 * c + 1];
-                a2 += a * p[3 * c + 2];
-            }
-            for (int idx = node_ptr[i] + lane; idx < node_ptr[i + 1]; idx += kGatherLanes) {
-                const double* c = eo + (size_t)node_inc[idx] * 3;
-                a0 -= c[0]; a1 -= c[1]; a2 -= c[2];
-            }
+            double ap[3] = {0.0, 0.0, 0.0}, kp[3] = {0.0, 0.0, 0.0};
+            csr_row_product(A, p, A.rp[i], A.rp[i + 1], lane, ap);
+            sum_incident(node_inc, eo, node_ptr[i], node_ptr[i + 1], lane, kp);
+            a0 = ap[0] - kp[0];
+            a1 = ap[1] - kp[1];
+            a2 = ap[2] - kp[2];
         }
         group_sum(a0);
         group_sum(a1);
@@ -1520,6 +1564,7 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap) {
 void launch_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap, cudaStream_t st) {
     k_loop_cond<<<1, 1, 0, st>>>(h, ctrl, cap);
 }
+
 
 template void launch_sts<double>(const SpmvPlan<double>&, const double*, double*, double*, const Ctrl*,
                                  cudaStream_t);

@@ -105,6 +105,7 @@ constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
 
+
 // Anderson acceleration + gate ------------------------------------------------------------------
 void launch_aa_reduce(int n3, const double* x, const double* x_raw, const unsigned char* fixed_dof,
                       const double* fixed_val, double* dG, double* dX, double* last_g, double* last_x, int ld,

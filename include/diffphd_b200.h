@@ -188,6 +188,9 @@ int dphd_warmstart_target(dphd_deformable* h, double dt, const double* d_q_next,
  * with the host copy of S (the set-up self-check of forward_gpu.cpp:653-670), and the GPU local step
  * (ProjectiveDynamicsLocalStep, deformable_projective_dynamics_forward.cpp:186-292). */
 int dphd_debug_ainv(dphd_deformable* h, double dt, const double* b, double* x, int fp32);
+/* Host-only structure of the sparse inverse factor (no GPU needed): per S row its first column lo_i (row i is
+ * dense on [lo_i, i]) and the node at each permuted position. */
+int dphd_debug_s_rows(dphd_deformable* h, double dt, int* row_lo, int* perm);
 int dphd_debug_host_sts(dphd_deformable* h, double dt, const double* b, double* x);
 int dphd_debug_local_step(dphd_deformable* h, double dt, const double* q, double* rhs);
 /* Average device time (ms, CUDA events on the library's stream) of one S^T S pair over `reps` applications,
