@@ -707,8 +707,12 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected) {
     const int n = M.n, n3 = 3 * n;
     Ctrl* c = d_ctrl.as<Ctrl>();
     const int capK = has_contact_ ? contact_.K : 0;
-    launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_pp.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
-                    d_elem_out64.as<double>(), c, st);
+    if (f32)  // mixed precision: FP32 packed symmetric Jacobians (a quarter of the bytes), FP64 sums
+        launch_kpd_elem32(M.m, M.k, M.s, dE.as<int>(), d_pp.as<double>(), dgrad.as<double>(), M.hex,
+                          d_J32.as<float>(), d_elem_out64.as<double>(), c, st);
+    else
+        launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_pp.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
+                        d_elem_out64.as<double>(), c, st);
     launch_pcg_gather(n, Acsr_, d_pp.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
                       d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
                       d_part_gate.as<double>(), gather_blocks_, c, st);
@@ -1288,8 +1292,11 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
     Ctrl* c = d_ctrl.as<Ctrl>();
     init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
     CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    const bool j32 = o.fp32_bulk && o.bwd_solver == 1;
+    if (j32) d_J32.alloc((size_t)m * M.s * 48 * sizeof(float));
     launch_jac_build(m, M.k, M.s, dE.as<int>(), d_q_next, dgrad.as<double>(), M.hex, vol_over_s, ep,
-                     o.bwd_mean_stiffness, o.bwd_eigen_filter, d_J.as<double>(), c, st);
+                     o.bwd_mean_stiffness, o.bwd_eigen_filter, d_J.as<double>(), j32 ? d_J32.as<float>() : nullptr, c,
+                     st);
     CUDA_OK(cudaMemsetAsync(d_x.p, 0, n3 * sizeof(double), st));
     launches_ += 2;
     if (graph_dt_ != h) {

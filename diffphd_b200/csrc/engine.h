@@ -215,7 +215,7 @@ private:
     DeviceBuffer d_elem_out64, d_elem_out32, d_vperm64, d_vperm32, d_y64, d_y32;
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
-    DeviceBuffer d_item_desc, d_item_slot, d_trow_desc, d_trow_off;
+    DeviceBuffer d_item_desc, d_item_slot, d_trow_desc, d_trow_off, d_J32;
     DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv, d_wlog, d_mu_prev;
     bool mu_prev_valid_ = false;
     const double* ws_predict(const double* d_q, const double* d_v, const double* d_f, double dt, cudaStream_t st);

@@ -807,10 +807,21 @@ __device__ void jacobi_eig9(double* A, double* Q) {
     }
 }
 
+// FP32 copy of a symmetric 9x9 Jacobian (the projections' differentials are Hessians of scalar functions):
+// upper triangle, row by row, (J_ic + J_ci) / 2, padded to 48 floats for 16-byte loads.
+constexpr int kJ32Stride = 48;
+__device__ __forceinline__ void pack_sym32(const double* Jt, float* o) {
+    int k = 0;
+    for (int i = 0; i < 9; ++i)
+        for (int c = i; c < 9; ++c) o[k++] = (float)(0.5 * (Jt[c * 9 + i] + Jt[i * 9 + c]));
+    for (; k < kJ32Stride; ++k) o[k] = 0.f;
+}
+
 template <int K, int S>
 __global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict__ E, const double* __restrict__ q,
                                                    const double* __restrict__ grad, double vol_over_s, EnergyPack ep,
-                                                   int mean_w, int filter, double* __restrict__ J, Ctrl* ctrl) {
+                                                   int mean_w, int filter, double* __restrict__ J,
+                                                   float* __restrict__ J32, Ctrl* ctrl) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = t / S, smp = t % S;
     if (e >= m) return;
@@ -840,7 +851,10 @@ __global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict_
 #pragma unroll
         for (int i = 0; i < 9; ++i) Jt[col * 9 + i] = out[i];  // column col (column-major 9x9)
     }
-    if (filter == 0) return;
+    if (filter == 0) {
+        if (J32) pack_sym32(Jt, J32 + (size_t)t * kJ32Stride);
+        return;
+    }
     // State-adaptive filter of the local Hessian H = wsum I - J (the PD energy's per-sample Hessian), with the
     // rule of ProjectedNewtonMatrix (cpp/core/src/fem/deformable_newton_forward.cpp:394-434): kept as is when
     // diagonally dominant (|H_kk| >= sum_j |H_kj| + 1e-5 in every row); otherwise eigen-decomposed and its
@@ -855,7 +869,10 @@ __global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict_
             if (j != i) off += fabs(H[i * 9 + j]);
         dd = !(fabs(H[i * 9 + i]) < off + 1e-5);
     }
-    if (dd) return;
+    if (dd) {
+        if (J32) pack_sym32(Jt, J32 + (size_t)t * kJ32Stride);
+        return;
+    }
     double Q[81];
     jacobi_eig9(H, Q);
     double lam[9];
@@ -870,6 +887,7 @@ __global__ void __launch_bounds__(128) k_jac_build(int m, const int* __restrict_
             Jt[j * 9 + i] = (i == j ? wsum : 0.0) - h;
         }
     atomicAdd(&ctrl->arrive[3], 1u);  // number of filtered samples (diagnostic)
+    if (J32) pack_sym32(Jt, J32 + (size_t)t * kJ32Stride);
 }
 
 template <int K, int S>
@@ -902,6 +920,76 @@ __global__ void __launch_bounds__(kThreads) k_kpd_elem(int m, const int* __restr
             const double g0 = __ldg(g + a * 3), g1 = __ldg(g + a * 3 + 1), g2 = __ldg(g + a * 3 + 2);
 #pragma unroll
             for (int i = 0; i < 3; ++i) acc[a][i] = P[i] * g0 + P[i + 3] * g1 + P[i + 6] * g2;
+        }
+    }
+    if (S == 8) {
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+            for (int a = 0; a < K; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) acc[a][i] += __shfl_xor_sync(0xffffffffu, acc[a][i], o);
+        if (valid) {
+#pragma unroll
+            for (int a = 0; a < K; ++a)
+                if (a == smp) {
+                    double* o = out + ((size_t)e * K + a) * 3;
+                    o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
+                }
+        }
+    } else if (valid) {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            double* o = out + ((size_t)e * K + a) * 3;
+            o[0] = acc[a][0]; o[1] = acc[a][1]; o[2] = acc[a][2];
+        }
+    }
+}
+
+// K_pd u from the FP32 packed symmetric Jacobians (mixed precision): P = J dF in FP32, element sums in FP64.
+template <int K, int S>
+__global__ void __launch_bounds__(kThreads) k_kpd_elem32(int m, const int* __restrict__ E,
+                                                         const double* __restrict__ u, const double* __restrict__ grad,
+                                                         const float* __restrict__ J32, double* __restrict__ out,
+                                                         const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = t / S, smp = t % S;
+    const bool valid = e < m;
+    double acc[K][3];
+#pragma unroll
+    for (int a = 0; a < K; ++a) acc[a][0] = acc[a][1] = acc[a][2] = 0.0;
+    if (valid) {
+        const double* g = (S == 8) ? grad + smp * 24 : grad + (size_t)e * 12;
+        float Mv[kJ32Stride];
+        const float4* src = reinterpret_cast<const float4*>(J32 + (size_t)t * kJ32Stride);
+#pragma unroll
+        for (int k = 0; k < kJ32Stride / 4; ++k) {
+            const float4 x = __ldg(src + k);
+            Mv[4 * k] = x.x; Mv[4 * k + 1] = x.y; Mv[4 * k + 2] = x.z; Mv[4 * k + 3] = x.w;
+        }
+        double dFd[9];
+        def_grad<K>(E, e, u, g, dFd);
+        float dF[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) dF[i] = (float)dFd[i];
+        float P[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) P[i] = 0.f;
+        int k = 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+#pragma unroll
+            for (int c = i; c < 9; ++c, ++k) {
+                P[i] += Mv[k] * dF[c];
+                if (c != i) P[c] += Mv[k] * dF[i];
+            }
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            const double g0 = __ldg(g + a * 3), g1 = __ldg(g + a * 3 + 1), g2 = __ldg(g + a * 3 + 2);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                acc[a][i] = (double)P[i] * g0 + (double)P[i + 3] * g1 + (double)P[i + 6] * g2;
         }
     }
     if (S == 8) {
@@ -1366,12 +1454,20 @@ void launch_velocity(int n3, const double* q_next, const double* q, double inv_h
 }
 
 void launch_jac_build(int m, int k, int s, const int* E, const double* q, const double* grad, int hex,
-                      double vol_over_s, const EnergyPack& ep, int mean_w, int filter, double* J, Ctrl* ctrl,
-                      cudaStream_t st) {
+                      double vol_over_s, const EnergyPack& ep, int mean_w, int filter, double* J, float* J32,
+                      Ctrl* ctrl, cudaStream_t st) {
     (void)k;
     const int grid = blocks_for((long long)m * s, 128);
-    if (hex) k_jac_build<8, 8><<<grid, 128, 0, st>>>(m, E, q, grad, vol_over_s, ep, mean_w, filter, J, ctrl);
-    else k_jac_build<4, 1><<<grid, 128, 0, st>>>(m, E, q, grad, vol_over_s, ep, mean_w, filter, J, ctrl);
+    if (hex) k_jac_build<8, 8><<<grid, 128, 0, st>>>(m, E, q, grad, vol_over_s, ep, mean_w, filter, J, J32, ctrl);
+    else k_jac_build<4, 1><<<grid, 128, 0, st>>>(m, E, q, grad, vol_over_s, ep, mean_w, filter, J, J32, ctrl);
+}
+
+void launch_kpd_elem32(int m, int k, int s, const int* E, const double* u, const double* grad, int hex,
+                       const float* J32, double* elem_out, const Ctrl* ctrl, cudaStream_t st) {
+    (void)k;
+    const int grid = blocks_for((long long)m * s, kThreads);
+    if (hex) k_kpd_elem32<8, 8><<<grid, kThreads, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
+    else k_kpd_elem32<4, 1><<<grid, kThreads, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
 }
 
 void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const double* grad, int hex, const double* J,

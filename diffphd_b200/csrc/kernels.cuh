@@ -121,12 +121,15 @@ void launch_velocity(int n3, const double* q_next, const double* q, double inv_h
 
 // Adjoint ------------------------------------------------------------------------------------------
 // Per-sample 9x9 local Jacobians J_s = sum_energies w (vol/s) dBp/dF at q_next (optionally eigen-filtered).
+// With J32 set, also an FP32 packed symmetric copy (48 floats per sample) for the mixed-precision adjoint.
 void launch_jac_build(int m, int k, int s, const int* E, const double* q, const double* grad, int hex,
-                      double vol_over_s, const EnergyPack& ep, int mean_w, int filter, double* J, Ctrl* ctrl,
-                      cudaStream_t st);
+                      double vol_over_s, const EnergyPack& ep, int mean_w, int filter, double* J, float* J32,
+                      Ctrl* ctrl, cudaStream_t st);
 // K_pd u element contributions from the cached Jacobians.
 void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const double* grad, int hex, const double* J,
                      double* elem_out, const Ctrl* ctrl, cudaStream_t st);
+void launch_kpd_elem32(int m, int k, int s, const int* E, const double* u, const double* grad, int hex,
+                       const float* J32, double* elem_out, const Ctrl* ctrl, cudaStream_t st);
 // rhs = gbar + K_pd u, Dirichlet rows zero, permuted SoA.
 void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* gbar,
                        const unsigned char* fixed_node, const int* iperm, double* v_perm, int npad, const Ctrl* ctrl,

@@ -205,7 +205,9 @@ def test_device_entry_points_match_host_entry_points():
 @pytest.mark.parametrize("fp32", [0, 1])
 def test_pcg_adjoint_matches_converged_oracle_adjoint(fp32):
     """The conjugate-gradient adjoint (FP64 residual against A, S^T S preconditioner in FP64 or FP32) reaches
-    the converged adjoint of the oracle to 1e-7."""
+    the converged adjoint of the oracle to 1e-7 in FP64.  In mixed precision the K_pd apply also runs in FP32
+    (packed symmetric per-sample Jacobians), so the converged adjoint carries that operator's rounding: 5e-6
+    (measured about 1e-6 on this block)."""
     sc = scenes.nh_tet_block(cells=(6, 3, 3), dx=0.01, steps=2)
     opts = dict(sc.options)
     opts.update(aa_window=0, rel_tol=1e-13, abs_tol=1e-16, max_pd_iter=20000)
@@ -218,9 +220,13 @@ def test_pcg_adjoint_matches_converged_oracle_adjoint(fp32):
     gopts = dict(opts, alg_phd_bwd_solver=1, fp32_bulk=fp32, rel_tol=1e-12, max_pd_iter=2000)
     out = d.backward("pd_eigen_alg_phd", qs[1], vs[1], [], sc.f_ext, sc.dt, qs[2], vs[2], [], gq, gv, gopts)
     assert out["iters"] < 2000
+    tol, ptol = (5e-6, 1e-5) if fp32 else (1e-7, 1e-6)
+    errs = {key: _rel(out[key], ref[key]) for key in ("dl_dq", "dl_dv", "dl_df_ext")}
+    errs["dl_dparams"] = _rel(out["dl_dparams"], np.concatenate(ref["dl_dparams"]))
+    print("relative errors vs the oracle:", errs)
     for key in ("dl_dq", "dl_dv", "dl_df_ext"):
-        assert _rel(out[key], ref[key]) < 1e-7, key
-    assert _rel(out["dl_dparams"], np.concatenate(ref["dl_dparams"])) < 1e-6
+        assert errs[key] < tol, (key, errs[key])
+    assert errs["dl_dparams"] < ptol, errs["dl_dparams"]
 
 
 def test_mixed_precision_forward_error_vs_fp64():
