@@ -174,6 +174,17 @@ def options(sc, precision, warm=False):
     return o
 
 
+def max_over_ranks(values, world, dev):
+    """Each value's maximum over the ranks of the process group (the slowest replica sets the job's time);
+    the values themselves when running alone."""
+    if world <= 1:
+        return [float(x) for x in values]
+    import torch
+    t = torch.tensor([float(x) for x in values], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def train_warm_start(dev, args):
     """Trains the warm-start MLP on plain-solver rollouts of held-out material seeds (not the timed seed 0)."""
     import torch
@@ -343,10 +354,7 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
     fwd_iters, conv = d.frame_stats()
 
     if not full:
-        if world > 1:
-            t = torch.tensor([t_dev], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            t_dev = float(t[0])
+        (t_dev,) = max_over_ranks([t_dev], world, dev)
         if rank != 0:
             return None
         return {"value": args.steps * world / t_dev, "ms_per_step": t_dev / args.steps * 1e3,
@@ -383,11 +391,7 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
     if world > 1:
         torch.distributed.barrier()
 
-    # max over ranks
-    if world > 1:
-        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_dev, t_e2e = float(t[0]), float(t[1])
+    t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], world, dev)
     if rank != 0:
         return None
 
