@@ -107,7 +107,8 @@ __global__ void __launch_bounds__(1024) k_ncp_prepare(ContactDev c, const double
 }
 
 // A^-1 b at active candidate nodes: dot of the node's S column path with y = S b (3 right-hand sides).
-__global__ void __launch_bounds__(256) k_ncp_ainvb(ContactDev c, const double* __restrict__ y, int npad,
+template <typename T>
+__global__ void __launch_bounds__(256) k_ncp_ainvb(ContactDev c, const T* __restrict__ y, int npad,
                                                    const double* __restrict__ x_base, const Ctrl* ctrl) {
     if (ctrl->done) return;
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -119,9 +120,9 @@ __global__ void __launch_bounds__(256) k_ncp_ainvb(ContactDev c, const double* _
     for (int d = lane; d < L; d += 32) {
         const int r = c.prow[o + d];
         const double v = c.pval[o + d];
-        s0 += v * y[r];
-        s1 += v * y[npad + r];
-        s2 += v * y[2 * (size_t)npad + r];
+        s0 += v * (double)y[r];
+        s1 += v * (double)y[npad + r];
+        s2 += v * (double)y[2 * (size_t)npad + r];
     }
     s0 = warp_sum_d(s0);
     s1 = warp_sum_d(s1);
@@ -135,19 +136,22 @@ __global__ void __launch_bounds__(256) k_ncp_ainvb(ContactDev c, const double* _
 }
 
 // Dense solve of the active NCP system, multiplier updates and the contact right-hand side (one CTA).
+// vcon: without r64, J^T f (zero elsewhere); with r64 (the FP64 residual of the refinement form), the S-pass
+// input itself, overwritten at the candidates with r + J^T f formed in FP64 (no FP32 cancellation of the two).
+template <typename T>
 __global__ void __launch_bounds__(1024) k_ncp_solve(ContactDev c, const double* __restrict__ q0,
-                                                    const int* __restrict__ iperm, double* __restrict__ vcon, int npad,
-                                                    Ctrl* ctrl) {
+                                                    const int* __restrict__ iperm, T* __restrict__ vcon, int npad,
+                                                    const double* __restrict__ r64, Ctrl* ctrl) {
     if (ctrl->done) return;
     const int K = c.K, ka = c.kact[0];
     const int tid = threadIdx.x, nt = blockDim.x;
     const double n0 = c.n[0], n1 = c.n[1], n2 = c.n[2];
     // clear the previous contact right-hand side at every candidate node
     for (int k = tid; k < K; k += nt) {
-        const int j = iperm[c.cand[k]];
-        vcon[j] = 0.0;
-        vcon[npad + j] = 0.0;
-        vcon[2 * (size_t)npad + j] = 0.0;
+        const int node = c.cand[k], j = iperm[node];
+        vcon[j] = r64 ? (T)r64[3 * node] : T(0);
+        vcon[npad + j] = r64 ? (T)r64[3 * node + 1] : T(0);
+        vcon[2 * (size_t)npad + j] = r64 ? (T)r64[3 * node + 2] : T(0);
     }
     if (ka == 0) {
         for (int k = tid; k < K; k += nt) c.lt1[k] = c.lt2[k] = 0.0;
@@ -268,10 +272,12 @@ __global__ void __launch_bounds__(1024) k_ncp_solve(ContactDev c, const double* 
     for (int a = tid; a < ka; a += nt) {
         const int k = c.act[a];
         const double fn = c.omega[k] * c.lam[k];
-        const int j = iperm[c.cand[k]];
-        vcon[j] = fn * n0 + c.lt1[k] * c.t1[0] + c.lt2[k] * c.t2[0];
-        vcon[npad + j] = fn * n1 + c.lt1[k] * c.t1[1] + c.lt2[k] * c.t2[1];
-        vcon[2 * (size_t)npad + j] = fn * n2 + c.lt1[k] * c.t1[2] + c.lt2[k] * c.t2[2];
+        const int node = c.cand[k], j = iperm[node];
+        const double r0 = r64 ? r64[3 * node] : 0.0, r1 = r64 ? r64[3 * node + 1] : 0.0,
+                     r2 = r64 ? r64[3 * node + 2] : 0.0;
+        vcon[j] = (T)(r0 + fn * n0 + c.lt1[k] * c.t1[0] + c.lt2[k] * c.t2[0]);
+        vcon[npad + j] = (T)(r1 + fn * n1 + c.lt1[k] * c.t1[1] + c.lt2[k] * c.t2[1]);
+        vcon[2 * (size_t)npad + j] = (T)(r2 + fn * n2 + c.lt1[k] * c.t1[2] + c.lt2[k] * c.t2[2]);
     }
 }
 
@@ -301,12 +307,18 @@ void launch_delassus(int K, const int64_t* off, const int* prow, const double* p
     if (npairs > 0) k_delassus<<<(unsigned)blocks, 256, 0, st>>>(K, off, prow, pval, G);
 }
 
-void launch_ncp_iteration(const ContactDev& c, const double* x, const double* y, int npad, const double* x_base,
-                          const double* q0, const int* iperm, double* vcon, Ctrl* ctrl, cudaStream_t st) {
+template <typename T>
+void launch_ncp_iteration(const ContactDev& c, const double* x, const T* y, int npad, const double* x_base,
+                          const double* q0, const int* iperm, T* vcon, const double* r64, Ctrl* ctrl,
+                          cudaStream_t st) {
     k_ncp_prepare<<<1, 1024, 0, st>>>(c, x, ctrl);
-    k_ncp_ainvb<<<(c.K * 32 + 255) / 256, 256, 0, st>>>(c, y, npad, x_base, ctrl);
-    k_ncp_solve<<<1, 1024, 0, st>>>(c, q0, iperm, vcon, npad, ctrl);
+    k_ncp_ainvb<T><<<(c.K * 32 + 255) / 256, 256, 0, st>>>(c, y, npad, x_base, ctrl);
+    k_ncp_solve<T><<<1, 1024, 0, st>>>(c, q0, iperm, vcon, npad, r64, ctrl);
 }
+template void launch_ncp_iteration<double>(const ContactDev&, const double*, const double*, int, const double*,
+                                           const double*, const int*, double*, const double*, Ctrl*, cudaStream_t);
+template void launch_ncp_iteration<float>(const ContactDev&, const double*, const float*, int, const double*,
+                                          const double*, const int*, float*, const double*, Ctrl*, cudaStream_t);
 
 void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,
                         double slop, cudaStream_t st) {

@@ -485,6 +485,7 @@ void Engine::build_device(int threads) {
     d_q0.alloc(ld * sizeof(double));
     d_vcon.alloc((size_t)npad_ * 3 * sizeof(double));
     CUDA_OK(cudaMemset(d_vcon.p, 0, d_vcon.bytes));
+    d_r64.alloc((size_t)n3 * sizeof(double));
     build_contact(built_dt_);
     drop_graphs();
     device_ready_ = true;
@@ -593,8 +594,44 @@ std::vector<double> Engine::contact_lambda() {
 
 // One PD iteration with contact (FP64): b (Dirichlet rows kept, as the reference's contact branch),
 // y = S b, NCP on the active set, y += S J^T f, x_raw = S^T y, Anderson + gate.
-void Engine::enqueue_contact_iteration(cudaStream_t st) {
+void Engine::enqueue_contact_iteration(cudaStream_t st, bool f32) {
     const int n = M.n, n3 = 3 * n;
+    const double inv_h2m = M.mass() / (graph_dt_ * graph_dt_);
+    const EnergyPack ep = energy_pack();
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    if (f32) {
+        // Mixed precision: FP32 projections and SpMVs in refinement form.  r = b - A x (FP64 against the node
+        // CSR of A, also kept in FP64), y = S r in FP32; the NCP sees A^-1 b = x + S^T-path(y) at the
+        // candidates and solves in FP64; the S input becomes r + J^T f (summed in FP64 at the candidates:
+        // near the fixed point the two nearly cancel there), y = S (r + J^T f), x_raw = x + S^T y.
+        launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                               d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, M.vol / M.s, ep,
+                               d_elem_out64.as<double>(), c, st);
+        launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
+                                 d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
+                                 d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
+                                 gather_blocks_, Acsr_, d_x.as<double>(), 1, c, st, d_r64.as<double>());
+        launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
+        launch_ncp_iteration<float>(contact_, d_x.as<double>(), d_y32.as<float>(), npad_, d_x.as<double>(),
+                                    d_q0.as<double>(), d_iperm.as<int>(), d_vperm32.as<float>(),
+                                    d_r64.as<double>(), c, st);
+        launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
+        SpmvPlan<float> ref = plan32_;
+        ref.x_base = d_x.as<double>();
+        launch_st_only<float>(ref, d_y32.as<float>(), d_xraw.as<double>(), c, st);
+    } else {
+        enqueue_contact_iteration64(st);
+    }
+    launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
+                     d_lx.as<double>(), n3, d_part_aa.as<double>(), red_blocks_, c, st);
+    launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
+                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3, d_part_upd.as<double>(),
+                     d_part_gate.as<double>(), gather_blocks_, red_blocks_, c, st);
+}
+
+void Engine::enqueue_contact_iteration64(cudaStream_t st) {
+    const int n = M.n;
     const double inv_h2m = M.mass() / (graph_dt_ * graph_dt_);
     const EnergyPack ep = energy_pack();
     Ctrl* c = d_ctrl.as<Ctrl>();
@@ -606,18 +643,12 @@ void Engine::enqueue_contact_iteration(cudaStream_t st) {
                               d_vperm64.as<double>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
                               gather_blocks_, NodeCsr(), nullptr, 0, c, st);
     launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
-    launch_ncp_iteration(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, nullptr, d_q0.as<double>(),
-                         d_iperm.as<int>(), d_vcon.as<double>(), c, st);
+    launch_ncp_iteration<double>(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, nullptr,
+                                 d_q0.as<double>(), d_iperm.as<int>(), d_vcon.as<double>(), nullptr, c, st);
     SpmvPlan<double> acc = plan64_;
     acc.y_accumulate = 1;
     launch_s_only<double>(acc, d_vcon.as<double>(), d_y64.as<double>(), c, st);
     launch_st_only<double>(plan64_, d_y64.as<double>(), d_xraw.as<double>(), c, st);
-    launch_aa_reduce(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
-                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), d_lg.as<double>(),
-                     d_lx.as<double>(), n3, d_part_aa.as<double>(), red_blocks_, c, st);
-    launch_aa_update(n3, d_x.as<double>(), d_xraw.as<double>(), d_fixed_dof.as<unsigned char>(),
-                     d_fixed_val.as<double>(), d_dG.as<double>(), d_dX.as<double>(), n3, d_part_upd.as<double>(),
-                     d_part_gate.as<double>(), gather_blocks_, red_blocks_, c, st);
 }
 
 EnergyPack Engine::energy_pack() const {
@@ -744,7 +775,7 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected) {
 // host and the control block polled every few iterations (doubling up to poll_chunk).
 void Engine::enqueue_iteration(int mode, cudaStream_t cap) {
     if (mode == 2) enqueue_bwd_iteration(cap);
-    else if (mode == 5) enqueue_contact_iteration(cap);
+    else if (mode == 5 || mode == 8) enqueue_contact_iteration(cap, mode == 8);
     else if (mode == 6 || mode == 7) enqueue_pcg_iteration(mode == 7, cap, true);
     else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
     else enqueue_fwd_iteration(mode == 1, cap);
@@ -873,16 +904,17 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
         graph_dt_ = h;
     }
     if (has_contact_) {
-        DPHD_CHECK(!o.fp32_bulk, "fp32_bulk is not available with frictional contact on this path yet.");
         contact_.mu = o.friction_mu;
         CUDA_OK(cudaMemsetAsync(dc_lt1.p, 0, dc_lt1.bytes, st));
         CUDA_OK(cudaMemsetAsync(dc_lt2.p, 0, dc_lt2.bytes, st));
-        if (graphs_[5] && graph_mu_ != o.friction_mu) {
-            cudaGraphExecDestroy(graphs_[5]);
-            graphs_[5] = nullptr;
-        }
+        if (graph_mu_ != o.friction_mu)  // the friction coefficient is captured in the contact iteration graphs
+            for (int md : {5, 8})
+                if (graphs_[md]) {
+                    cudaGraphExecDestroy(graphs_[md]);
+                    graphs_[md] = nullptr;
+                }
         graph_mu_ = o.friction_mu;
-        run_iterations(5, o, st);
+        run_iterations(o.fp32_bulk ? 8 : 5, o, st);
     } else {
         run_iterations(o.fp32_bulk ? 1 : 0, o, st);
     }

@@ -171,7 +171,8 @@ private:
     void contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t st);
     DeviceBuffer d_wb_nodes, d_wb_dirs, d_wb_ndir, d_wb_count, d_wb_gath, d_wb_mu, d_cmp, d_rq, d_rv;
     double* h_cmp_ = nullptr;
-    void enqueue_contact_iteration(cudaStream_t st);
+    void enqueue_contact_iteration(cudaStream_t st, bool f32);
+    void enqueue_contact_iteration64(cudaStream_t st);
     void build_contact(double dt);
     void enqueue_fwd_iteration(bool fp32, cudaStream_t st);
     void enqueue_bwd_iteration(cudaStream_t st);
@@ -186,8 +187,9 @@ private:
     NodeMatrix A;
     int npad_ = 0, ntiles_ = 0, red_blocks_ = 1, gather_blocks_ = 1;
     double graph_dt_ = -1, graph_mu_ = 0;
-    // 0 fwd64, 1 fwd mixed, 2 adjoint fixed point, 3/4 CG adjoint f64/f32, 5 contact, 6/7 projected CG f64/f32
-    static constexpr int kModes = 8;
+    // 0 fwd64, 1 fwd mixed, 2 adjoint fixed point, 3/4 CG adjoint f64/f32, 5 contact f64, 6/7 projected CG
+    // f64/f32, 8 contact mixed
+    static constexpr int kModes = 9;
     cudaGraphExec_t graphs_[kModes] = {};
     size_t graph_nodes_[kModes] = {};
     bool graph_is_while_[kModes] = {};
@@ -223,7 +225,7 @@ private:
     int ws_which_ = 0;
     DeviceBuffer d_ws_master, d_ws_packed, d_ws_X, d_ws_out, d_ws_base0, d_ws_base1, d_ws_qprev, d_ws_qinit;
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
-        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_M, dc_ltmp, d_vcon, d_q0;
+        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_M, dc_ltmp, d_vcon, d_r64, d_q0;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

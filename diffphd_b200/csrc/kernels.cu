@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
                                                          const int* __restrict__ iperm, T* __restrict__ v, int npad,
                                                          double* __restrict__ prev, double* __restrict__ part,
                                                          NodeCsr A, const double* __restrict__ q, int zero_dirichlet,
-                                                         Ctrl* ctrl) {
+                                                         double* __restrict__ r_out, Ctrl* ctrl) {
     if (ctrl->done) return;
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
@@ -275,8 +275,9 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
                 acc[0] += (p[d] - pr) * (p[d] - pr);
                 acc[1] += pr * pr;
                 prev[3 * i + d] = p[d];
-                v[(size_t)d * npad + j] =
-                    (fx && zero_dirichlet) ? T(0) : (T)(inv_h2m * qt[3 * i + d] + p[d] - aq[d]);
+                const double val = (fx && zero_dirichlet) ? 0.0 : inv_h2m * qt[3 * i + d] + p[d] - aq[d];
+                v[(size_t)d * npad + j] = (T)val;
+                if (r_out) r_out[3 * i + d] = val;
             }
         }
     }
@@ -1413,9 +1414,9 @@ template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
                        double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, int zero_dirichlet,
-                       Ctrl* ctrl, cudaStream_t st) {
+                       Ctrl* ctrl, cudaStream_t st, double* r_out) {
     k_gather_fwd<T><<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
-                                                     v_perm, npad, prev_pd, part, A, q, zero_dirichlet, ctrl);
+                                                     v_perm, npad, prev_pd, part, A, q, zero_dirichlet, r_out, ctrl);
 }
 
 template <typename T>
@@ -1501,10 +1502,10 @@ template void launch_elem_fwd<float>(int, int, int, const int*, const double*, c
                                      const double*, int, double, const EnergyPack&, double*, Ctrl*, cudaStream_t);
 template void launch_gather_fwd<double>(int, const int*, const int*, const double*, const double*, double,
                                         const unsigned char*, const int*, double*, int, double*, double*, int, NodeCsr,
-                                        const double*, int, Ctrl*, cudaStream_t);
+                                        const double*, int, Ctrl*, cudaStream_t, double*);
 template void launch_gather_fwd<float>(int, const int*, const int*, const double*, const double*, double,
                                        const unsigned char*, const int*, float*, int, double*, double*, int, NodeCsr,
-                                       const double*, int, Ctrl*, cudaStream_t);
+                                       const double*, int, Ctrl*, cudaStream_t, double*);
 
 void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
                        const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,

@@ -59,7 +59,8 @@ template <typename T>
 void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* qt,
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
                        double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, int zero_dirichlet,
-                       Ctrl* ctrl, cudaStream_t st);
+                       Ctrl* ctrl, cudaStream_t st,
+                       double* r_out = nullptr);
 // Sparse-inverse SpMV pair x = S^T (S v) (3 right-hand sides, permuted SoA v and y, x node-major FP64).
 // S row i: row_len[i] values from column row_a[i] (both multiples of 4) at vals[row_off[i]].
 template <typename T>
@@ -185,8 +186,13 @@ struct ContactDev {
     double* ltmp = nullptr;          // 2K
 };
 void launch_delassus(int K, const int64_t* off, const int* prow, const double* pval, double* G, cudaStream_t st);
-void launch_ncp_iteration(const ContactDev& c, const double* x, const double* y, int npad, const double* x_base,
-                          const double* q0, const int* iperm, double* vcon, Ctrl* ctrl, cudaStream_t st);
+// One NCP iteration: y (T) holds S r for the iteration's right-hand side (S b in FP64; S (b - A x) in the
+// FP32 refinement form, where x_base = x adds the current iterate back).  vcon (T) receives J^T f; with r64
+// (FP64 r, refinement form) vcon is the S-pass input and receives r + J^T f at the candidates instead.
+template <typename T>
+void launch_ncp_iteration(const ContactDev& c, const double* x, const T* y, int npad, const double* x_base,
+                          const double* q0, const int* iperm, T* vcon, const double* r64, Ctrl* ctrl,
+                          cudaStream_t st);
 void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,
                         double slop, cudaStream_t st);
 // y (+)= S v only (first half of the pair), and x = S^T y only (second half).

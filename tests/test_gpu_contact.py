@@ -61,3 +61,38 @@ def test_contact_rollout_matches_oracle_reference_defaults():
     q, _, _ = _roll_gpu(d, sc, sc.steps, opts)
     disp = np.abs(q_ref - sc.q0).max()
     assert np.abs(q - q_ref).max() <= 1e-4 * disp
+
+
+def test_contact_mixed_precision_vs_fp64():
+    """Contact in mixed precision (FP32 projections and S/S^T passes in refinement form, FP64 NCP solve and
+    residual), with a fixed number of PD iterations per step (gate disabled, so both precisions reach their
+    fixed points).  Frictionless, the 20-step rollout stays within 2e-6 of the FP64 one with the same active
+    sets (measured 2e-7 per step).  With friction the Coulomb stick/slip law amplifies FP32 rounding, so each
+    mixed step is compared from the same FP64 input state: within 2e-4 of the displacement from rest
+    (measured 9e-5 at worst over 14 steps)."""
+    sc = scenes.contact_drop(cells=(3, 3, 3), dx=0.02, steps=20, height=0.004, friction_mu=0.0)
+    opts = dict(sc.options)
+    opts.update(aa_window=0, rel_tol=0.0, abs_tol=0.0, max_pd_iter=2000, friction_mu=0.0, verbose=-1)
+    q64, _, acts64 = _roll_gpu(core.from_scene(sc), sc, sc.steps, opts)
+    q32, _, acts32 = _roll_gpu(core.from_scene(sc), sc, sc.steps, dict(opts, fp32_bulk=1))
+    assert any(len(a) for a in acts64), "the block never touched the plane"
+    assert acts32 == acts64
+    assert np.abs(q32 - q64).max() <= 2e-6 * np.abs(q64 - sc.q0).max()
+
+    sc = scenes.contact_drop(cells=(3, 3, 3), dx=0.02, steps=14, height=0.004, friction_mu=0.5)
+    opts.update(friction_mu=0.5)
+    d64, d32 = core.from_scene(sc), core.from_scene(sc)
+    q, v = sc.q0.copy(), sc.v0.copy()
+    touched, worst = 0, 0.0
+    for _ in range(sc.steps):
+        q6, v6, a6 = np.zeros(sc.dofs), np.zeros(sc.dofs), []
+        q3, v3, a3 = np.zeros(sc.dofs), np.zeros(sc.dofs), []
+        d64.PyForward("pd_eigen_alg_phd", q, v, [], sc.f_ext, sc.dt, opts, q6, v6, a6)
+        d32.PyForward("pd_eigen_alg_phd", q, v, [], sc.f_ext, sc.dt, dict(opts, fp32_bulk=1), q3, v3, a3)
+        assert sorted(a3) == sorted(a6)
+        touched += len(a6) > 0
+        worst = max(worst, np.abs(q3 - q6).max() / np.abs(q6 - sc.q0).max())
+        q, v = q6, v6
+    print("worst per-step mixed vs FP64 difference / displacement from rest:", worst)
+    assert touched > 0
+    assert worst <= 2e-4
