@@ -145,6 +145,58 @@ def build_scene(name=None):
     raise SystemExit(f"unknown scene {name}")
 
 
+def run_contact_drop(args):
+    """Secondary measurement on the contact-rich drop (24^3 hex block, E 5e5, nu 0.4, seeded rotation, dropped
+    onto z = 0, Coulomb mu 0.5, every node a candidate): W untimed FP64 steps bring the block into contact,
+    then K forward steps + their adjoints are timed in FP64 (reference starts) and in mixed precision with the
+    adjoint warm start.  Not the headline workload."""
+    import torch
+    from diffphd_b200 import core, scenes
+    dev = torch.device("cuda", 0)
+    sc = scenes.contact_drop()
+    out = {"metric": "sim steps/s fwd+adjoint, contact-rich drop (secondary)", "unit": "steps/s",
+           "config": {"workload": "contact_drop_hex_24x24x24_mu0.5", "nodes": sc.n, "elements": sc.m,
+                      "candidates": int(len(sc.plane[1])), "dt": sc.dt, "pre_contact_steps": args.warmup}}
+    for name, prec, warm in (("fp64", "f64", False), ("mixed_adjoint_warm", "mixed", True)):
+        d = core.from_scene(sc)
+        opts = options(sc, prec, warm=warm)
+        T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev).contiguous()
+        f = T(sc.f_ext)
+        q, v = T(sc.q0), T(sc.v0)
+        qn, vn = torch.empty_like(q), torch.empty_like(q)
+        o64 = options(sc, "f64")
+        for _ in range(args.warmup):  # free fall into contact
+            d.forward_device("pd_eigen_alg_phd", q, v, f, sc.dt, o64, qn, vn)
+            q, v = qn.clone(), vn.clone()
+        d.reset_frame_stats()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        qs, vs = [q], [v]
+        e0.record()
+        for _ in range(args.steps):
+            qn, vn = torch.empty_like(q), torch.empty_like(q)
+            d.forward_device("pd_eigen_alg_phd", qs[-1], vs[-1], f, sc.dt, opts, qn, vn)
+            qs.append(qn)
+            vs.append(vn)
+        g, gv = T(sc.extra.get("loss_r", np.ones(sc.dofs))), torch.zeros_like(q)
+        bw = []
+        for i in reversed(range(args.steps)):
+            dq, dv, df = torch.empty_like(g), torch.empty_like(g), torch.empty_like(g)
+            d.backward_device("pd_eigen_alg_phd", qs[i + 1], g, gv, sc.dt, opts, dq, dv, df)
+            bw.append(d._L.dphd_last_backward_iters(d._h))
+            g, gv = dq, dv
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        it, cv = d.frame_stats()
+        act = len(d.contact_lambda().nonzero())
+        out[name] = {"value": args.steps / t, "ms_per_step": t / args.steps * 1e3,
+                     "pd_iters_per_step": float(np.mean(it)), "adjoint_iters_per_step": float(np.mean(bw)),
+                     "converged_frac": float(np.mean(cv)), "active_contacts_last": int(act)}
+    out["speedup_mixed"] = out["mixed_adjoint_warm"]["value"] / out["fp64"]["value"]
+    print(json.dumps(out), flush=True)
+
+
 def run_ainv_only(args):
     """Kernel-only mode for profiling: builds the scene's factor, then applies the S^T S pair `reps` times."""
     import numpy as np
@@ -484,6 +536,8 @@ def main():
     ap.add_argument("--ainv-reps", type=int, default=0,
                     help="profiling mode: only apply the S^T S pair this many times on --scene")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--contact-drop", action="store_true",
+                    help="secondary measurement: the contact-rich 24^3 drop (--warmup = untimed free-fall steps)")
     ap.add_argument("--no-warm-start", action="store_true", help="headline without the learned / adjoint starts")
     ap.add_argument("--host-loop", action="store_true",
                     help="profiling: replay each iteration graph from the host instead of one device-side WHILE "
@@ -498,6 +552,9 @@ def main():
         args.warmup = 3
     if args.ainv_reps > 0:
         run_ainv_only(args)
+        return
+    if args.contact_drop:
+        run_contact_drop(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
