@@ -90,6 +90,8 @@ def load_library():
     L.dphd_contact_lambda_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.dphd_mlp_pack.argtypes = [C.c_void_p] * 3
     L.dphd_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.dphd_mlp_forward_tc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
     L.dphd_mlp_train_step.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_void_p] + [C.c_float] * 5 + \
         [C.c_int] + [C.c_void_p] * 5
     L.dphd_warmstart_features.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 8
@@ -97,6 +99,7 @@ def load_library():
     L.dphd_warmstart_target.argtypes = [C.c_void_p, C.c_double] + [C.c_void_p] * 4
     L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     L.dphd_debug_s_rows.argtypes = [C.c_void_p, C.c_double, _ip, _ip]
+    L.dphd_debug_set_s_kernel.argtypes = [C.c_void_p, C.c_int]
     L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     _lib = L
     return L
@@ -397,6 +400,11 @@ class Deformable:
         lo, perm = np.zeros(n, np.int32), np.zeros(n, np.int32)
         self._check(self._L.dphd_debug_s_rows(self._h, float(dt), _iptr(lo), _iptr(perm)))
         return lo, perm
+
+    def set_s_kernel(self, row_groups=True):
+        """FP32 y = S v pass: one warp per row group or one warp per row segment (bit-identical sums; by default
+        the faster one is picked by timing both when the factor is built)."""
+        self._check(self._L.dphd_debug_set_s_kernel(self._h, int(bool(row_groups))))
 
     def debug_ainv(self, b, dt, fp32=False):
         b = _arr(b, self.dofs())

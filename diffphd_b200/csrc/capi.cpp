@@ -303,6 +303,18 @@ int dphd_mlp_forward(float* d_master, void* d_packed, const void* d_X, int n, fl
     });
 }
 
+int dphd_mlp_forward_tc(float* d_master, void* d_packed, const void* d_X, int n, float* d_out, int* d_err,
+                        void* stream) {
+    return guard([&] {
+        DPHD_CHECK(d_master && d_packed && d_X && d_out && d_err, "null device pointer");
+        DPHD_CHECK(n >= 0, "negative row count");
+        DPHD_CHECK(((uintptr_t)d_X & 15) == 0 && ((uintptr_t)d_out & 15) == 0 && ((uintptr_t)d_packed & 15) == 0,
+                   "packed weights, X and out must be 16-byte aligned");
+        dphd::mlp_forward_tc_flat(d_master, d_packed, d_X, n, d_out, d_err, (cudaStream_t)stream);
+        CUDA_OK(cudaGetLastError());
+    });
+}
+
 int dphd_mlp_train_step(float* d_master, void* d_packed, const void* d_X, const float* d_Y, int n, float* d_part,
                         float lr, float beta1, float beta2, float eps, float weight_decay, int step, float* d_m,
                         float* d_v, float* d_grad, float* d_loss, void* stream) {
@@ -372,6 +384,10 @@ int dphd_debug_time_ainv(dphd_deformable* h, double dt, int reps, int fp32, int 
         DPHD_CHECK(ms_per_apply && reps > 0, "bad arguments");
         *ms_per_apply = E(h).time_ainv(dt, reps, fp32 != 0, flush_l2 != 0);
     });
+}
+
+int dphd_debug_set_s_kernel(dphd_deformable* h, int row_groups) {
+    return guard([&] { E(h).set_s_units(row_groups != 0); });
 }
 
 int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream) {

@@ -66,6 +66,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.basis_topk = (int)get("alg_phd_bwd_basis_topk", 0);
     o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
     o.graph_while = (int)get("graph_while", 1);
+    o.ws_tcgen05 = (int)get("ws_tcgen05", 1);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -91,6 +92,8 @@ void Engine::drop_graphs() {
 Engine::~Engine() {
     drop_graphs();
     if (h_ctrl_) cudaFreeHost(h_ctrl_);
+    if (h_cmp_) cudaFreeHost(h_cmp_);
+    if (h_ws_err_) cudaFreeHost(h_ws_err_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -261,19 +264,27 @@ void Engine::build_device(int threads) {
         for (int t = ra[i] / kTileCols; t <= (ra[i] + rl[i] - 1) / kTileCols; ++t) trows[tpos[t]++] = i;
     // y = S v schedule: rows cut into segments of <= kSegCols columns.  Segments of consecutive rows that
     // share their first column (one separator) are emitted row-fastest so one CTA reads one slice of v.
+    // The items of one group and segment form one unit of the row-group kernel (first item, rows, first column,
+    // widest row's columns).
     std::vector<int> it_row, it_c0, it_nc;
+    std::vector<int4> units;
     for (int i = 0; i < n;) {
         int j = i + 1;
-        while (j < n && ra[j] == ra[i] && j - i < 8) ++j;
+        while (j < n && ra[j] == ra[i] && j - i < kUnitRows) ++j;
         int glen = 0;
         for (int r = i; r < j; ++r) glen = std::max(glen, rl[r]);
-        for (int c0 = 0; c0 < glen; c0 += kSegCols)
+        for (int c0 = 0; c0 < glen; c0 += kSegCols) {
+            const int first = (int)it_row.size();
+            int ncmax = 0;
             for (int r = i; r < j; ++r)
                 if (c0 < rl[r]) {
                     it_row.push_back(r);
                     it_c0.push_back(c0);
                     it_nc.push_back(std::min(kSegCols, rl[r] - c0));
+                    ncmax = std::max(ncmax, it_nc.back());
                 }
+            units.push_back(make_int4(first, (int)it_row.size() - first, ra[i] + c0, ncmax));
+        }
         i = j;
     }
     std::vector<int> r_ptr(n + 1, 0), r_items(it_row.size());
@@ -320,6 +331,7 @@ void Engine::build_device(int threads) {
     }
     d_item_desc.upload(idesc);
     d_item_slot.upload(slot);
+    d_unit_desc.upload(units);
     d_trow_desc.upload(tdesc);
     d_trow_off.upload(toff);
     d_short_rows.upload(it_row);
@@ -384,6 +396,9 @@ void Engine::build_device(int threads) {
     // the factor stays in L2 across PD iterations when it takes at most about half of it (126 MB on B200)
     plan64_.keep_in_l2 = d_vals64.bytes <= (64ull << 20) ? 1 : 0;
     plan32_.keep_in_l2 = d_vals32.bytes <= (64ull << 20) ? 1 : 0;
+    plan32_.n_units = (int)units.size();
+    plan32_.unit_desc = d_unit_desc.as<int4>();
+    plan32_.use_units = s_units_ ? 1 : 0;
     // mesh, samples, constraints
     dE.upload(M.E);
     dX.upload(M.X);
@@ -452,6 +467,31 @@ void Engine::build_device(int threads) {
     CUDA_OK(cudaMemset(d_y32.p, 0, d_y32.bytes));
     d_ctrl.alloc(sizeof(Ctrl));
     CUDA_OK(cudaMemset(d_ctrl.p, 0, sizeof(Ctrl)));
+    // The two FP32 y = S v kernels (one warp per row segment, one warp per row group) give bit-identical sums
+    // (the same per-lane order); which is faster depends on the factor's shape, so both are timed once here on
+    // this factor (a warm-up and 5 launches each) and the faster one is kept.
+    {
+        cudaEvent_t e0, e1;
+        CUDA_OK(cudaEventCreate(&e0));
+        CUDA_OK(cudaEventCreate(&e1));
+        float ms[2] = {0.f, 0.f};
+        const Ctrl* c = d_ctrl.as<Ctrl>();
+        for (int which = 0; which < 2; ++which) {
+            SpmvPlan<float> p = plan32_;
+            p.use_units = which;
+            launch_s_only<float>(p, d_vperm32.as<float>(), d_y32.as<float>(), c, stream_);
+            CUDA_OK(cudaEventRecord(e0, stream_));
+            for (int r = 0; r < 5; ++r) launch_s_only<float>(p, d_vperm32.as<float>(), d_y32.as<float>(), c, stream_);
+            CUDA_OK(cudaEventRecord(e1, stream_));
+            CUDA_OK(cudaEventSynchronize(e1));
+            CUDA_OK(cudaEventElapsedTime(&ms[which], e0, e1));
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        s_units_ = ms[1] < ms[0];
+        plan32_.use_units = s_units_ ? 1 : 0;
+        launches_ += 24;
+    }
     double gf[3] = {0, 0, 0};
     if (M.has_gravity)
         for (int d = 0; d < 3; ++d) gf[d] = M.mass() * M.gravity[d];
@@ -936,7 +976,7 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     const int n3 = dofs();
     const double h2m = dt * dt / M.mass();
     const bool learned = !d_init && ws_net_;
-    if (learned) d_init = ws_predict(dq, dv, df, dt, st);
+    if (learned) d_init = ws_predict(dq, dv, df, dt, o.ws_tcgen05 != 0, st);
     // new-rollout detection of the contact tape (forward_gpu.cpp:437-449): the input must continue the last
     // frame; the comparison is read after the solve's own synchronisation
     const bool check_tape = has_contact_ && !tape_.empty();
@@ -949,6 +989,11 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     launch_qtilde(n3, dq, dv, df, dt, h2m, d_gravf.as<double>(), d_qt.as<double>(), st);
     CUDA_OK(cudaMemcpyAsync(d_q0.p, dq, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     run_forward_loop(dq, dt, o, st, d_init);
+    if (learned && *h_ws_err_) {  // the loop's synchronisation has landed the flag
+        *h_ws_err_ = 0;
+        CUDA_OK(cudaMemsetAsync(d_ws_err.p, 0, sizeof(int), st));
+        throw Error("warm-start MLP: a tensor-core completion wait timed out.");
+    }
     if (learned) {
         CUDA_OK(cudaMemcpyAsync(d_ws_qprev.p, dq, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
         ws_which_ ^= 1;
@@ -973,6 +1018,12 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     CUDA_OK(cudaGetLastError());
 }
 
+void Engine::set_s_units(bool on) {
+    drop_graphs();
+    s_units_ = on;
+    plan32_.use_units = on ? 1 : 0;
+}
+
 double Engine::ws_dx() const { return std::pow(M.vol, 1.0 / 3.0); }
 
 void Engine::set_ws_net(const float* d_master, const void* d_packed) {
@@ -990,8 +1041,17 @@ void Engine::set_ws_net(const float* d_master, const void* d_packed) {
     ws_prev_valid_ = false;
 }
 
-const double* Engine::ws_predict(const double* dq, const double* dv, const double* df, double dt, cudaStream_t st) {
+const double* Engine::ws_predict(const double* dq, const double* dv, const double* df, double dt, bool tcgen05,
+                                 cudaStream_t st) {
     const int n = M.n, n3 = 3 * n;
+    if (!d_ws_err.p) {
+        d_ws_err.alloc(sizeof(int));
+        CUDA_OK(cudaMemsetAsync(d_ws_err.p, 0, sizeof(int), st));
+    }
+    if (!h_ws_err_) {
+        CUDA_OK(cudaMallocHost(&h_ws_err_, sizeof(int)));
+        *h_ws_err_ = 0;
+    }
     d_ws_X.alloc((size_t)n * 16 * 2);
     d_ws_out.alloc((size_t)n * 8 * sizeof(float));
     d_ws_base0.alloc(n3 * sizeof(double));
@@ -1002,7 +1062,13 @@ const double* Engine::ws_predict(const double* dq, const double* dv, const doubl
     const double* prev_base = ws_prev_valid_ ? (ws_which_ ? d_ws_base0 : d_ws_base1).as<double>() : nullptr;
     const double* qp = ws_prev_valid_ ? d_ws_qprev.as<double>() : dq;
     ws_features(dt, dq, qp, dv, df, prev_base, d_ws_X.p, base, st);
-    mlp_forward_flat(d_ws_master.as<float>(), d_ws_packed.p, d_ws_X.p, n, d_ws_out.as<float>(), st);
+    if (tcgen05) {
+        mlp_forward_tc_flat(d_ws_master.as<float>(), d_ws_packed.p, d_ws_X.p, n, d_ws_out.as<float>(),
+                            d_ws_err.as<int>(), st);
+        CUDA_OK(cudaMemcpyAsync(h_ws_err_, d_ws_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    } else {
+        mlp_forward_flat(d_ws_master.as<float>(), d_ws_packed.p, d_ws_X.p, n, d_ws_out.as<float>(), st);
+    }
     ws_apply(dt, base, d_ws_out.as<float>(), d_ws_qinit.as<double>(), st);
     launches_ += 1;
     return d_ws_qinit.as<double>();

@@ -40,6 +40,7 @@ struct Options {
     double tangent_lambda_min = 1e-8, rhs_prune_rel = 1e-3, rhs_prune_abs = 1e-12;
     int poll_chunk = 8;
     int graph_while = 1;         // device-side WHILE graph per solve (0: host polling every poll_chunk iterations)
+    int ws_tcgen05 = 1;          // warm-start inference on tcgen05 MMAs with TMEM accumulators (0: mma.sync)
     static Options parse(const std::map<std::string, double>& m);
 };
 
@@ -125,6 +126,9 @@ public:
     int contact_candidates() const;
     void contact_lambda_device(double* d_buf, bool set, cudaStream_t st);
     bool ws_net_attached() const { return ws_net_; }
+    // selects the row-group or the one-warp-per-item kernel of the FP32 y = S v pass (overriding the choice
+    // timed at factor build); drops the captured iteration graphs
+    void set_s_units(bool on);
 
     void backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,
                          double* d_dq, double* d_dv, double* d_df, double* d_dmat_w, double* d_dparams,
@@ -218,12 +222,17 @@ private:
     DeviceBuffer d_qn, d_vn, d_gbar, d_J, d_gw, d_gmat, d_gnh;
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
     DeviceBuffer d_item_desc, d_item_slot, d_trow_desc, d_trow_off, d_J32;
+    DeviceBuffer d_unit_desc;    // row-group units of the FP32 y = S v pass
+    bool s_units_ = false;       // chosen by timing both kernels when the factor is built
     DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv, d_wlog, d_mu_prev;
     bool mu_prev_valid_ = false;
-    const double* ws_predict(const double* d_q, const double* d_v, const double* d_f, double dt, cudaStream_t st);
+    const double* ws_predict(const double* d_q, const double* d_v, const double* d_f, double dt, bool tcgen05,
+                             cudaStream_t st);
     bool ws_net_ = false, ws_prev_valid_ = false;
     int ws_which_ = 0;
     DeviceBuffer d_ws_master, d_ws_packed, d_ws_X, d_ws_out, d_ws_base0, d_ws_base1, d_ws_qprev, d_ws_qinit;
+    DeviceBuffer d_ws_err;       // set by the tcgen05 inference kernel when a tensor-core wait gave up
+    int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_M, dc_ltmp, d_vcon, d_r64, d_q0;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -387,6 +388,79 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __restrict__ v, const Ctrl* ctrl) {
     if (ctrl->done) return;
     s_items_body(p, v, blockIdx.x);
+}
+
+// y = S v, stage 1 by row groups (FP32): one warp per unit (up to kUnitRows rows of one nested-dissection
+// group over one column segment).  Each lane loads the three float4 of v at its columns once and the float4
+// of S of every row of the unit, so v is read once per unit instead of once per row, and every lane keeps up to
+// kUnitRows + 3 independent 16-byte loads in flight.  Rows shorter than the unit's widest row are masked per
+// float4 (row lengths and segment starts are multiples of 4).  Partial sums go to the rows' item slots.
+__global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const float* __restrict__ v,
+                                                      const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int u = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (u >= p.n_units) return;
+    const int4 ud = __ldg(p.unit_desc + u);
+    const int first = ud.x, nr = ud.y, a = ud.z, ncmax = ud.w;
+    const float* sp[kUnitRows];
+    int nc[kUnitRows];
+#pragma unroll
+    for (int r = 0; r < kUnitRows; ++r) {
+        sp[r] = p.vals;
+        nc[r] = 0;
+        if (r < nr) {
+            const int4 d = __ldg(p.item_desc + first + r);
+            sp[r] = p.vals + ((int64_t)(uint32_t)d.x | ((int64_t)d.y << 32));
+            nc[r] = d.w;
+        }
+    }
+    const size_t npad = (size_t)p.npad;
+    const float* v0 = v + a;
+    const float* v1 = v + npad + a;
+    const float* v2 = v + 2 * npad + a;
+    float acc[kUnitRows][3];
+#pragma unroll
+    for (int r = 0; r < kUnitRows; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
+    for (int c = lane * 4; c < ncmax; c += 128) {
+        Vec4<float> x0, x1, x2, sv[kUnitRows];
+        x0.load(v0 + c);
+        x1.load(v1 + c);
+        x2.load(v2 + c);
+#pragma unroll
+        for (int r = 0; r < kUnitRows; ++r) {
+            if (c < nc[r]) sv[r].load_s(sp[r] + c, p.keep_in_l2);
+            else sv[r].v[0] = sv[r].v[1] = sv[r].v[2] = sv[r].v[3] = 0.f;
+        }
+#pragma unroll
+        for (int r = 0; r < kUnitRows; ++r)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc[r][0] += sv[r].v[q] * x0.v[q];
+                acc[r][1] += sv[r].v[q] * x1.v[q];
+                acc[r][2] += sv[r].v[q] * x2.v[q];
+            }
+    }
+#pragma unroll
+    for (int r = 0; r < kUnitRows; ++r)
+        if (r < nr) {
+            acc[r][0] = warp_sum(acc[r][0]);
+            acc[r][1] = warp_sum(acc[r][1]);
+            acc[r][2] = warp_sum(acc[r][2]);
+        }
+    if (lane < nr) {  // lane r stores row r's partial (the values are warp-uniform after the sums)
+        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+#pragma unroll
+        for (int r = 0; r < kUnitRows; ++r)
+            if (r == lane) {
+                o0 = acc[r][0];
+                o1 = acc[r][1];
+                o2 = acc[r][2];
+            }
+        float* o = p.ypart + (size_t)__ldg(p.item_slot + first + lane) * 3;
+        o[0] = o0;
+        o[1] = o1;
+        o[2] = o2;
+    }
 }
 
 // y = S v, stage 2: per row, the item partials in item order.
@@ -1419,9 +1493,21 @@ void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const do
                                                      v_perm, npad, prev_pd, part, A, q, zero_dirichlet, r_out, ctrl);
 }
 
+// stage 1 of y = S v: the row-group kernel for FP32 factors with a unit schedule, else one warp per item
+template <typename T>
+static void launch_s_items(const SpmvPlan<T>& p, const T* v, const Ctrl* ctrl, cudaStream_t st) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (p.use_units && p.n_units > 0) {
+            k_spmv_S_units<<<blocks_for((long long)p.n_units * 32, 256), 256, 0, st>>>(p, v, ctrl);
+            return;
+        }
+    }
+    k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
+}
+
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
-    k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
+    launch_s_items(p, v, ctrl, st);
     if (p.y_accumulate) {
         k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
         k_spmv_ST_part<T, false><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
@@ -1639,7 +1725,7 @@ void launch_param_reduce(int m, int ne, const int* np_k, const int* type_k, cons
 
 template <typename T>
 void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st) {
-    k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
+    launch_s_items(p, v, ctrl, st);
     k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
 }
 template <typename T>

@@ -98,8 +98,14 @@ struct SpmvPlan {
     const int* perm = nullptr;
     const double* x_base = nullptr;  // when set, x_out = x_base + S^T S v (refinement form)
     int y_accumulate = 0;            // when set, y += S v instead of y = S v
+    // y = S v by row groups (FP32 factors): unit u = the items of one group of at most kUnitRows rows that
+    // share a column segment (unit_desc: first item, rows, first column, widest row's columns); one warp
+    // reads the segment of v once for all rows.  use_units = 0 selects the one-warp-per-item kernel.
+    int n_units = 0, use_units = 0;
+    const int4* unit_desc = nullptr;
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
+constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
 constexpr int kChunkRows = 64;       // rows per S^T chunk CTA
 constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 
@@ -232,6 +238,9 @@ int mlp_part_size();      // floats of one CTA's gradient partial
 int mlp_rows_per_block(); // rows (nodes) per CTA
 void mlp_pack_flat(float* master, void* packed, cudaStream_t st);
 void mlp_forward_flat(float* master, void* packed, const void* X, int n, float* out, cudaStream_t st);
+// Same network on tcgen05 MMAs (mlp_tc.cu): BF16 operands in shared memory, FP32 accumulators in TMEM; *err is
+// set to 1 when a completion wait gave up (the outputs of that CTA's remaining rows are then not written).
+void mlp_forward_tc_flat(float* master, void* packed, const void* X, int n, float* out, int* err, cudaStream_t st);
 int mlp_train_flat(float* master, void* packed, const void* X, const float* Y, int n, float* part, cudaStream_t st);
 void mlp_adamw_flat(float* master, void* packed, const float* part, int nblocks, float lr, float b1, float b2,
                     float eps, float wd, int step, float* m, float* v, float* grad_out, float* loss_out,

@@ -508,6 +508,15 @@ void mlp_pack_flat(float* master, void* packed, cudaStream_t st) { launch_mlp_pa
 void mlp_forward_flat(float* master, void* packed, const void* X, int n, float* out, cudaStream_t st) {
     launch_mlp_forward(flat_params(master, packed), X, n, out, st);
 }
+void launch_mlp_forward_tc(const void* W1T, const void* W2T, const void* W3T, const float* b1, const float* b2,
+                           const float* b3, const void* X, int n, float* out, int* err, int max_ctas, cudaStream_t st);
+void mlp_forward_tc_flat(float* master, void* packed, const void* X, int n, float* out, int* err, cudaStream_t st) {
+    const MlpParams p = flat_params(master, packed);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    launch_mlp_forward_tc(p.W1T, p.W2T, p.W3T, p.b1, p.b2, p.b3, X, n, out, err, 2 * (sms > 0 ? sms : 148), st);
+}
 int mlp_train_flat(float* master, void* packed, const void* X, const float* Y, int n, float* part, cudaStream_t st) {
     return launch_mlp_train(flat_params(master, packed), X, Y, n, part, st);
 }

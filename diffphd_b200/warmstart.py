@@ -63,6 +63,7 @@ class WarmStartMLP:
         self.step_count = 0
         self.loss_buf = torch.zeros(1, dtype=torch.float32, device=self.device)
         self._part = None
+        self._err = None
         self.pack()
 
     @property
@@ -79,14 +80,27 @@ class WarmStartMLP:
         self.master.copy_(torch.as_tensor(flat, dtype=torch.float32))
         self.pack()
 
-    def forward(self, X, out=None):
-        """X: BF16 [n][16] CUDA tensor -> FP32 [n][8] (columns 0..2 used)."""
+    def forward(self, X, out=None, tcgen05=True):
+        """X: BF16 [n][16] CUDA tensor -> FP32 [n][8] (columns 0..2 used).  tcgen05: the kernel on tcgen05 MMAs
+        with TMEM accumulators (dphd_mlp_forward_tc), else the mma.sync kernel (dphd_mlp_forward)."""
         n = X.shape[0]
         if out is None:
             out = torch.empty(n, N_OUT, dtype=torch.float32, device=self.device)
-        core.Deformable._check(self._L.dphd_mlp_forward(_p(self.master), _p(self.packed), _p(X), int(n), _p(out),
-                                                        self._stream()))
+        if tcgen05:
+            if self._err is None:
+                self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
+            core.Deformable._check(self._L.dphd_mlp_forward_tc(_p(self.master), _p(self.packed), _p(X), int(n),
+                                                               _p(out), _p(self._err), self._stream()))
+        else:
+            core.Deformable._check(self._L.dphd_mlp_forward(_p(self.master), _p(self.packed), _p(X), int(n),
+                                                            _p(out), self._stream()))
         return out
+
+    def check_tensor_core_waits(self):
+        """Raises if a tcgen05 inference kernel gave up a completion wait since the last check (synchronises)."""
+        if self._err is not None and int(self._err.item()) != 0:
+            self._err.zero_()
+            raise RuntimeError("warm-start MLP: a tensor-core completion wait timed out")
 
     def _partials(self, n):
         blocks = (n + self.rows_per_block - 1) // self.rows_per_block

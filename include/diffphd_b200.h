@@ -123,6 +123,11 @@ long long dphd_s_nnz(const dphd_deformable* h);
 /* Stored S values including the 16-byte alignment padding of each row segment. */
 long long dphd_s_padded_values(const dphd_deformable* h);
 
+/* Selects the kernel of the FP32 y = S v pass: 1 one warp per row group of up to 8 rows that share a column
+ * segment (v read once per group); 0 one warp per row segment.  Both give bit-identical sums; by default the
+ * faster one on the factor is chosen by timing both when the factor is built.  Captured iteration graphs are
+ * dropped.  No counterpart in the reference (profiling and A/B timing). */
+int dphd_debug_set_s_kernel(dphd_deformable* h, int row_groups);
 /* x = A^-1 b through the S^T S pair on device pointers (b, x: 3n FP64 node-major; Dirichlet rows of b are
  * taken as zero, as in the forward step), allocating no GPU memory: its temporaries live in a static 32 MiB
  * device array instead.  No counterpart in the reference.  For callers that cannot call cudaMalloc during a
@@ -161,6 +166,12 @@ int dphd_set_warm_start_network(dphd_deformable* h, const float* d_master, const
 int dphd_mlp_sizes(int* n_master, int* n_packed, int* part_floats_per_block, int* rows_per_block);
 int dphd_mlp_pack(float* d_master, void* d_packed, void* stream);
 int dphd_mlp_forward(float* d_master, void* d_packed, const void* d_X, int n, float* d_out, void* stream);
+/* The same inference on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in shared memory, FP32
+ * accumulators in tensor memory); the engine's warm start uses it unless the option ws_tcgen05 = 0.  d_err: one
+ * device int the caller zeroes; the kernel sets it to 1 if a tensor-core completion wait gave up (bounded
+ * wait; the rows that CTA had not finished are then left unwritten).  d_packed, d_X and d_out 16-byte aligned. */
+int dphd_mlp_forward_tc(float* d_master, void* d_packed, const void* d_X, int n, float* d_out, int* d_err,
+                        void* stream);
 /* One training step on rows [0, n): loss = sum over rows and the 3 outputs of (pred - Y)^2 / n (Y: FP32
  * [n][3]); d_part holds ceil(n / rows_per_block) * part_floats_per_block floats of per-block gradient
  * partials, summed in a fixed order (deterministic); AdamW (bias-corrected, decoupled decay on weights only)
