@@ -329,8 +329,26 @@ void Engine::build_device(int threads) {
         tdesc[q] = make_int4(ra[r], rl[r], r_ptr[r], r_ptr[r + 1]);
         toff[q] = ro[r];
     }
-    d_item_desc.upload(idesc);
-    d_item_slot.upload(slot);
+    // Launch orders, longest work first so that the last wave is made of short work items: the
+    // one-warp-per-item kernel takes (descriptor, slot) pairs sorted by decreasing length; the row-group kernel
+    // reads its rows from the pairs in emission order and takes its units sorted by decreasing size.
+    {
+        std::vector<int> ord(idesc.size());
+        for (size_t t = 0; t < ord.size(); ++t) ord[t] = (int)t;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return idesc[x].w > idesc[y].w; });
+        std::vector<int4> od(ord.size());
+        std::vector<int> os(ord.size());
+        for (size_t t = 0; t < ord.size(); ++t) {
+            od[t] = idesc[ord[t]];
+            os[t] = slot[ord[t]];
+        }
+        d_item_desc.upload(od);
+        d_item_slot.upload(os);
+        std::stable_sort(units.begin(), units.end(),
+                         [](const int4& x, const int4& y) { return (long long)x.y * x.w > (long long)y.y * y.w; });
+    }
+    d_unit_item_desc.upload(idesc);
+    d_unit_item_slot.upload(slot);
     d_unit_desc.upload(units);
     d_trow_desc.upload(tdesc);
     d_trow_off.upload(toff);
@@ -398,6 +416,8 @@ void Engine::build_device(int threads) {
     plan32_.keep_in_l2 = d_vals32.bytes <= (64ull << 20) ? 1 : 0;
     plan32_.n_units = (int)units.size();
     plan32_.unit_desc = d_unit_desc.as<int4>();
+    plan32_.unit_item_desc = d_unit_item_desc.as<int4>();
+    plan32_.unit_item_slot = d_unit_item_slot.as<int>();
     plan32_.use_units = s_units_ ? 1 : 0;
     // mesh, samples, constraints
     dE.upload(M.E);

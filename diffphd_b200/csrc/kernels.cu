@@ -331,11 +331,13 @@ template <> struct Vec4<double> {
 // y = S v, stage 1: one warp per work item (a row segment of <= kSegCols columns), four 16-byte loads of S
 // in flight per lane, v through L1 (the CTA's warps share the segment's columns).
 template <typename T>
-__device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __restrict__ v, int vb) {
+__device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __restrict__ v, int vb, const Ctrl* ctrl) {
+    const int done = ctrl->done;  // in flight together with the descriptor loads, tested after them
     const int it = (vb * (int)blockDim.x + (int)threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (it >= p.n_items) return;
     const int4 dsc = __ldg(p.item_desc + it);
     const int slot = __ldg(p.item_slot + it);
+    if (done) return;
     const T* __restrict__ sv = p.vals + ((int64_t)(uint32_t)dsc.x | ((int64_t)dsc.y << 32));
     const int a = dsc.z, nc = dsc.w;
     const T* __restrict__ v0 = v + a;
@@ -386,8 +388,7 @@ __device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __re
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __restrict__ v, const Ctrl* ctrl) {
-    if (ctrl->done) return;
-    s_items_body(p, v, blockIdx.x);
+    s_items_body(p, v, blockIdx.x, ctrl);
 }
 
 // y = S v, stage 1 by row groups (FP32): one warp per unit (up to kUnitRows rows of one nested-dissection
@@ -397,10 +398,11 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
 // float4 (row lengths and segment starts are multiples of 4).  Partial sums go to the rows' item slots.
 __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const float* __restrict__ v,
                                                       const Ctrl* ctrl) {
-    if (ctrl->done) return;
+    const int done = ctrl->done;  // in flight together with the unit descriptor, tested after it
     const int u = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (u >= p.n_units) return;
     const int4 ud = __ldg(p.unit_desc + u);
+    if (done) return;
     const int first = ud.x, nr = ud.y, a = ud.z, ncmax = ud.w;
     const float* sp[kUnitRows];
     int nc[kUnitRows];
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const f
         sp[r] = p.vals;
         nc[r] = 0;
         if (r < nr) {
-            const int4 d = __ldg(p.item_desc + first + r);
+            const int4 d = __ldg(p.unit_item_desc + first + r);
             sp[r] = p.vals + ((int64_t)(uint32_t)d.x | ((int64_t)d.y << 32));
             nc[r] = d.w;
         }
@@ -456,7 +458,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const f
                 o1 = acc[r][1];
                 o2 = acc[r][2];
             }
-        float* o = p.ypart + (size_t)__ldg(p.item_slot + first + lane) * 3;
+        float* o = p.ypart + (size_t)__ldg(p.unit_item_slot + first + lane) * 3;
         o[0] = o0;
         o[1] = o1;
         o[2] = o2;
@@ -492,8 +494,9 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
 constexpr int kStRows = 4;
 
 template <typename T, bool FROM_ITEMS>
-__device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __restrict__ y, int ch) {
+__device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __restrict__ y, int ch, const Ctrl* ctrl) {
     __shared__ T red[8][3][kTileCols];
+    const int done = ctrl->done;  // in flight together with the chunk's bounds; the same in every thread
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tile = __ldg(p.chunk_tile + ch);
     const int c = tile * kTileCols + lane * 4;
@@ -503,8 +506,9 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
     for (int d = 0; d < 3; ++d)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[d][q] = T(0);
-    const int pe = __ldg(p.chunk_p1 + ch);
-    for (int pp = __ldg(p.chunk_p0 + ch) + wid; pp < pe; pp += 8 * kStRows) {
+    const int pe = __ldg(p.chunk_p1 + ch), p0 = __ldg(p.chunk_p0 + ch);
+    if (done) return;
+    for (int pp = p0 + wid; pp < pe; pp += 8 * kStRows) {
         int4 dsc[kStRows];
         int64_t off[kStRows];
 #pragma unroll
@@ -566,13 +570,14 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
 
 template <typename T, bool FROM_ITEMS>
 __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
-    if (ctrl->done) return;
-    st_part_body<T, FROM_ITEMS>(p, y, blockIdx.x);
+    st_part_body<T, FROM_ITEMS>(p, y, blockIdx.x, ctrl);
 }
 
 // x = S^T y, stage 2: per tile column, sum the chunk partials in order and scatter to node-major x.
 template <typename T>
-__device__ __forceinline__ void st_fin_body(const SpmvPlan<T>& p, double* __restrict__ x_out, int vb) {
+__device__ __forceinline__ void st_fin_body(const SpmvPlan<T>& p, double* __restrict__ x_out, int vb,
+                                            const Ctrl* ctrl) {
+    const int done = ctrl->done;  // in flight together with the tile's chunk range, tested after it
     const int t = vb * (int)blockDim.x + (int)threadIdx.x;
     if (t >= p.ntiles * 3 * kTileCols) return;
     const int tile = t / (3 * kTileCols), r = t % (3 * kTileCols);
@@ -581,6 +586,7 @@ __device__ __forceinline__ void st_fin_body(const SpmvPlan<T>& p, double* __rest
     if (j >= p.n) return;
     double s = 0.0;
     const int c0 = __ldg(p.tile_chunk_ptr + tile), c1 = __ldg(p.tile_chunk_ptr + tile + 1);
+    if (done) return;
     for (int ch = c0; ch < c1; ch += 8) {  // eight independent loads in flight, summed in chunk order
         T t8[8];
 #pragma unroll
@@ -595,8 +601,7 @@ __device__ __forceinline__ void st_fin_body(const SpmvPlan<T>& p, double* __rest
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double* __restrict__ x_out,
                                                           const Ctrl* ctrl) {
-    if (ctrl->done) return;
-    st_fin_body(p, x_out, blockIdx.x);
+    st_fin_body(p, x_out, blockIdx.x, ctrl);
 }
 
 

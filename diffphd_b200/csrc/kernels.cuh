@@ -103,6 +103,8 @@ struct SpmvPlan {
     // reads the segment of v once for all rows.  use_units = 0 selects the one-warp-per-item kernel.
     int n_units = 0, use_units = 0;
     const int4* unit_desc = nullptr;
+    const int4* unit_item_desc = nullptr;  // the items in emission order (a unit's rows are consecutive here)
+    const int* unit_item_slot = nullptr;
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
