@@ -497,6 +497,8 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
         "pd_iters_per_step": float(np.mean(fwd_iters)) if len(fwd_iters) else None,
         "adjoint_iters_per_step": float(np.mean(bwd_iters)) if bwd_iters else None,
         "forward_converged_frac": float(np.mean(conv)) if len(conv) else None,
+        # device time of each timed call (forward steps, then the adjoints in reverse order), for the spread
+        "call_ms": [round(a.elapsed_time(b), 3) for a, b in ev],
     }
     return line
 

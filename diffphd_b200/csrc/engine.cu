@@ -470,7 +470,7 @@ void Engine::build_device(int threads) {
     d_dG.alloc(ld * kMaxWindow * sizeof(double));
     d_dX.alloc(ld * kMaxWindow * sizeof(double));
     red_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256));
-    gather_blocks_ = std::max(1, std::min(kMaxRedBlocks, (n * kGatherLanes + 255) / 256));
+    gather_blocks_ = gather_grid(n);
     d_part_gate.alloc(kMaxRedBlocks * 2 * sizeof(double));
     d_part_aa.alloc(kMaxRedBlocks * 64 * sizeof(double));
     d_part_upd.alloc(kMaxRedBlocks * 3 * sizeof(double));

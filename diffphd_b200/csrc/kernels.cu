@@ -241,7 +241,7 @@ __device__ __forceinline__ void csr_row_product(const NodeCsr& A, const double* 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __restrict__ node_ptr,
+__global__ void __launch_bounds__(kGatherMaxThreads) k_gather_fwd(int n, const int* __restrict__ node_ptr,
                                                          const int* __restrict__ node_inc, const double* __restrict__ eo,
                                                          const double* __restrict__ qt, double inv_h2m,
                                                          const unsigned char* __restrict__ fixed,
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kThreads) k_gather_fwd(int n, const int* __res
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
     const int lane = threadIdx.x & (kGatherLanes - 1);
-    constexpr int per_block = kThreads / kGatherLanes;
+    const int per_block = (int)blockDim.x / kGatherLanes;
     for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
         const int i = base + (int)threadIdx.x / kGatherLanes;
         const bool valid = i < n;
@@ -703,8 +703,11 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
             A[i][i] += reg;
             b[i] = tot[kMaxWindow + i];
         }
+    // one reciprocal per column (a single thread runs this: FP64 divisions dominate its latency)
+    double inv_diag[kMaxWindow];
 #pragma unroll
     for (int j = 0; j < kMaxWindow; ++j) {
+        inv_diag[j] = 0.0;
         if (j < m) {
             double d = A[j][j];
 #pragma unroll
@@ -712,6 +715,8 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
                 if (k < j) d -= A[j][k] * A[j][k];
             d = sqrt(fmax(d, 1e-300));
             A[j][j] = d;
+            const double inv = 1.0 / d;
+            inv_diag[j] = inv;
 #pragma unroll
             for (int i = 0; i < kMaxWindow; ++i)
                 if (i > j && i < m) {
@@ -719,7 +724,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
 #pragma unroll
                     for (int k = 0; k < kMaxWindow; ++k)
                         if (k < j) t -= A[i][k] * A[j][k];
-                    A[i][j] = t / d;
+                    A[i][j] = t * inv;
                 }
         }
     }
@@ -730,7 +735,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
 #pragma unroll
             for (int k = 0; k < kMaxWindow; ++k)
                 if (k < i) t -= A[i][k] * b[k];
-            b[i] = t / A[i][i];
+            b[i] = t * inv_diag[i];
         }
 #pragma unroll
     for (int i = kMaxWindow - 1; i >= 0; --i)
@@ -739,7 +744,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
 #pragma unroll
             for (int k = 0; k < kMaxWindow; ++k)
                 if (k > i && k < m) t -= A[k][i] * b[k];
-            b[i] = t / A[i][i];
+            b[i] = t * inv_diag[i];
         }
     double gn = 0;
 #pragma unroll
@@ -1096,7 +1101,7 @@ __global__ void __launch_bounds__(kThreads) k_kpd_elem32(int m, const int* __res
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_gather_bwd(int n, const int* __restrict__ node_ptr,
+__global__ void __launch_bounds__(kGatherMaxThreads) k_gather_bwd(int n, const int* __restrict__ node_ptr,
                                                          const int* __restrict__ node_inc,
                                                          const double* __restrict__ eo, const double* __restrict__ gbar,
                                                          const unsigned char* __restrict__ fixed,
@@ -1104,7 +1109,7 @@ __global__ void __launch_bounds__(kThreads) k_gather_bwd(int n, const int* __res
                                                          int npad, const Ctrl* ctrl) {
     if (ctrl->done) return;
     const int lane = threadIdx.x & (kGatherLanes - 1);
-    constexpr int per_block = kThreads / kGatherLanes;
+    const int per_block = (int)blockDim.x / kGatherLanes;
     for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
         const int i = base + (int)threadIdx.x / kGatherLanes;
         const bool valid = i < n;
@@ -1229,7 +1234,7 @@ __global__ void __launch_bounds__(128) k_param_grad(int m, const int* __restrict
 // ------------------------------------------------------------------------------------------------
 // Conjugate-gradient adjoint
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const double* __restrict__ p,
+__global__ void __launch_bounds__(kGatherMaxThreads) k_pcg_gather(int n, NodeCsr A, const double* __restrict__ p,
                                                          const int* __restrict__ node_ptr,
                                                          const int* __restrict__ node_inc,
                                                          const double* __restrict__ eo,
@@ -1240,7 +1245,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_gather(int n, NodeCsr A, const
     __shared__ double sh[32];
     double acc[1] = {0.0};
     const int lane = threadIdx.x & (kGatherLanes - 1);
-    constexpr int per_block = kThreads / kGatherLanes;
+    const int per_block = (int)blockDim.x / kGatherLanes;
     for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
         const int i = base + (int)threadIdx.x / kGatherLanes;
         const bool valid = i < n;
@@ -1477,6 +1482,48 @@ inline int blocks_for(long long work, int threads) { return (int)((work + thread
 
 }  // namespace
 
+int device_sms() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = sms > 0 ? sms : 148;
+    }
+    return cached[dev];
+}
+
+void even_grid(long long threads, int max_bs, int max_grid, int* grid, int* bs) {
+    const long long sms = device_sms();
+    if (threads <= 0) {
+        *grid = 1;
+        *bs = 32;
+        return;
+    }
+    const long long k = std::max(1LL, (threads + (long long)max_bs * sms - 1) / ((long long)max_bs * sms));
+    long long per = (threads + k * sms - 1) / (k * sms);
+    per = std::min<long long>(max_bs, (per + 31) / 32 * 32);
+    const long long g = (threads + per - 1) / per;
+    *bs = (int)per;
+    *grid = (int)std::max(1LL, std::min<long long>(g, max_grid));
+}
+
+int gather_grid(int n) {
+    int g, b;
+    even_grid((long long)n * kGatherLanes, kGatherMaxThreads, kMaxRedBlocks, &g, &b);
+    return g;
+}
+int gather_bs(int n) {
+    int g, b;
+    even_grid((long long)n * kGatherLanes, kGatherMaxThreads, kMaxRedBlocks, &g, &b);
+    return b;
+}
+
+namespace {
+
+}  // namespace
+
 // ------------------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------------------
@@ -1484,9 +1531,10 @@ template <typename T>
 void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const double* qb, const unsigned char* elem_dir,
                      const double* grad, int hex, double vol_over_s, const EnergyPack& ep, double* elem_out, Ctrl* ctrl,
                      cudaStream_t st) {
-    const int grid = blocks_for((long long)m * s, kThreads);
-    if (hex) k_elem_fwd<T, 8, 8><<<grid, kThreads, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
-    else k_elem_fwd<T, 4, 1><<<grid, kThreads, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
+    int grid, bs;
+    even_grid((long long)m * s, kThreads, 1 << 30, &grid, &bs);
+    if (hex) k_elem_fwd<T, 8, 8><<<grid, bs, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
+    else k_elem_fwd<T, 4, 1><<<grid, bs, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
 }
 
 template <typename T>
@@ -1494,7 +1542,7 @@ void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const do
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
                        double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, int zero_dirichlet,
                        Ctrl* ctrl, cudaStream_t st, double* r_out) {
-    k_gather_fwd<T><<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
+    k_gather_fwd<T><<<blocks, gather_bs(n), 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
                                                      v_perm, npad, prev_pd, part, A, q, zero_dirichlet, r_out, ctrl);
 }
 
@@ -1557,24 +1605,26 @@ void launch_jac_build(int m, int k, int s, const int* E, const double* q, const 
 void launch_kpd_elem32(int m, int k, int s, const int* E, const double* u, const double* grad, int hex,
                        const float* J32, double* elem_out, const Ctrl* ctrl, cudaStream_t st) {
     (void)k;
-    const int grid = blocks_for((long long)m * s, kThreads);
-    if (hex) k_kpd_elem32<8, 8><<<grid, kThreads, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
-    else k_kpd_elem32<4, 1><<<grid, kThreads, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
+    int grid, bs;
+    even_grid((long long)m * s, kThreads, 1 << 30, &grid, &bs);
+    if (hex) k_kpd_elem32<8, 8><<<grid, bs, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
+    else k_kpd_elem32<4, 1><<<grid, bs, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
 }
 
 void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const double* grad, int hex, const double* J,
                      double* elem_out, const Ctrl* ctrl, cudaStream_t st) {
     (void)k;
-    const int grid = blocks_for((long long)m * s, kThreads);
-    if (hex) k_kpd_elem<8, 8><<<grid, kThreads, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
-    else k_kpd_elem<4, 1><<<grid, kThreads, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
+    int grid, bs;
+    even_grid((long long)m * s, kThreads, 1 << 30, &grid, &bs);
+    if (hex) k_kpd_elem<8, 8><<<grid, bs, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
+    else k_kpd_elem<4, 1><<<grid, bs, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
 }
 
 void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* gbar,
                        const unsigned char* fixed_node, const int* iperm, double* v_perm, int npad, const Ctrl* ctrl,
                        cudaStream_t st) {
     const int blocks = std::max(1, std::min(kMaxRedBlocks, (n * kGatherLanes + kThreads - 1) / kThreads));
-    k_gather_bwd<<<blocks, kThreads, 0, st>>>(n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm, npad,
+    k_gather_bwd<<<blocks, gather_bs(n), 0, st>>>(n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm, npad,
                                               ctrl);
 }
 
@@ -1601,7 +1651,7 @@ template void launch_gather_fwd<float>(int, const int*, const int*, const double
 void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
                        const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
                        Ctrl* ctrl, cudaStream_t st, int init) {
-    k_pcg_gather<<<blocks, kThreads, 0, st>>>(n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl,
+    k_pcg_gather<<<blocks, gather_bs(n), 0, st>>>(n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl,
                                               init);
 }
 

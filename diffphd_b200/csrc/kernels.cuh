@@ -110,6 +110,15 @@ constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
 constexpr int kChunkRows = 64;       // rows per S^T chunk CTA
 constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
+constexpr int kGatherMaxThreads = 512;  // block-size bound of the node gathers
+
+// Launch shapes spread evenly over the SMs: `threads` independent threads in at most `max_grid` blocks of at
+// most `max_bs` threads (a multiple of 32), with the fewest blocks per SM that fit and equal-sized blocks, so
+// that no SM holds a block more than the others (a partly filled last wave doubles a short kernel's time).
+int device_sms();
+void even_grid(long long threads, int max_bs, int max_grid, int* grid, int* bs);
+int gather_grid(int n);  // grid of the node gathers for n nodes (also the count of their per-block partials)
+int gather_bs(int n);    // block size of the node gathers for n nodes
 
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
