@@ -374,11 +374,15 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
         torch.cuda.nvtx.range_push("timed_value")  # lets a profiler restrict itself to the timed steps
         q, v = q_start, v_start
         qs, vs = [q], [v]
-        for _ in range(args.steps):
+        # every output is allocated before the timed region: an allocator call inside an event window would be
+        # timed as device time
+        q_out = [(torch.empty_like(q), torch.empty_like(q)) for _ in range(args.steps)]
+        g_out = [(torch.empty_like(q), torch.empty_like(q), torch.empty_like(q)) for _ in range(args.steps)]
+        for k in range(args.steps):
             flush.random_(0, 255)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            qn, vn = q_out[k]
             e0.record(stream)
-            qn, vn = torch.empty_like(q), torch.empty_like(q)
             d.forward_device(method, qs[-1], vs[-1], f_ext, sc.dt, opts, qn, vn, stream=sh)
             e1.record(stream)
             ev.append((e0, e1))
@@ -389,8 +393,8 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
         for i in reversed(range(args.steps)):
             flush.random_(0, 255)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            dq, dv, df = g_out[i]
             e0.record(stream)
-            dq, dv, df = torch.empty_like(gq), torch.empty_like(gq), torch.empty_like(gq)
             d.backward_device(method, qs[i + 1], gq, gv, sc.dt, opts, dq, dv, df, dl_dparams=dpar, stream=sh)
             e1.record(stream)
             ev.append((e0, e1))

@@ -818,12 +818,19 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected) {
         launch_pcg_update1<double>(n, d_x.as<double>(), d_r.as<double>(), d_pp.as<double>(), d_wv.as<double>(),
                                    d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_,
                                    d_part_upd.as<double>(), gather_blocks_, c, st);
-    launch_ainv(f32, st);
-    if (projected)  // z = P A^-1 P r
+    if (projected) {  // z = P A^-1 P r, then the z-side update
+        launch_ainv(f32, st);
         launch_wb_project<double>(capK, d_wb_count.as<int>(), d_wb_nodes.as<int>(), d_wb_dirs.as<double>(),
                                   d_wb_ndir.as<int>(), d_xraw.as<double>(), nullptr, nullptr, npad_, c, st);
-    launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
-                       gather_blocks_, red_blocks_, c, st);
+        launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(),
+                           d_part_upd.as<double>(), gather_blocks_, red_blocks_, c, st);
+    } else if (f32) {  // z = A^-1 r with the z-side update in the S^T pass's last stage
+        launch_sts_cg<float>(plan32_, d_vperm32.as<float>(), d_xraw.as<double>(), d_r.as<double>(),
+                             d_part_aa.as<double>(), d_part_upd.as<double>(), gather_blocks_, c, st);
+    } else {
+        launch_sts_cg<double>(plan64_, d_vperm64.as<double>(), d_xraw.as<double>(), d_r.as<double>(),
+                              d_part_aa.as<double>(), d_part_upd.as<double>(), gather_blocks_, c, st);
+    }
     launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
 }
 

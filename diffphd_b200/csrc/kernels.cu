@@ -1313,6 +1313,9 @@ __global__ void __launch_bounds__(kThreads) k_pcg_update1(int n, double* __restr
     if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
 }
 
+__device__ __forceinline__ void pcg_update2_tail(const double* __restrict__ part, const double* __restrict__ mu_part,
+                                                 int mu_blocks, Ctrl* ctrl, double* sh);
+
 __global__ void __launch_bounds__(kThreads) k_pcg_update2(int n3, const double* __restrict__ r,
                                                           const double* __restrict__ z, double* __restrict__ part,
                                                           const double* __restrict__ mu_part, int mu_blocks,
@@ -1329,6 +1332,12 @@ __global__ void __launch_bounds__(kThreads) k_pcg_update2(int n3, const double* 
         part[blockIdx.x * 2] = acc[0];
         part[blockIdx.x * 2 + 1] = acc[1];
     }
+    pcg_update2_tail(part, mu_part, mu_blocks, ctrl, sh);
+}
+
+// Last-block part of the z-side update: r.z and |z| summed over the blocks' partials, beta, the stop rule.
+__device__ __forceinline__ void pcg_update2_tail(const double* __restrict__ part, const double* __restrict__ mu_part,
+                                                 int mu_blocks, Ctrl* ctrl, double* sh) {
     if (!arrive_last(&ctrl->arrive[1])) return;
     double t[2], mu2[1] = {0.0};
     sum_partials<2>(part, gridDim.x, t, sh);
@@ -1354,6 +1363,52 @@ __global__ void __launch_bounds__(kThreads) k_pcg_update2(int n3, const double* 
     if (conv) ctrl->converged = 1;
     if (conv || ctrl->iter >= ctrl->max_iter || (ctrl->status & (kStatusNonFinite | kStatusDiverged)))
         ctrl->done = 1;
+}
+
+// x = S^T y stage 2 fused with the z-side update of the conjugate-gradient adjoint: each thread finishes one
+// column of z = S^T S r (the chunk partials summed in order, scattered to node order) and adds its r.z and
+// z.z terms to the block's partials; the last block sums them (pcg_update2_tail).  Replaces the ST fin +
+// k_pcg_update2 pair when z is not projected afterwards.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_spmv_ST_fin_cg(SpmvPlan<T> p, double* __restrict__ z_out,
+                                                             const double* __restrict__ r, double* __restrict__ part,
+                                                             const double* __restrict__ mu_part, int mu_blocks,
+                                                             Ctrl* ctrl) {
+    __shared__ double sh[2 * 32];
+    const int done = ctrl->done;
+    const int t = blockIdx.x * (int)blockDim.x + (int)threadIdx.x;
+    double acc[2] = {0.0, 0.0};
+    int rr = 0, d = 0, j = -1, c0 = 0, c1 = 0;
+    if (t < p.ntiles * 3 * kTileCols) {
+        const int tile = t / (3 * kTileCols);
+        rr = t % (3 * kTileCols);
+        d = rr / kTileCols;
+        j = tile * kTileCols + rr % kTileCols;
+        c0 = __ldg(p.tile_chunk_ptr + tile);
+        c1 = __ldg(p.tile_chunk_ptr + tile + 1);
+    }
+    if (done) return;  // the same in every block: no block arrives, no tail runs
+    if (j >= 0 && j < p.n) {
+        double sum = 0.0;
+        for (int ch = c0; ch < c1; ch += 8) {  // eight independent loads in flight, summed in chunk order
+            T t8[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t8[u] = ch + u < c1 ? p.xpart[(size_t)(ch + u) * 3 * kTileCols + rr] : T(0);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) sum += (double)t8[u];
+        }
+        const size_t o = 3 * (size_t)__ldg(p.perm + j) + d;
+        const double zv = p.x_base ? p.x_base[o] + sum : sum;
+        z_out[o] = zv;
+        acc[0] = r[o] * zv;
+        acc[1] = zv * zv;
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2] = acc[0];
+        part[blockIdx.x * 2 + 1] = acc[1];
+    }
+    pcg_update2_tail(part, mu_part, mu_blocks, ctrl, sh);
 }
 
 __global__ void k_pcg_p(int n3, double* __restrict__ p, const double* __restrict__ z, const Ctrl* ctrl) {
@@ -1741,6 +1796,19 @@ void launch_pcg_update2(int n3, const double* r, const double* z, double* part, 
                         int blocks, Ctrl* ctrl, cudaStream_t st) {
     k_pcg_update2<<<blocks, kThreads, 0, st>>>(n3, r, z, part, mu_part, mu_blocks, ctrl);
 }
+template <typename T>
+void launch_sts_cg(const SpmvPlan<T>& p, const T* v, double* z, const double* r, double* part, const double* mu_part,
+                   int mu_blocks, Ctrl* ctrl, cudaStream_t st) {
+    launch_s_items(p, v, ctrl, st);
+    k_spmv_ST_part<T, true><<<p.n_chunks, 256, 0, st>>>(p, nullptr, ctrl);
+    k_spmv_ST_fin_cg<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(
+        p, z, r, part, mu_part, mu_blocks, ctrl);
+}
+template void launch_sts_cg<float>(const SpmvPlan<float>&, const float*, double*, const double*, double*,
+                                   const double*, int, Ctrl*, cudaStream_t);
+template void launch_sts_cg<double>(const SpmvPlan<double>&, const double*, double*, const double*, double*,
+                                    const double*, int, Ctrl*, cudaStream_t);
+
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st) {
     k_pcg_p<<<std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st>>>(n3, p, z, ctrl);
 }

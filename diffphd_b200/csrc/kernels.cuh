@@ -122,6 +122,11 @@ int gather_bs(int n);    // block size of the node gathers for n nodes
 
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st);
+// z = S^T S v (y = S v without its fix-up stage) whose last stage also performs the conjugate-gradient z-side
+// update: r.z, |z|, beta and the stop rule, as launch_pcg_update2 over (r, z) would (p.y_accumulate must be 0).
+template <typename T>
+void launch_sts_cg(const SpmvPlan<T>& p, const T* v, double* z, const double* r, double* part, const double* mu_part,
+                   int mu_blocks, Ctrl* ctrl, cudaStream_t st);
 
 
 // Anderson acceleration + gate ------------------------------------------------------------------
