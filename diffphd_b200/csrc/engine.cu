@@ -344,11 +344,26 @@ void Engine::build_device(int threads) {
         }
         d_item_desc.upload(od);
         d_item_slot.upload(os);
+        std::vector<int2> ors(ord.size());
+        for (size_t t = 0; t < ord.size(); ++t) {
+            const int r = it_row[ord[t]];
+            ors[t] = make_int2(r_ptr[r], r_ptr[r + 1]);
+        }
+        d_item_rslots.upload(ors);
         std::stable_sort(units.begin(), units.end(),
                          [](const int4& x, const int4& y) { return (long long)x.y * x.w > (long long)y.y * y.w; });
     }
     d_unit_item_desc.upload(idesc);
     d_unit_item_slot.upload(slot);
+    {
+        std::vector<int2> rs(it_row.size());
+        for (size_t t = 0; t < it_row.size(); ++t) rs[t] = make_int2(r_ptr[it_row[t]], r_ptr[it_row[t] + 1]);
+        d_unit_item_rslots.upload(rs);
+        d_row_cnt.alloc(std::max<size_t>(1, it_row.size()) * sizeof(unsigned int));
+        CUDA_OK(cudaMemset(d_row_cnt.p, 0, d_row_cnt.bytes));
+        d_yrow32.alloc(std::max<size_t>(1, it_row.size()) * 3 * sizeof(float));
+        d_yrow64.alloc(std::max<size_t>(1, it_row.size()) * 3 * sizeof(double));
+    }
     d_unit_desc.upload(units);
     d_trow_desc.upload(tdesc);
     d_trow_off.upload(toff);
@@ -417,6 +432,15 @@ void Engine::build_device(int threads) {
     plan32_.n_units = (int)units.size();
     plan32_.unit_desc = d_unit_desc.as<int4>();
     plan32_.unit_item_desc = d_unit_item_desc.as<int4>();
+    plan32_.unit_item_rslots = d_unit_item_rslots.as<int2>();
+    for (auto* P : {&plan32_}) {
+        P->yrow = d_yrow32.as<float>();
+        P->row_cnt = d_row_cnt.as<unsigned int>();
+        P->item_rslots = d_item_rslots.as<int2>();
+    }
+    plan64_.yrow = d_yrow64.as<double>();
+    plan64_.row_cnt = d_row_cnt.as<unsigned int>();
+    plan64_.item_rslots = d_item_rslots.as<int2>();
     plan32_.unit_item_slot = d_unit_item_slot.as<int>();
     plan32_.use_units = s_units_ ? 1 : 0;
     // mesh, samples, constraints

@@ -223,6 +223,7 @@ private:
     DeviceBuffer d_ctrl, d_adjnorm, d_part_adj, d_np_k, d_type_k, d_off_k, d_dmat_dev, d_dpar_dev, d_dstate_dev;
     DeviceBuffer d_item_desc, d_item_slot, d_trow_desc, d_trow_off, d_J32;
     DeviceBuffer d_unit_desc, d_unit_item_desc, d_unit_item_slot;  // row-group units of the FP32 y = S v pass
+    DeviceBuffer d_item_rslots, d_unit_item_rslots, d_row_cnt, d_yrow32, d_yrow64;  // multi-item row totals
     bool s_units_ = false;       // chosen by timing both kernels when the factor is built
     DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv, d_wlog, d_mu_prev;
     bool mu_prev_valid_ = false;

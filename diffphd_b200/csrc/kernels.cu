@@ -328,6 +328,27 @@ template <> struct Vec4<double> {
     }
 };
 
+// One thread per finished item of a row cut into several items: after its partial is stored, it counts itself
+// in; the last one sums the row's partials in slot order (the order the S^T pass would use) into yrow.
+template <typename T>
+__device__ __forceinline__ void row_arrive(const SpmvPlan<T>& p, int z, int w) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(p.row_cnt + z, 1u);
+    if (prev != (unsigned int)(w - z - 1)) return;
+    p.row_cnt[z] = 0u;  // ready for the next apply
+    __threadfence();
+    T s0 = T(0), s1 = T(0), s2 = T(0);
+    for (int k = z; k < w; ++k) {
+        s0 += __ldcg(p.ypart + 3 * (size_t)k);
+        s1 += __ldcg(p.ypart + 3 * (size_t)k + 1);
+        s2 += __ldcg(p.ypart + 3 * (size_t)k + 2);
+    }
+    T* o = p.yrow + 3 * (size_t)z;
+    o[0] = s0;
+    o[1] = s1;
+    o[2] = s2;
+}
+
 // y = S v, stage 1: one warp per work item (a row segment of <= kSegCols columns), four 16-byte loads of S
 // in flight per lane, v through L1 (the CTA's warps share the segment's columns).
 template <typename T>
@@ -337,6 +358,7 @@ __device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __re
     if (it >= p.n_items) return;
     const int4 dsc = __ldg(p.item_desc + it);
     const int slot = __ldg(p.item_slot + it);
+    const int2 rs = p.yrow ? __ldg(p.item_rslots + it) : make_int2(0, 1);
     if (done) return;
     const T* __restrict__ sv = p.vals + ((int64_t)(uint32_t)dsc.x | ((int64_t)dsc.y << 32));
     const int a = dsc.z, nc = dsc.w;
@@ -383,6 +405,7 @@ __device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __re
     if (lane == 0) {
         T* o = p.ypart + (size_t)slot * 3;
         o[0] = s0; o[1] = s1; o[2] = s2;
+        if (rs.y - rs.x > 1) row_arrive(p, rs.x, rs.y);
     }
 }
 
@@ -462,6 +485,10 @@ __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const f
         o[0] = o0;
         o[1] = o1;
         o[2] = o2;
+        if (p.yrow) {
+            const int2 rs = __ldg(p.unit_item_rslots + first + lane);
+            if (rs.y - rs.x > 1) row_arrive(p, rs.x, rs.y);
+        }
     }
 }
 
@@ -530,10 +557,19 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
             if (in[u]) sv[u].load_s(p.vals + off[u] + (c - dsc[u].x), p.keep_in_l2);
             yv[u][0] = yv[u][1] = yv[u][2] = T(0);
             if (FROM_ITEMS) {
-                for (int k = dsc[u].z; k < dsc[u].w; ++k) {
-                    yv[u][0] += __ldg(p.ypart + 3 * (size_t)k);
-                    yv[u][1] += __ldg(p.ypart + 3 * (size_t)k + 1);
-                    yv[u][2] += __ldg(p.ypart + 3 * (size_t)k + 2);
+                if (p.yrow) {  // one load per row: the item partial, or the row total of a multi-item row
+                    if (dsc[u].z < dsc[u].w) {
+                        const T* src = (dsc[u].w - dsc[u].z > 1 ? p.yrow : p.ypart) + 3 * (size_t)dsc[u].z;
+                        yv[u][0] = __ldg(src);
+                        yv[u][1] = __ldg(src + 1);
+                        yv[u][2] = __ldg(src + 2);
+                    }
+                } else {
+                    for (int k = dsc[u].z; k < dsc[u].w; ++k) {
+                        yv[u][0] += __ldg(p.ypart + 3 * (size_t)k);
+                        yv[u][1] += __ldg(p.ypart + 3 * (size_t)k + 1);
+                        yv[u][2] += __ldg(p.ypart + 3 * (size_t)k + 2);
+                    }
                 }
             } else if (pp + 8 * u < pe) {
                 const int i = __ldg(p.tile_rows + pp + 8 * u);

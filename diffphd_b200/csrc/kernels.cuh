@@ -101,6 +101,15 @@ struct SpmvPlan {
     // y = S v by row groups (FP32 factors): unit u = the items of one group of at most kUnitRows rows that
     // share a column segment (unit_desc: first item, rows, first column, widest row's columns); one warp
     // reads the segment of v once for all rows.  use_units = 0 selects the one-warp-per-item kernel.
+    // Rows cut into several items: the warp whose item of such a row finishes last sums the row's slot
+    // partials in slot order into yrow[3 z] (z = the row's first slot), so that the S^T pass reads one value
+    // per row.  item_rslots / unit_item_rslots: (first slot, end slot) of each item's row, in the launch order
+    // of the item kernel and in emission order; row_cnt: per-row arrival counters indexed by z (zero between
+    // applies: the last arrival resets its counter).  Null yrow keeps the S^T pass summing the slots itself.
+    T* yrow = nullptr;
+    unsigned int* row_cnt = nullptr;
+    const int2* item_rslots = nullptr;
+    const int2* unit_item_rslots = nullptr;
     int n_units = 0, use_units = 0;
     const int4* unit_desc = nullptr;
     const int4* unit_item_desc = nullptr;  // the items in emission order (a unit's rows are consecutive here)

@@ -90,6 +90,8 @@ void run(const SpmvPlan<T>& plan, const unsigned char* fixed_node, const double*
     p.ypart = reinterpret_cast<T*>(base + yp_off);
     p.xpart = reinterpret_cast<T*>(base + xp_off);
     p.x_base = nullptr;
+    p.yrow = nullptr;  // the S^T pass sums each row's item partials itself: no buffer outside the static array
+    p.row_cnt = nullptr;
     const Ctrl* ctrl = reinterpret_cast<const Ctrl*>(base + ctrl_off);
     const int threads = 256, blocks = (std::max(npad, 64) + threads - 1) / threads;
     k_noalloc_prepare<T><<<blocks, threads, 0, st>>>(n, npad, d_b, fixed_node, plan.perm, ctrl_off, v_off);
