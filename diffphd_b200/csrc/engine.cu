@@ -652,6 +652,7 @@ void Engine::build_contact(double dt) {
 void Engine::reset_warm_start() {
     if (has_contact_ && dc_lam.p) CUDA_OK(cudaMemset(dc_lam.p, 0, dc_lam.bytes));
     mu_prev_valid_ = false;
+    mu_prev2_valid_ = false;
     ws_prev_valid_ = false;
 }
 
@@ -1463,9 +1464,18 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         const bool warm = o.bwd_warm_start && mu_prev_valid_ && d_mu_prev.bytes == n3 * sizeof(double);
         const double* w0 = nullptr;
         if (warm) {
-            CUDA_OK(cudaMemcpyAsync(d_x.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-            launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
-                            d_J.as<double>(), d_elem_out64.as<double>(), c, st);
+            if (o.bwd_warm_start == 2 && mu_prev2_valid_)  // linear extrapolation of the last two adjoints
+                launch_extrapolate(n3, d_mu_prev.as<double>(), d_mu_prev2.as<double>(), d_x.as<double>(), st);
+            else
+                CUDA_OK(cudaMemcpyAsync(d_x.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            // the start's residual uses the iteration's own K_pd (FP32 Jacobians in mixed mode), so that the
+            // solve converges to the same adjoint whatever the start
+            if (f32)
+                launch_kpd_elem32(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
+                                  d_J32.as<float>(), d_elem_out64.as<double>(), c, st);
+            else
+                launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex,
+                                d_J.as<double>(), d_elem_out64.as<double>(), c, st);
             launch_pcg_gather(M.n, Acsr_, d_x.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
                               d_elem_out64.as<double>(), d_fixed_node.as<unsigned char>(), d_wv.as<double>(),
                               d_part_gate.as<double>(), gather_blocks_, c, st, 1);
@@ -1511,6 +1521,11 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         return;
     }
     if (o.bwd_warm_start) {
+        if (o.bwd_warm_start == 2 && mu_prev_valid_) {
+            d_mu_prev2.alloc(n3 * sizeof(double));
+            CUDA_OK(cudaMemcpyAsync(d_mu_prev2.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            mu_prev2_valid_ = true;
+        }
         d_mu_prev.alloc(n3 * sizeof(double));
         CUDA_OK(cudaMemcpyAsync(d_mu_prev.p, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
         mu_prev_valid_ = true;

@@ -1845,6 +1845,15 @@ template void launch_sts_cg<float>(const SpmvPlan<float>&, const float*, double*
 template void launch_sts_cg<double>(const SpmvPlan<double>&, const double*, double*, const double*, double*,
                                     const double*, int, Ctrl*, cudaStream_t);
 
+__global__ void k_extrapolate(int n3, const double* __restrict__ a, const double* __restrict__ b,
+                              double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) out[k] = 2.0 * a[k] - b[k];
+}
+void launch_extrapolate(int n3, const double* a, const double* b, double* out, cudaStream_t st) {
+    k_extrapolate<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, a, b, out);
+}
+
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st) {
     k_pcg_p<<<std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st>>>(n3, p, z, ctrl);
 }

@@ -186,6 +186,8 @@ void launch_pcg_update1(int n, double* mu, double* r, const double* p, const dou
 void launch_pcg_update2(int n3, const double* r, const double* z, double* part, const double* mu_part, int mu_blocks,
                         int blocks, Ctrl* ctrl, cudaStream_t st);
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st);
+// out = 2 a - b (linear extrapolation of the last two adjoints for the next solve's start)
+void launch_extrapolate(int n3, const double* a, const double* b, double* out, cudaStream_t st);
 // r = g_bar - w on free DoFs (0 on Dirichlet; w = (A - K_pd) mu_0 or null for mu_0 = 0), permuted right-hand
 // side for the first preconditioner apply.
 template <typename T>
