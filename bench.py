@@ -222,7 +222,7 @@ def options(sc, precision, warm=False):
     if precision == "mixed":
         o["fp32_bulk"] = 1
     if warm:
-        o["alg_phd_bwd_warm_start"] = 2  # extrapolated from the last two adjoints of the reverse sweep
+        o["alg_phd_bwd_warm_start"] = 3  # quadratic extrapolation of the last three adjoints of the sweep
     return o
 
 
@@ -485,7 +485,7 @@ def _measure(args, rank, world, local_rank, precision, full, sc, d, mlp, warm):
                    "precision": "fp32 bulk (projection, S/S^T) + fp64 gate/AA" if fp32 else "plain fp64",
                    "pd_start": "learned warm start (per-node MLP, BF16 tensor cores)" if mlp is not None
                    else "q (reference)",
-                   "adjoint_start": "2 mu_1 - mu_2 (last two adjoints of the sweep)" if warm else "0 (reference)",
+                   "adjoint_start": "3 (mu_1 - mu_2) + mu_3 (last three adjoints of the sweep)" if warm else "0 (reference)",
                    "rel_tol": opts["rel_tol"], "abs_tol": opts["abs_tol"], "aa_window": opts["aa_window"],
                    "max_pd_iter": opts["max_pd_iter"], "step": "forward PD step + adjoint step",
                    "adjoint_solver": "PCG on (A - K_pd) preconditioned by S^T S, FP64 residual",

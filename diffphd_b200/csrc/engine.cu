@@ -653,6 +653,7 @@ void Engine::reset_warm_start() {
     if (has_contact_ && dc_lam.p) CUDA_OK(cudaMemset(dc_lam.p, 0, dc_lam.bytes));
     mu_prev_valid_ = false;
     mu_prev2_valid_ = false;
+    mu_prev3_valid_ = false;
     ws_prev_valid_ = false;
 }
 
@@ -1464,7 +1465,10 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         const bool warm = o.bwd_warm_start && mu_prev_valid_ && d_mu_prev.bytes == n3 * sizeof(double);
         const double* w0 = nullptr;
         if (warm) {
-            if (o.bwd_warm_start == 2 && mu_prev2_valid_)  // linear extrapolation of the last two adjoints
+            if (o.bwd_warm_start == 3 && mu_prev3_valid_)  // quadratic extrapolation of the last three
+                launch_extrapolate3(n3, d_mu_prev.as<double>(), d_mu_prev2.as<double>(), d_mu_prev3.as<double>(),
+                                    d_x.as<double>(), st);
+            else if (o.bwd_warm_start >= 2 && mu_prev2_valid_)  // linear extrapolation of the last two adjoints
                 launch_extrapolate(n3, d_mu_prev.as<double>(), d_mu_prev2.as<double>(), d_x.as<double>(), st);
             else
                 CUDA_OK(cudaMemcpyAsync(d_x.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -1521,7 +1525,12 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         return;
     }
     if (o.bwd_warm_start) {
-        if (o.bwd_warm_start == 2 && mu_prev_valid_) {
+        if (o.bwd_warm_start == 3 && mu_prev2_valid_) {
+            d_mu_prev3.alloc(n3 * sizeof(double));
+            CUDA_OK(cudaMemcpyAsync(d_mu_prev3.p, d_mu_prev2.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            mu_prev3_valid_ = true;
+        }
+        if (o.bwd_warm_start >= 2 && mu_prev_valid_) {
             d_mu_prev2.alloc(n3 * sizeof(double));
             CUDA_OK(cudaMemcpyAsync(d_mu_prev2.p, d_mu_prev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
             mu_prev2_valid_ = true;

@@ -1853,6 +1853,14 @@ __global__ void k_extrapolate(int n3, const double* __restrict__ a, const double
 void launch_extrapolate(int n3, const double* a, const double* b, double* out, cudaStream_t st) {
     k_extrapolate<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, a, b, out);
 }
+__global__ void k_extrapolate3(int n3, const double* __restrict__ a, const double* __restrict__ b,
+                               const double* __restrict__ c, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) out[k] = 3.0 * (a[k] - b[k]) + c[k];
+}
+void launch_extrapolate3(int n3, const double* a, const double* b, const double* c, double* out, cudaStream_t st) {
+    k_extrapolate3<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, a, b, c, out);
+}
 
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st) {
     k_pcg_p<<<std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st>>>(n3, p, z, ctrl);
