@@ -100,6 +100,7 @@ def load_library():
     L.dphd_debug_host_sts.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     L.dphd_debug_s_rows.argtypes = [C.c_void_p, C.c_double, _ip, _ip]
     L.dphd_debug_set_s_kernel.argtypes = [C.c_void_p, C.c_int]
+    L.dphd_debug_set_pdl.argtypes = [C.c_void_p, C.c_int]
     L.dphd_debug_local_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     _lib = L
     return L
@@ -400,6 +401,10 @@ class Deformable:
         lo, perm = np.zeros(n, np.int32), np.zeros(n, np.int32)
         self._check(self._L.dphd_debug_s_rows(self._h, float(dt), _iptr(lo), _iptr(perm)))
         return lo, perm
+
+    def set_pdl(self, on=True):
+        """Programmatic dependent launch of the iteration-body kernels (process-wide; default on)."""
+        self._check(self._L.dphd_debug_set_pdl(self._h, int(bool(on))))
 
     def set_s_kernel(self, row_groups=True):
         """FP32 y = S v pass: one warp per row group or one warp per row segment (bit-identical sums; by default

@@ -390,6 +390,13 @@ int dphd_debug_set_s_kernel(dphd_deformable* h, int row_groups) {
     return guard([&] { E(h).set_s_units(row_groups != 0); });
 }
 
+int dphd_debug_set_pdl(dphd_deformable* h, int on) {
+    return guard([&] {
+        dphd::set_pdl(on != 0);
+        E(h).drop_captured_graphs();
+    });
+}
+
 int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream) {
     return guard([&] { E(h).ainv_noalloc(dt, d_b, d_x, fp32 != 0, (cudaStream_t)stream); });
 }

@@ -129,6 +129,7 @@ public:
     // selects the row-group or the one-warp-per-item kernel of the FP32 y = S v pass (overriding the choice
     // timed at factor build); drops the captured iteration graphs
     void set_s_units(bool on);
+    void drop_captured_graphs() { drop_graphs(); }
 
     void backward_device(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,
                          double* d_dq, double* d_dv, double* d_df, double* d_dmat_w, double* d_dparams,

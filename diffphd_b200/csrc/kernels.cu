@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <utility>
 
 #include "kernels.cuh"
 
@@ -14,6 +15,16 @@ namespace dphd {
 namespace {
 
 constexpr int kThreads = 256;
+
+// Programmatic dependent launch.  The kernels of an iteration body are launched with programmatic stream
+// serialization (launch_k below), so each grid is launched while its predecessor drains; every such kernel
+// begins with pdl_enter: it lets its own successor launch, then waits (griddepcontrol.wait) until the
+// predecessor grid has completed and its memory is visible, before reading anything.  Launched without the
+// attribute, the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -117,6 +128,7 @@ __global__ void __launch_bounds__(kThreads) k_elem_fwd(int m, const int* __restr
                                                        const unsigned char* __restrict__ elem_dir,
                                                        const double* __restrict__ grad, double vol_over_s,
                                                        EnergyPack ep, double* __restrict__ out, Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = t / S, smp = t % S;
@@ -249,6 +261,7 @@ __global__ void __launch_bounds__(kGatherMaxThreads) k_gather_fwd(int n, const i
                                                          double* __restrict__ prev, double* __restrict__ part,
                                                          NodeCsr A, const double* __restrict__ q, int zero_dirichlet,
                                                          double* __restrict__ r_out, Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
@@ -411,6 +424,7 @@ __device__ __forceinline__ void s_items_body(const SpmvPlan<T>& p, const T* __re
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __restrict__ v, const Ctrl* ctrl) {
+    pdl_enter();
     s_items_body(p, v, blockIdx.x, ctrl);
 }
 
@@ -421,6 +435,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
 // float4 (row lengths and segment starts are multiples of 4).  Partial sums go to the rows' item slots.
 __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const float* __restrict__ v,
                                                       const Ctrl* ctrl) {
+    pdl_enter();
     const int done = ctrl->done;  // in flight together with the unit descriptor, tested after it
     const int u = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (u >= p.n_units) return;
@@ -495,6 +510,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const f
 // y = S v, stage 2: per row, the item partials in item order.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __restrict__ y, const Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -606,6 +622,7 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
 
 template <typename T, bool FROM_ITEMS>
 __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
+    pdl_enter();
     st_part_body<T, FROM_ITEMS>(p, y, blockIdx.x, ctrl);
 }
 
@@ -637,6 +654,7 @@ __device__ __forceinline__ void st_fin_body(const SpmvPlan<T>& p, double* __rest
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_spmv_ST_fin(SpmvPlan<T> p, double* __restrict__ x_out,
                                                           const Ctrl* ctrl) {
+    pdl_enter();
     st_fin_body(p, x_out, blockIdx.x, ctrl);
 }
 
@@ -656,6 +674,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_reduce(int n3, const double* __
                                                         double* __restrict__ dX, double* __restrict__ lg,
                                                         double* __restrict__ lx, int ld, double* __restrict__ part,
                                                         Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     __shared__ double sh[kAaVals * 32];
     const int W = ctrl->window, count = ctrl->count, head = ctrl->head, mode = ctrl->mode;
@@ -804,6 +823,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_update(int n3, double* __restri
                                                         int ld, double* __restrict__ part,
                                                         const double* __restrict__ gate_part, int gate_blocks,
                                                         Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     __shared__ double sh[3 * 32];
     const int W = ctrl->window, head = ctrl->head, mode = ctrl->mode;
@@ -1015,6 +1035,7 @@ template <int K, int S>
 __global__ void __launch_bounds__(kThreads) k_kpd_elem(int m, const int* __restrict__ E, const double* __restrict__ u,
                                                        const double* __restrict__ grad, const double* __restrict__ J,
                                                        double* __restrict__ out, const Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = t / S, smp = t % S;
@@ -1073,6 +1094,7 @@ __global__ void __launch_bounds__(kThreads) k_kpd_elem32(int m, const int* __res
                                                          const double* __restrict__ u, const double* __restrict__ grad,
                                                          const float* __restrict__ J32, double* __restrict__ out,
                                                          const Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = t / S, smp = t % S;
@@ -1143,6 +1165,7 @@ __global__ void __launch_bounds__(kGatherMaxThreads) k_gather_bwd(int n, const i
                                                          const unsigned char* __restrict__ fixed,
                                                          const int* __restrict__ iperm, double* __restrict__ v,
                                                          int npad, const Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     const int lane = threadIdx.x & (kGatherLanes - 1);
     const int per_block = (int)blockDim.x / kGatherLanes;
@@ -1277,6 +1300,7 @@ __global__ void __launch_bounds__(kGatherMaxThreads) k_pcg_gather(int n, NodeCsr
                                                          const unsigned char* __restrict__ fixed,
                                                          double* __restrict__ w, double* __restrict__ part,
                                                          Ctrl* ctrl, int init) {
+    pdl_enter();
     if (ctrl->done) return;
     __shared__ double sh[32];
     double acc[1] = {0.0};
@@ -1327,6 +1351,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_update1(int n, double* __restr
                                                           const unsigned char* __restrict__ fixed,
                                                           const int* __restrict__ iperm, T* __restrict__ v, int npad,
                                                           double* __restrict__ part, Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     __shared__ double sh[32];
     const double alpha = ctrl->alpha;
@@ -1356,6 +1381,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_update2(int n3, const double* 
                                                           const double* __restrict__ z, double* __restrict__ part,
                                                           const double* __restrict__ mu_part, int mu_blocks,
                                                           Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     __shared__ double sh[2 * 32];
     double acc[2] = {0.0, 0.0};
@@ -1410,6 +1436,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_ST_fin_cg(SpmvPlan<T> p, doub
                                                              const double* __restrict__ r, double* __restrict__ part,
                                                              const double* __restrict__ mu_part, int mu_blocks,
                                                              Ctrl* ctrl) {
+    pdl_enter();
     __shared__ double sh[2 * 32];
     const int done = ctrl->done;
     const int t = blockIdx.x * (int)blockDim.x + (int)threadIdx.x;
@@ -1448,6 +1475,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_ST_fin_cg(SpmvPlan<T> p, doub
 }
 
 __global__ void k_pcg_p(int n3, double* __restrict__ p, const double* __restrict__ z, const Ctrl* ctrl) {
+    pdl_enter();
     if (ctrl->done) return;
     const double beta = ctrl->beta;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x) p[k] = z[k] + beta * p[k];
@@ -1570,8 +1598,30 @@ __global__ void k_param_reduce(int m, const int* __restrict__ np_k, const int* _
 }
 
 inline int blocks_for(long long work, int threads) { return (int)((work + threads - 1) / threads); }
+bool g_pdl = true;  // programmatic dependent launch of the iteration-body kernels (process-wide)
+
+// Launches `kern` with programmatic stream serialization when g_pdl is set: the grid may start while its
+// predecessor in the stream drains (the kernel's pdl_enter waits for the predecessor's completion before it
+// reads anything).  Inside stream capture this becomes a programmatic edge of the graph.
+template <typename... KArgs, typename... Args>
+void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 
 }  // namespace
+
+void set_pdl(bool on) { g_pdl = on; }
 
 int device_sms() {
     static int cached[64] = {0};
@@ -1624,8 +1674,8 @@ void launch_elem_fwd(int m, int k, int s, const int* E, const double* q, const d
                      cudaStream_t st) {
     int grid, bs;
     even_grid((long long)m * s, kThreads, 1 << 30, &grid, &bs);
-    if (hex) k_elem_fwd<T, 8, 8><<<grid, bs, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
-    else k_elem_fwd<T, 4, 1><<<grid, bs, 0, st>>>(m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
+    if (hex) launch_k(k_elem_fwd<T, 8, 8>, grid, bs, 0, st, m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
+    else launch_k(k_elem_fwd<T, 4, 1>, grid, bs, 0, st, m, E, q, qb, elem_dir, grad, vol_over_s, ep, elem_out, ctrl);
 }
 
 template <typename T>
@@ -1633,7 +1683,7 @@ void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const do
                        double inv_h2m, const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad,
                        double* prev_pd, double* part, int blocks, NodeCsr A, const double* q, int zero_dirichlet,
                        Ctrl* ctrl, cudaStream_t st, double* r_out) {
-    k_gather_fwd<T><<<blocks, gather_bs(n), 0, st>>>(n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
+    launch_k(k_gather_fwd<T>, blocks, gather_bs(n), 0, st, n, node_ptr, node_inc, elem_out, qt, inv_h2m, fixed_node, iperm,
                                                      v_perm, npad, prev_pd, part, A, q, zero_dirichlet, r_out, ctrl);
 }
 
@@ -1642,36 +1692,36 @@ template <typename T>
 static void launch_s_items(const SpmvPlan<T>& p, const T* v, const Ctrl* ctrl, cudaStream_t st) {
     if constexpr (std::is_same<T, float>::value) {
         if (p.use_units && p.n_units > 0) {
-            k_spmv_S_units<<<blocks_for((long long)p.n_units * 32, 256), 256, 0, st>>>(p, v, ctrl);
+            launch_k(k_spmv_S_units, blocks_for((long long)p.n_units * 32, 256), 256, 0, st, p, v, ctrl);
             return;
         }
     }
-    k_spmv_S_items<T><<<blocks_for((long long)p.n_items * 32, 256), 256, 0, st>>>(p, v, ctrl);
+    launch_k(k_spmv_S_items<T>, blocks_for((long long)p.n_items * 32, 256), 256, 0, st, p, v, ctrl);
 }
 
 template <typename T>
 void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
     launch_s_items(p, v, ctrl, st);
     if (p.y_accumulate) {
-        k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
-        k_spmv_ST_part<T, false><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
+        launch_k(k_spmv_S_fin<T>, blocks_for(p.n, kThreads), kThreads, 0, st, p, y, ctrl);
+        launch_k(k_spmv_ST_part<T, false>, p.n_chunks, 256, 0, st, p, y, ctrl);
     } else {
-        k_spmv_ST_part<T, true><<<p.n_chunks, 256, 0, st>>>(p, nullptr, ctrl);
+        launch_k(k_spmv_ST_part<T, true>, p.n_chunks, 256, 0, st, p, nullptr, ctrl);
     }
-    k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
+    launch_k(k_spmv_ST_fin<T>, blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st, p, x_out, ctrl);
 }
 
 void launch_aa_reduce(int n3, const double* x, const double* x_raw, const unsigned char* fixed_dof,
                       const double* fixed_val, double* dG, double* dX, double* last_g, double* last_x, int ld,
                       double* part, int blocks, Ctrl* ctrl, cudaStream_t st) {
-    k_aa_reduce<<<blocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, last_g, last_x, ld, part,
+    launch_k(k_aa_reduce, blocks, kThreads, 0, st, n3, x, x_raw, fixed_dof, fixed_val, dG, dX, last_g, last_x, ld, part,
                                                 ctrl);
 }
 
 void launch_aa_update(int n3, double* x, const double* x_raw, const unsigned char* fixed_dof, const double* fixed_val,
                       const double* dG, const double* dX, int ld, double* part, const double* gate_part,
                       int gate_blocks, int blocks, Ctrl* ctrl, cudaStream_t st) {
-    k_aa_update<<<blocks, kThreads, 0, st>>>(n3, x, x_raw, fixed_dof, fixed_val, dG, dX, ld, part, gate_part,
+    launch_k(k_aa_update, blocks, kThreads, 0, st, n3, x, x_raw, fixed_dof, fixed_val, dG, dX, ld, part, gate_part,
                                                 gate_blocks, ctrl);
 }
 
@@ -1698,8 +1748,8 @@ void launch_kpd_elem32(int m, int k, int s, const int* E, const double* u, const
     (void)k;
     int grid, bs;
     even_grid((long long)m * s, kThreads, 1 << 30, &grid, &bs);
-    if (hex) k_kpd_elem32<8, 8><<<grid, bs, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
-    else k_kpd_elem32<4, 1><<<grid, bs, 0, st>>>(m, E, u, grad, J32, elem_out, ctrl);
+    if (hex) launch_k(k_kpd_elem32<8, 8>, grid, bs, 0, st, m, E, u, grad, J32, elem_out, ctrl);
+    else launch_k(k_kpd_elem32<4, 1>, grid, bs, 0, st, m, E, u, grad, J32, elem_out, ctrl);
 }
 
 void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const double* grad, int hex, const double* J,
@@ -1707,15 +1757,15 @@ void launch_kpd_elem(int m, int k, int s, const int* E, const double* u, const d
     (void)k;
     int grid, bs;
     even_grid((long long)m * s, kThreads, 1 << 30, &grid, &bs);
-    if (hex) k_kpd_elem<8, 8><<<grid, bs, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
-    else k_kpd_elem<4, 1><<<grid, bs, 0, st>>>(m, E, u, grad, J, elem_out, ctrl);
+    if (hex) launch_k(k_kpd_elem<8, 8>, grid, bs, 0, st, m, E, u, grad, J, elem_out, ctrl);
+    else launch_k(k_kpd_elem<4, 1>, grid, bs, 0, st, m, E, u, grad, J, elem_out, ctrl);
 }
 
 void launch_gather_bwd(int n, const int* node_ptr, const int* node_inc, const double* elem_out, const double* gbar,
                        const unsigned char* fixed_node, const int* iperm, double* v_perm, int npad, const Ctrl* ctrl,
                        cudaStream_t st) {
     const int blocks = std::max(1, std::min(kMaxRedBlocks, (n * kGatherLanes + kThreads - 1) / kThreads));
-    k_gather_bwd<<<blocks, gather_bs(n), 0, st>>>(n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm, npad,
+    launch_k(k_gather_bwd, blocks, gather_bs(n), 0, st, n, node_ptr, node_inc, elem_out, gbar, fixed_node, iperm, v_perm, npad,
                                               ctrl);
 }
 
@@ -1742,7 +1792,7 @@ template void launch_gather_fwd<float>(int, const int*, const int*, const double
 void launch_pcg_gather(int n, NodeCsr A, const double* p, const int* node_ptr, const int* node_inc,
                        const double* elem_out, const unsigned char* fixed_node, double* w, double* part, int blocks,
                        Ctrl* ctrl, cudaStream_t st, int init) {
-    k_pcg_gather<<<blocks, gather_bs(n), 0, st>>>(n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl,
+    launch_k(k_pcg_gather, blocks, gather_bs(n), 0, st, n, A, p, node_ptr, node_inc, elem_out, fixed_node, w, part, ctrl,
                                               init);
 }
 
@@ -1826,18 +1876,18 @@ template <typename T>
 void launch_pcg_update1(int n, double* mu, double* r, const double* p, const double* w,
                         const unsigned char* fixed_node, const int* iperm, T* v_perm, int npad, double* part,
                         int blocks, Ctrl* ctrl, cudaStream_t st) {
-    k_pcg_update1<T><<<blocks, kThreads, 0, st>>>(n, mu, r, p, w, fixed_node, iperm, v_perm, npad, part, ctrl);
+    launch_k(k_pcg_update1<T>, blocks, kThreads, 0, st, n, mu, r, p, w, fixed_node, iperm, v_perm, npad, part, ctrl);
 }
 void launch_pcg_update2(int n3, const double* r, const double* z, double* part, const double* mu_part, int mu_blocks,
                         int blocks, Ctrl* ctrl, cudaStream_t st) {
-    k_pcg_update2<<<blocks, kThreads, 0, st>>>(n3, r, z, part, mu_part, mu_blocks, ctrl);
+    launch_k(k_pcg_update2, blocks, kThreads, 0, st, n3, r, z, part, mu_part, mu_blocks, ctrl);
 }
 template <typename T>
 void launch_sts_cg(const SpmvPlan<T>& p, const T* v, double* z, const double* r, double* part, const double* mu_part,
                    int mu_blocks, Ctrl* ctrl, cudaStream_t st) {
     launch_s_items(p, v, ctrl, st);
-    k_spmv_ST_part<T, true><<<p.n_chunks, 256, 0, st>>>(p, nullptr, ctrl);
-    k_spmv_ST_fin_cg<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(
+    launch_k(k_spmv_ST_part<T, true>, p.n_chunks, 256, 0, st, p, nullptr, ctrl);
+    launch_k(k_spmv_ST_fin_cg<T>, blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st, 
         p, z, r, part, mu_part, mu_blocks, ctrl);
 }
 template void launch_sts_cg<float>(const SpmvPlan<float>&, const float*, double*, const double*, double*,
@@ -1863,7 +1913,7 @@ void launch_extrapolate3(int n3, const double* a, const double* b, const double*
 }
 
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st) {
-    k_pcg_p<<<std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st>>>(n3, p, z, ctrl);
+    launch_k(k_pcg_p, std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st, n3, p, z, ctrl);
 }
 template <typename T>
 void launch_pcg_init(int n, const double* gbar, const double* w, const unsigned char* fixed_node, const int* iperm,
@@ -1902,12 +1952,12 @@ void launch_param_reduce(int m, int ne, const int* np_k, const int* type_k, cons
 template <typename T>
 void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cudaStream_t st) {
     launch_s_items(p, v, ctrl, st);
-    k_spmv_S_fin<T><<<blocks_for(p.n, kThreads), kThreads, 0, st>>>(p, y, ctrl);
+    launch_k(k_spmv_S_fin<T>, blocks_for(p.n, kThreads), kThreads, 0, st, p, y, ctrl);
 }
 template <typename T>
 void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
-    k_spmv_ST_part<T, false><<<p.n_chunks, 256, 0, st>>>(p, y, ctrl);
-    k_spmv_ST_fin<T><<<blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st>>>(p, x_out, ctrl);
+    launch_k(k_spmv_ST_part<T, false>, p.n_chunks, 256, 0, st, p, y, ctrl);
+    launch_k(k_spmv_ST_fin<T>, blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st, p, x_out, ctrl);
 }
 template void launch_s_only<double>(const SpmvPlan<double>&, const double*, double*, const Ctrl*, cudaStream_t);
 template void launch_s_only<float>(const SpmvPlan<float>&, const float*, float*, const Ctrl*, cudaStream_t);

@@ -125,6 +125,9 @@ constexpr int kGatherMaxThreads = 512;  // block-size bound of the node gathers
 // most `max_bs` threads (a multiple of 32), with the fewest blocks per SM that fit and equal-sized blocks, so
 // that no SM holds a block more than the others (a partly filled last wave doubles a short kernel's time).
 int device_sms();
+// Programmatic dependent launch of the iteration-body kernels (default on; process-wide).  Graphs captured
+// afterwards use the setting; already captured graphs keep theirs.
+void set_pdl(bool on);
 void even_grid(long long threads, int max_bs, int max_grid, int* grid, int* bs);
 int gather_grid(int n);  // grid of the node gathers for n nodes (also the count of their per-block partials)
 int gather_bs(int n);    // block size of the node gathers for n nodes

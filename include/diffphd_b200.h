@@ -128,6 +128,11 @@ long long dphd_s_padded_values(const dphd_deformable* h);
  * faster one on the factor is chosen by timing both when the factor is built.  Captured iteration graphs are
  * dropped.  No counterpart in the reference (profiling and A/B timing). */
 int dphd_debug_set_s_kernel(dphd_deformable* h, int row_groups);
+/* Programmatic dependent launch of the kernels inside the iteration graphs (1, the default: each kernel may
+ * launch while its predecessor drains and waits for it on the device; 0: plain stream order).  The setting is
+ * process-wide; this handle's captured graphs are dropped so that they are captured again with it.  No
+ * counterpart in the reference (A/B timing). */
+int dphd_debug_set_pdl(dphd_deformable* h, int on);
 /* x = A^-1 b through the S^T S pair on device pointers (b, x: 3n FP64 node-major; Dirichlet rows of b are
  * taken as zero, as in the forward step), allocating no GPU memory: its temporaries live in a static 32 MiB
  * device array instead.  No counterpart in the reference.  For callers that cannot call cudaMalloc during a
