@@ -20,7 +20,10 @@ constexpr int kThreads = 256;
 // serialization (launch_k below), so each grid is launched while its predecessor drains; every such kernel
 // begins with pdl_enter: it lets its own successor launch, then waits (griddepcontrol.wait) until the
 // predecessor grid has completed and its memory is visible, before reading anything.  Launched without the
-// attribute, the wait returns at once.
+// attribute, the wait returns at once.  Every such kernel then reads ctrl->done with an ordinary load (ordered
+// after the wait's memory clobber) and branches on it before it touches data a predecessor wrote: loads through
+// the read-only path (ld.global.nc, which the compiler may treat as invariant and move across the wait) stay
+// behind that branch, so none is issued before the wait.
 __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");
