@@ -548,9 +548,9 @@ def main():
     ap.add_argument("--host-loop", action="store_true",
                     help="profiling: replay each iteration graph from the host instead of one device-side WHILE "
                          "graph per solve (same kernels; ncu does not profile kernels inside conditional nodes)")
-    ap.add_argument("--ws-seeds", type=int, default=8, help="material seeds of the warm-start training rollouts")
+    ap.add_argument("--ws-seeds", type=int, default=12, help="material seeds of the warm-start training rollouts")
     ap.add_argument("--ws-steps", type=int, default=60, help="rollout steps per training seed")
-    ap.add_argument("--ws-fit-steps", type=int, default=1500, help="AdamW steps of warm-start training")
+    ap.add_argument("--ws-fit-steps", type=int, default=4000, help="AdamW steps of warm-start training")
     args = ap.parse_args()
     global HOST_LOOP
     HOST_LOOP = args.host_loop
