@@ -654,6 +654,7 @@ void Engine::reset_warm_start() {
     mu_prev_valid_ = false;
     mu_prev2_valid_ = false;
     mu_prev3_valid_ = false;
+    mu_prev4_valid_ = false;
     ws_prev_valid_ = false;
 }
 
@@ -1465,7 +1466,10 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         const bool warm = o.bwd_warm_start && mu_prev_valid_ && d_mu_prev.bytes == n3 * sizeof(double);
         const double* w0 = nullptr;
         if (warm) {
-            if (o.bwd_warm_start == 3 && mu_prev3_valid_)  // quadratic extrapolation of the last three
+            if (o.bwd_warm_start == 4 && mu_prev4_valid_)  // cubic extrapolation of the last four
+                launch_extrapolate4(n3, d_mu_prev.as<double>(), d_mu_prev2.as<double>(), d_mu_prev3.as<double>(),
+                                    d_mu_prev4.as<double>(), d_x.as<double>(), st);
+            else if (o.bwd_warm_start >= 3 && mu_prev3_valid_)  // quadratic extrapolation of the last three
                 launch_extrapolate3(n3, d_mu_prev.as<double>(), d_mu_prev2.as<double>(), d_mu_prev3.as<double>(),
                                     d_x.as<double>(), st);
             else if (o.bwd_warm_start >= 2 && mu_prev2_valid_)  // linear extrapolation of the last two adjoints
@@ -1525,7 +1529,12 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         return;
     }
     if (o.bwd_warm_start) {
-        if (o.bwd_warm_start == 3 && mu_prev2_valid_) {
+        if (o.bwd_warm_start == 4 && mu_prev3_valid_) {
+            d_mu_prev4.alloc(n3 * sizeof(double));
+            CUDA_OK(cudaMemcpyAsync(d_mu_prev4.p, d_mu_prev3.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            mu_prev4_valid_ = true;
+        }
+        if (o.bwd_warm_start >= 3 && mu_prev2_valid_) {
             d_mu_prev3.alloc(n3 * sizeof(double));
             CUDA_OK(cudaMemcpyAsync(d_mu_prev3.p, d_mu_prev2.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
             mu_prev3_valid_ = true;

@@ -227,8 +227,8 @@ private:
     DeviceBuffer d_item_rslots, d_unit_item_rslots, d_row_cnt, d_yrow32, d_yrow64;  // multi-item row totals
     bool s_units_ = false;       // chosen by timing both kernels when the factor is built
     DeviceBuffer d_gq, d_gv, d_dq, d_dv, d_df, d_A_rp, d_A_ci, d_A_v, d_r, d_pp, d_wv, d_wlog, d_mu_prev;
-    bool mu_prev_valid_ = false, mu_prev2_valid_ = false, mu_prev3_valid_ = false;
-    DeviceBuffer d_mu_prev2, d_mu_prev3;  // the adjoints before d_mu_prev (bwd_warm_start 2 / 3: extrapolation)
+    bool mu_prev_valid_ = false, mu_prev2_valid_ = false, mu_prev3_valid_ = false, mu_prev4_valid_ = false;
+    DeviceBuffer d_mu_prev2, d_mu_prev3, d_mu_prev4;  // the adjoints before d_mu_prev (bwd_warm_start 2-4)
     const double* ws_predict(const double* d_q, const double* d_v, const double* d_f, double dt, bool tcgen05,
                              cudaStream_t st);
     bool ws_net_ = false, ws_prev_valid_ = false;

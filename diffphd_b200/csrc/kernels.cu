@@ -1914,6 +1914,15 @@ __global__ void k_extrapolate3(int n3, const double* __restrict__ a, const doubl
 void launch_extrapolate3(int n3, const double* a, const double* b, const double* c, double* out, cudaStream_t st) {
     k_extrapolate3<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, a, b, c, out);
 }
+__global__ void k_extrapolate4(int n3, const double* __restrict__ a, const double* __restrict__ b,
+                               const double* __restrict__ c, const double* __restrict__ d, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) out[k] = 4.0 * (a[k] + c[k]) - 6.0 * b[k] - d[k];
+}
+void launch_extrapolate4(int n3, const double* a, const double* b, const double* c, const double* d, double* out,
+                         cudaStream_t st) {
+    k_extrapolate4<<<blocks_for(n3, kThreads), kThreads, 0, st>>>(n3, a, b, c, d, out);
+}
 
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st) {
     launch_k(k_pcg_p, std::max(1, std::min(kMaxRedBlocks, (n3 + 255) / 256)), kThreads, 0, st, n3, p, z, ctrl);

@@ -193,6 +193,9 @@ void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStre
 void launch_extrapolate(int n3, const double* a, const double* b, double* out, cudaStream_t st);
 // out = 3 (a - b) + c (quadratic extrapolation of the last three adjoints)
 void launch_extrapolate3(int n3, const double* a, const double* b, const double* c, double* out, cudaStream_t st);
+// out = 4 (a + c) - 6 b - d (cubic extrapolation of the last four adjoints)
+void launch_extrapolate4(int n3, const double* a, const double* b, const double* c, const double* d, double* out,
+                         cudaStream_t st);
 // r = g_bar - w on free DoFs (0 on Dirichlet; w = (A - K_pd) mu_0 or null for mu_0 = 0), permuted right-hand
 // side for the first preconditioner apply.
 template <typename T>

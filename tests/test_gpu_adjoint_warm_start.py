@@ -1,6 +1,7 @@
 """Adjoint warm starts of the conjugate-gradient backward (alg_phd_bwd_warm_start): 0 starts every solve from
 zero, 1 from the previous backward call's adjoint (the next time step of a reverse sweep), 2 from the linear
-extrapolation 2 mu_1 - mu_2 of the last two, 3 from the quadratic extrapolation 3 (mu_1 - mu_2) + mu_3.  The stop rule is unchanged, so a reverse sweep must give the same
+extrapolation 2 mu_1 - mu_2 of the last two, 3 from the quadratic extrapolation 3 (mu_1 - mu_2) + mu_3, 4 from
+the cubic 4 (mu_1 + mu_3) - 6 mu_2 - mu_4.  The stop rule is unchanged, so a reverse sweep must give the same
 gradients in all three modes up to the solver tolerance, with fewer conjugate-gradient iterations."""
 import numpy as np
 import pytest
@@ -48,7 +49,7 @@ def test_adjoint_warm_starts_agree_and_save_iterations(fp32):
     # 12-step sweep, measured on a B200 -- the size of the mixed adjoint's own error against FP64.
     tol = 5e-5 if fp32 else 1e-6
     ref = _sweep(d, sc, qs, opts, 0, dev)
-    for ws in (1, 2, 3):
+    for ws in (1, 2, 3, 4):
         out = _sweep(d, sc, qs, opts, ws, dev)
         for a, b in zip(out[:2], ref[:2]):
             err = np.abs(a - b).max() / np.abs(b).max()
