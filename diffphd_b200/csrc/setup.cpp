@@ -375,13 +375,9 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
     S.vals.assign(S.row_ptr[n], 0.0);
     S.Dinv_sqrt.resize(n);
     for (int i = 0; i < n; ++i) S.Dinv_sqrt[i] = 1.0 / std::sqrt(D[i]);
-    // level schedule by etree height (children strictly below parents)
-    std::vector<int> height(n, 0);
-    for (int j = 0; j < n; ++j)
-        if (S.parent[j] != -1) height[S.parent[j]] = std::max(height[S.parent[j]], height[j] + 1);
-    const int H = n ? *std::max_element(height.begin(), height.end()) + 1 : 0;
-    std::vector<std::vector<int>> levels(H);
-    for (int j = 0; j < n; ++j) levels[height[j]].push_back(j);
+    // Column c of L^-1 depends only on column c of the rows above it, so the recurrence runs over independent
+    // column blocks in parallel; inside a block the rows go in increasing order (every row k < i that row i
+    // needs is done by then).  Each entry is summed in the same order as a row-at-a-time sweep would.
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #endif
@@ -398,23 +394,13 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
             for (int c = a; c < b; ++c) out[c] -= l * rk[c];
         }
     };
-    for (int h = 0; h < H; ++h) {
-        const std::vector<int>& lev = levels[h];
-        if ((int)lev.size() >= 16) {
-#pragma omp parallel for schedule(dynamic, 4)
-            for (size_t t = 0; t < lev.size(); ++t) row_span(lev[t], S.lo[lev[t]], lev[t] + 1);
-        } else {
-            for (int i : lev) {
-                const int len = i - S.lo[i] + 1;
-                const int chunk = 4096;
-                const int nchunk = (len + chunk - 1) / chunk;
-#pragma omp parallel for schedule(dynamic, 1) if (nchunk > 1)
-                for (int c = 0; c < nchunk; ++c) {
-                    const int c0 = S.lo[i] + c * chunk;
-                    row_span(i, c0, std::min(i + 1, c0 + chunk));
-                }
-            }
-        }
+    constexpr int kColBlock = 64;
+    const int nblk = (n + kColBlock - 1) / kColBlock;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int c0 = blk * kColBlock, c1 = std::min(n, c0 + kColBlock);
+        for (int i = c0; i < n; ++i)
+            if (S.lo[i] < c1) row_span(i, std::max(c0, S.lo[i]), std::min(c1, i + 1));
     }
     // scale rows by D^-1/2
 #pragma omp parallel for schedule(static)
