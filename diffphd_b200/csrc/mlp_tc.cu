@@ -7,7 +7,7 @@
 //   layer 2: D2[128 x 128] = gelu(D1 + b1) W2^T       8 MMAs
 //   layer 3: D3[128 x 16]  = gelu(D2 + b2) W3^T       8 MMAs (N = 16: outputs 0..7 used, 8..15 zero rows)
 // Between layers each thread reads its row of the accumulator (tcgen05.ld 32x32b), adds the bias, applies
-// GELU, rounds to BF16 and writes the row into the next layer's A tile; one elected thread of warp 0 issues the
+// GELU, rounds to BF16 and writes the row into the next layer's A tile; thread 0 issues the
 // MMAs and commits them to an mbarrier that every thread waits on (bounded).  The weights are staged into
 // shared memory once per CTA; CTAs loop over tiles.
 //
