@@ -8,6 +8,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -38,18 +39,22 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
         return LIB
     common = ["-O3", "-std=c++17", "-lineinfo", "-ccbin", _host_cxx(), "-Xcompiler", "-fPIC,-fopenmp,-O3",
               "-I", str(PKG.parent / "include")] + ARCH
-    objs = []
-    for src in SOURCES:
+    def compile_one(src):
         obj = BUILD / (src + ".o")
         cmd = [nvcc, "-c", str(CSRC / src), "-o", str(obj)] + common
         if verbose_ptxas and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
-        res = subprocess.run(cmd, capture_output=True, text=True)
-        if res.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {src}:\n{res.stdout}\n{res.stderr}")
-        if verbose_ptxas and res.stderr:
-            sys.stderr.write(res.stderr)
-        objs.append(str(obj))
+        return src, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    objs = []
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        for src, obj, res in ex.map(compile_one, SOURCES):
+            if res.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {src}:\n{res.stdout}\n{res.stderr}")
+            if verbose_ptxas and res.stderr:
+                sys.stderr.write(f"--- {src}\n" + res.stderr)
+            objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, "-shared", "-o", str(tmp)] + objs + ARCH + ["-ccbin", _host_cxx(), "-Xcompiler", "-fopenmp",
                                                              "-lgomp", "-cudart", "static"]

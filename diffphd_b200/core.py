@@ -75,6 +75,7 @@ def load_library():
     L.dphd_reset_warm_start.argtypes = [C.c_void_p]
     L.dphd_kernel_launches.argtypes = [C.c_void_p]
     L.dphd_kernel_launches.restype = C.c_longlong
+    L.dphd_device.argtypes = [C.c_void_p]
     L.dphd_s_padded_values.argtypes = [C.c_void_p]
     L.dphd_s_padded_values.restype = C.c_longlong
     L.dphd_debug_time_ainv.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, _dp]
@@ -331,6 +332,10 @@ class Deformable:
 
     def reset_warm_start(self):
         self._check(self._L.dphd_reset_warm_start(self._h))
+
+    def device(self):
+        """CUDA device holding this deformable's GPU state (-1 before the first call that builds it)."""
+        return int(self._L.dphd_device(self._h))
 
     def kernel_launches(self):
         return int(self._L.dphd_kernel_launches(self._h))

@@ -377,6 +377,8 @@ int dphd_reset_warm_start(dphd_deformable* h) {
     return guard([&] { E(h).reset_warm_start(); });
 }
 
+int dphd_device(const dphd_deformable* h) { return h && h->eng ? h->eng->device() : -2; }
+
 long long dphd_kernel_launches(const dphd_deformable* h) { return h && h->eng ? h->eng->kernel_launches() : -1; }
 
 int dphd_debug_time_ainv(dphd_deformable* h, double dt, int reps, int fp32, int flush_l2, double* ms_per_apply) {

@@ -209,9 +209,19 @@ long long Engine::s_memory_bytes() const {
            d_row_len.bytes + d_tile_ptr.bytes + d_tile_rows.bytes;
 }
 
+void Engine::check_device() const {
+    if (device_ < 0) return;
+    int cur = -1;
+    CUDA_OK(cudaGetDevice(&cur));
+    DPHD_CHECK(cur == device_, "this deformable's GPU state lives on device " + std::to_string(device_) +
+                                   " but device " + std::to_string(cur) +
+                                   " is current; make its device current (cudaSetDevice) before the call");
+}
+
 void Engine::ensure_built(double dt, int threads) {
     DPHD_CHECK(M.n > 0, "Deformable is not initialized.");
     DPHD_CHECK(!M.energies.empty(), "No PD energy was added.");
+    check_device();
     if (built_ && built_dt_ == dt) {
         if (!device_ready_) build_device(threads);
         return;
@@ -234,6 +244,7 @@ void Engine::ensure_built(double dt, int threads) {
 
 void Engine::build_device(int threads) {
     (void)threads;
+    if (device_ < 0) CUDA_OK(cudaGetDevice(&device_));
     if (!stream_) CUDA_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     if (!h_ctrl_) CUDA_OK(cudaMallocHost(&h_ctrl_, sizeof(Ctrl)));
     const int n = M.n, m = M.m, k = M.k;
@@ -1615,6 +1626,7 @@ void Engine::ainv_noalloc(double dt, const double* d_b, double* d_x, bool fp32, 
                "dphd_ainv_noalloc: the factor for this dt is not on the device yet; make one allocating call "
                "first (dphd_forward, dphd_forward_device or dphd_debug_ainv with the same dt)");
     DPHD_CHECK(d_b && d_x, "null device pointer");
+    check_device();  // the factor and the scratch address used below must belong to the same device
     dphd::ainv_noalloc(plan64_, plan32_, d_fixed_node.as<unsigned char>(), d_b, d_x, fp32, st);
     launches_ += 5;
 }

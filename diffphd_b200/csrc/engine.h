@@ -137,6 +137,9 @@ public:
     // time `reps` applications of the S^T S pair on the device; returns ms per application
     double time_ainv(double dt, int reps, bool fp32, bool flush_l2);
     long long kernel_launches() const { return launches_; }
+    // CUDA device that holds this handle's GPU state (-1 until the first call that builds it); every later
+    // call must be made with that device current
+    int device() const { return device_; }
 
     // contact state: normal multipliers of the planar candidates (the frame-to-frame warm start)
     void reset_warm_start();
@@ -185,6 +188,8 @@ private:
     void run_iterations(int mode, const Options& o, cudaStream_t st);
     void drop_graphs();
     void check_status(const char* where);
+    void check_device() const;
+    int device_ = -1;
 
     bool built_ = false;
     double built_dt_ = -1;

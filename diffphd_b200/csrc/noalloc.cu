@@ -11,7 +11,10 @@
 // zeroes what must start at zero (its control block) and overwrites the rest before reading it.  Calls that
 // overlap on the GPU (two streams, or two host threads) race on the array and must be serialised by the
 // caller.  The first call on a device looks the array's device address up (cudaGetSymbolAddress, with that
-// device current) and caches it; make that first call before any stream capture.
+// device current) and caches it; make that first call before any stream capture.  The cached address belongs
+// to the device's primary context as it was then: after a cudaDeviceReset in the same process the module is
+// loaded again and the cached address is stale, so this entry point is not for use across a device reset.
+// The handle's device must be current (the engine checks it before the lookup).
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -378,9 +378,8 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
     // Column c of L^-1 depends only on column c of the rows above it, so the recurrence runs over independent
     // column blocks in parallel; inside a block the rows go in increasing order (every row k < i that row i
     // needs is done by then).  Each entry is summed in the same order as a row-at-a-time sweep would.
-#ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#endif
+    // the thread count goes to these two loops only (num_threads clauses), not to the process-wide default
+    const int nthr = threads > 0 ? threads : 0;
     auto row_span = [&](int i, int c0, int c1) {
         // accumulate columns [c0, c1) of row i
         double* out = &S.vals[S.row_ptr[i]] - S.lo[i];
@@ -396,14 +395,14 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
     };
     constexpr int kColBlock = 64;
     const int nblk = (n + kColBlock - 1) / kColBlock;
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr > 0 ? nthr : omp_get_max_threads())
     for (int blk = 0; blk < nblk; ++blk) {
         const int c0 = blk * kColBlock, c1 = std::min(n, c0 + kColBlock);
         for (int i = c0; i < n; ++i)
             if (S.lo[i] < c1) row_span(i, std::max(c0, S.lo[i]), std::min(c1, i + 1));
     }
     // scale rows by D^-1/2
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(nthr > 0 ? nthr : omp_get_max_threads())
     for (int i = 0; i < n; ++i) {
         double* r = &S.vals[S.row_ptr[i]];
         const int64_t len = S.row_ptr[i + 1] - S.row_ptr[i];

@@ -102,6 +102,11 @@ int dphd_reset_warm_start(dphd_deformable* h);
 
 /* Number of kernels this library launched on the GPU since the handle was created (graph nodes included). */
 long long dphd_kernel_launches(const dphd_deformable* h);
+/* CUDA device that holds this handle's GPU state: -1 until the first call that builds the factor (it records
+ * the device current then), -2 for a null handle.  Later calls made while another device is current fail with
+ * an error instead of mixing pointers of two devices.  No counterpart in the reference (fixed to device 0,
+ * forward_gpu.cpp:579). */
+int dphd_device(const dphd_deformable* h);
 
 /* Per-frame statistics (AlgPhdFrameIters / AlgPhdFrameConverged / AlgPhdResetFrameStats,
  * cpp/core/include/fem/alg_phd_gpu_memory.h:25-27; forward_gpu.cpp:324-332). */
@@ -140,7 +145,8 @@ int dphd_debug_set_pdl(dphd_deformable* h, int on);
  * Requires the factor for this dt to be on the device already (one earlier allocating call on the handle);
  * fails with a clear error when the mesh needs more scratch than the array holds.  All calls share the
  * array: calls that overlap on the GPU race and must be serialised by the caller.  The first call on a
- * device looks up the array's address; make it before any stream capture. */
+ * device looks up the array's address; make it before any stream capture.  That cached address is not valid
+ * across a cudaDeviceReset in the same process.  The handle's device (dphd_device) must be current. */
 int dphd_ainv_noalloc(dphd_deformable* h, double dt, const double* d_b, double* d_x, int fp32, void* stream);
 
 /* Contact candidates of the frictional boundary (0 without one; -1 before the first forward call builds them)

@@ -17,6 +17,13 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, s), f"missing export {s}"
 
 
+def test_device_is_recorded_only_once_built():
+    sc = scenes.cantilever(cells=(2, 1, 1), steps=1)
+    d = core.from_scene(sc)
+    assert d.device() == -1  # nothing built yet: no device bound to the handle
+    assert core.load_library().dphd_device(None) == -2
+
+
 def test_bad_element_dim_reports_error():
     L = core.load_library()
     h = C.c_void_p()
