@@ -135,115 +135,326 @@ __global__ void __launch_bounds__(256) k_ncp_ainvb(ContactDev c, const T* __rest
     }
 }
 
-// Dense solve of the active NCP system, multiplier updates and the contact right-hand side (one CTA).
-// vcon: without r64, J^T f (zero elsewhere); with r64 (the FP64 residual of the refinement form), the S-pass
-// input itself, overwritten at the candidates with r + J^T f formed in FP64 (no FP32 cancellation of the two).
+// ---- Dense solve of the active NCP system (multi-CTA, one cooperative launch per PD iteration) -------------
+//
+// M = Omega G Omega + E over the ka active candidates (ka <= K, known only on the device) is factored by a
+// blocked right-looking Cholesky in 64 x 64 tiles, and M dlambda = h - J A^-1 g solved, by every CTA of one
+// cooperative grid (all CTAs co-resident) with grid-wide barriers between the dependent phases:
+//   A  assemble M (lower triangle, padded to a multiple of 64 with identity rows) and the right-hand side;
+//   B  per block column kb: factor the 64 x 64 diagonal block (redundantly in every CTA that needs it) and
+//      solve its panel tiles; barrier; update the trailing lower tiles and the right-hand side; barrier;
+//   C  backward substitution by block rows, one barrier per block;
+//   D  clamp lambda to [0, 1e8]; barrier; Coulomb cone per active contact and the contact right-hand side.
+// The barrier is a counter + generation word with a bounded spin: a CTA that waits too long sets
+// kStatusBarrierTimeout and `done` in the control block and every later barrier returns at once, so the
+// kernel always ends (the host turns the status into an error).
+constexpr int kNcpTile = 64;
+constexpr int kNcpThreads = 256;
+constexpr int kNcpLd = kNcpTile + 1;  // padded smem row (doubles) for the row-major 64 x 64 tiles
+constexpr long long kBarrierSpins = 1ll << 24;
+
+// Returns false when the grid is aborting (a barrier timed out somewhere): the caller returns.
+__device__ __forceinline__ bool ncp_grid_sync(unsigned int* bar, Ctrl* ctrl) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* vbar = bar;
+        int ok = vbar[2] == 0u;
+        if (ok) {
+            const unsigned int gen = vbar[1];
+            __threadfence();
+            const unsigned int arrived = atomicAdd(bar, 1u);
+            if (arrived == gridDim.x - 1) {
+                vbar[0] = 0u;
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                long long spins = 0;
+                while (vbar[1] == gen) {
+                    if (vbar[2] != 0u || ++spins > kBarrierSpins) {
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                if (!ok && vbar[2] == 0u) {
+                    atomicExch(bar + 2, 1u);
+                    atomicOr(&ctrl->status, (int)kStatusBarrierTimeout);
+                    ctrl->done = 1;
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Cholesky of the 64 x 64 lower block sD (row-major, ld kNcpLd) in place, the reference's pivot guard
+// (sqrt(max(d, 1e-300))); all threads of the CTA take part.
+__device__ void ncp_tile_cholesky(double* sD) {
+    __shared__ double piv;
+    for (int j = 0; j < kNcpTile; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = sD[j * kNcpLd + j];
+            piv = sqrt(d > 1e-300 ? d : 1e-300);
+            sD[j * kNcpLd + j] = piv;
+        }
+        __syncthreads();
+        const double inv = 1.0 / piv;
+        for (int r = j + 1 + (int)threadIdx.x; r < kNcpTile; r += blockDim.x) sD[r * kNcpLd + j] *= inv;
+        __syncthreads();
+        const int rem = kNcpTile - j - 1;
+        for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
+            const int r = j + 1 + t / rem, l = j + 1 + t % rem;
+            if (l <= r) sD[r * kNcpLd + l] -= sD[r * kNcpLd + j] * sD[l * kNcpLd + j];
+        }
+        __syncthreads();
+    }
+}
+
 template <typename T>
-__global__ void __launch_bounds__(1024) k_ncp_solve(ContactDev c, const double* __restrict__ q0,
-                                                    const int* __restrict__ iperm, T* __restrict__ vcon, int npad,
-                                                    const double* __restrict__ r64, Ctrl* ctrl) {
-    if (ctrl->done) return;
+__global__ void __launch_bounds__(kNcpThreads, 1)
+k_ncp_block_solve(ContactDev c, const double* __restrict__ q0, const int* __restrict__ iperm, T* __restrict__ vcon,
+                  int npad, const double* __restrict__ r64, Ctrl* ctrl) {
+    extern __shared__ double smem[];
+    double* sA = smem;                           // 64 x kNcpLd: diagonal block / k-major panel i
+    double* sB = smem + kNcpTile * kNcpLd;       // 64 x kNcpLd: panel tile / k-major panel j
+    double* sy = smem + 2 * kNcpTile * kNcpLd;   // 64: the block's right-hand side / solution
+    if (ctrl->done) return;  // every CTA reads the same value: no CTA reaches a barrier the others skip
     const int K = c.K, ka = c.kact[0];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, G = gridDim.x, bid = blockIdx.x;
+    const int gt = bid * nt + tid, nthr = G * nt;
+    const int lane = tid & 31, gw = gt >> 5, nwarps = nthr >> 5;
     const double n0 = c.n[0], n1 = c.n[1], n2 = c.n[2];
     // clear the previous contact right-hand side at every candidate node
-    for (int k = tid; k < K; k += nt) {
+    for (int k = gt; k < K; k += nthr) {
         const int node = c.cand[k], j = iperm[node];
         vcon[j] = r64 ? (T)r64[3 * node] : T(0);
         vcon[npad + j] = r64 ? (T)r64[3 * node + 1] : T(0);
         vcon[2 * (size_t)npad + j] = r64 ? (T)r64[3 * node + 2] : T(0);
     }
     if (ka == 0) {
-        for (int k = tid; k < K; k += nt) c.lt1[k] = c.lt2[k] = 0.0;
+        for (int k = gt; k < K; k += nthr) c.lt1[k] = c.lt2[k] = 0.0;
         return;
     }
-    double* M = c.Mwork;      // ka x ka, row-major
-    double* rhs = c.rhs;      // ka
-    // A^-1 g at active nodes and the right-hand side h - J A^-1 g
-    for (int a = tid; a < ka; a += nt) {
+    const int nb = (ka + kNcpTile - 1) / kNcpTile, ld = nb * kNcpTile;
+    double* M = c.Mwork;  // ld x ld, row-major, lower triangle used
+    double* rhs = c.rhs;  // ld
+    // ---- A: M and the right-hand side h - J A^-1 g (one warp per row) ----
+    for (int a = gw; a < ld; a += nwarps) {
+        double* Ma = M + (size_t)a * ld;
+        if (a >= ka) {  // identity padding row
+            for (int b = lane; b <= a; b += 32) Ma[b] = (a == b) ? 1.0 : 0.0;
+            if (lane == 0) rhs[a] = 0.0;
+            continue;
+        }
         const int k = c.act[a];
-        double g0 = c.ainvb[3 * a], g1 = c.ainvb[3 * a + 1], g2 = c.ainvb[3 * a + 2];
-        for (int b = 0; b < ka; ++b) {
+        const double om = c.omega[k];
+        const double* Gk = c.G + (size_t)k * K;
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        for (int b = lane; b < ka; b += 32) {
             const int kb = c.act[b];
-            const double Gab = c.G[(size_t)k * K + kb];
+            const double Gab = Gk[kb];
             const double fn = c.omega[kb] * c.lam[kb];
             const double f1 = c.lt1[kb], f2 = c.lt2[kb];
             g0 += Gab * (fn * n0 + f1 * c.t1[0] + f2 * c.t2[0]);
             g1 += Gab * (fn * n1 + f1 * c.t1[1] + f2 * c.t2[1]);
             g2 += Gab * (fn * n2 + f1 * c.t1[2] + f2 * c.t2[2]);
+            if (b <= a) Ma[b] = om * Gab * c.omega[kb] + (a == b ? c.Ediag[k] : 0.0);
         }
-        rhs[a] = c.hvec[k] - c.omega[k] * (n0 * g0 + n1 * g1 + n2 * g2);
-        for (int b = 0; b < ka; ++b) {
-            const int kb = c.act[b];
-            M[(size_t)a * ka + b] = c.omega[k] * c.G[(size_t)k * K + kb] * c.omega[kb] + (a == b ? c.Ediag[k] : 0.0);
+        g0 = warp_sum_d(g0);
+        g1 = warp_sum_d(g1);
+        g2 = warp_sum_d(g2);
+        if (lane == 0) {
+            g0 += c.ainvb[3 * a];
+            g1 += c.ainvb[3 * a + 1];
+            g2 += c.ainvb[3 * a + 2];
+            rhs[a] = c.hvec[k] - om * (n0 * g0 + n1 * g1 + n2 * g2);
         }
     }
-    __syncthreads();
-    // Cholesky M = L L^T in place (lower triangle), right-looking
-    for (int j = 0; j < ka; ++j) {
-        __shared__ double piv;
-        if (tid == 0) {
-            double d = M[(size_t)j * ka + j];
-            piv = sqrt(d > 1e-300 ? d : 1e-300);
-            M[(size_t)j * ka + j] = piv;
+    if (!ncp_grid_sync(c.bar, ctrl)) return;
+    // ---- B: blocked factorisation with the forward substitution folded in ----
+    for (int kb = 0; kb < nb; ++kb) {
+        const int below = nb - kb - 1;
+        if (bid == 0 || bid < below) {
+            const double* Dg = M + (size_t)kb * kNcpTile * ld + kb * kNcpTile;
+            for (int t = tid; t < kNcpTile * kNcpTile; t += nt) {
+                const int r = t / kNcpTile, l = t % kNcpTile;
+                if (l <= r) sA[r * kNcpLd + l] = Dg[(size_t)r * ld + l];
+            }
+            if (bid == 0 && tid < kNcpTile) sy[tid] = rhs[kb * kNcpTile + tid];
+            __syncthreads();
+            ncp_tile_cholesky(sA);
+            if (bid == 0) {  // y_kb = L_kk^-1 rhs_kb (one warp, column-oriented); L_kk goes back after the barrier
+                if (tid < 32) {
+                    for (int j = 0; j < kNcpTile; ++j) {
+                        double yj = 0.0;
+                        if (lane == 0) sy[j] /= sA[j * kNcpLd + j];
+                        __syncwarp();
+                        yj = sy[j];
+                        for (int r = j + 1 + lane; r < kNcpTile; r += 32) sy[r] -= sA[r * kNcpLd + j] * yj;
+                        __syncwarp();
+                    }
+                }
+                __syncthreads();
+                if (tid < kNcpTile) rhs[kb * kNcpTile + tid] = sy[tid];  // no other CTA reads rhs_kb in this phase
+            }
+            // panel tiles L[i, kb] = M[i, kb] L_kk^-T
+            for (int i = kb + 1 + bid; i < nb; i += G) {
+                double* Pg = M + (size_t)i * kNcpTile * ld + kb * kNcpTile;
+                __syncthreads();
+                for (int t = tid; t < kNcpTile * kNcpTile; t += nt) {
+                    const int r = t / kNcpTile, l = t % kNcpTile;
+                    sB[r * kNcpLd + l] = Pg[(size_t)r * ld + l];
+                }
+                __syncthreads();
+                if (tid < kNcpTile) {
+                    double* row = sB + tid * kNcpLd;
+                    for (int j = 0; j < kNcpTile; ++j) {
+                        double x = row[j];
+                        const double* Lj = sA + j * kNcpLd;
+                        for (int l = 0; l < j; ++l) x -= row[l] * Lj[l];
+                        row[j] = x / Lj[j];
+                    }
+                }
+                __syncthreads();
+                for (int t = tid; t < kNcpTile * kNcpTile; t += nt) {
+                    const int r = t / kNcpTile, l = t % kNcpTile;
+                    Pg[(size_t)r * ld + l] = sB[r * kNcpLd + l];
+                }
+            }
         }
-        __syncthreads();
-        for (int i = j + 1 + tid; i < ka; i += nt) M[(size_t)i * ka + j] /= piv;
-        __syncthreads();
-        const int rem = ka - j - 1;
-        for (long long t = tid; t < (long long)rem * rem; t += nt) {
-            const int i = j + 1 + (int)(t / rem), l = j + 1 + (int)(t % rem);
-            if (l <= i) M[(size_t)i * ka + l] -= M[(size_t)i * ka + j] * M[(size_t)l * ka + j];
+        if (!ncp_grid_sync(c.bar, ctrl)) return;
+        // every CTA has now read M[kb][kb]: CTA 0 stores L_kk (still in its sA) in its place
+        if (bid == 0) {
+            double* Dw = M + (size_t)kb * kNcpTile * ld + kb * kNcpTile;
+            for (int t = tid; t < kNcpTile * kNcpTile; t += nt) {
+                const int r = t / kNcpTile, l = t % kNcpTile;
+                if (l <= r) Dw[(size_t)r * ld + l] = sA[r * kNcpLd + l];
+            }
         }
-        __syncthreads();
+        // trailing update M[i][j] -= L[i,kb] L[j,kb]^T for kb < j <= i, and rhs_i -= L[i,kb] y_kb
+        const int ntri = below * (below + 1) / 2;
+        const int ty = tid >> 4, tx = tid & 15;
+        for (int w = bid; w < ntri + below; w += G) {
+            __syncthreads();
+            if (w < ntri) {
+                int ii = (int)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);
+                while ((ii + 1) * (ii + 2) / 2 <= w) ++ii;
+                while (ii * (ii + 1) / 2 > w) --ii;
+                const int jj = w - ii * (ii + 1) / 2;
+                const int i = kb + 1 + ii, j = kb + 1 + jj;
+                const double* Pi = M + (size_t)i * kNcpTile * ld + kb * kNcpTile;
+                const double* Pj = M + (size_t)j * kNcpTile * ld + kb * kNcpTile;
+                // k-major copies: sA[k][r] = L[i*64 + r, kb*64 + k]
+                for (int t = tid; t < kNcpTile * kNcpTile; t += nt) {
+                    const int r = t / kNcpTile, k = t % kNcpTile;
+                    sA[k * kNcpLd + r] = Pi[(size_t)r * ld + k];
+                    sB[k * kNcpLd + r] = Pj[(size_t)r * ld + k];
+                }
+                __syncthreads();
+                double acc[4][4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+#pragma unroll 4
+                for (int k = 0; k < kNcpTile; ++k) {
+                    double av[4], bv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) av[u] = sA[k * kNcpLd + ty * 4 + u];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) bv[v] = sB[k * kNcpLd + tx * 4 + v];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) acc[u][v] += av[u] * bv[v];
+                }
+                double* Cg = M + (size_t)i * kNcpTile * ld + j * kNcpTile;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) Cg[(size_t)(ty * 4 + u) * ld + tx * 4 + v] -= acc[u][v];
+            } else {
+                const int i = kb + 1 + (w - ntri);
+                if (tid < kNcpTile) {
+                    const double* Li = M + (size_t)(i * kNcpTile + tid) * ld + kb * kNcpTile;
+                    const double* y = rhs + kb * kNcpTile;
+                    double s = 0.0;
+                    for (int k = 0; k < kNcpTile; ++k) s += Li[k] * y[k];
+                    rhs[i * kNcpTile + tid] -= s;
+                }
+            }
+        }
+        if (!ncp_grid_sync(c.bar, ctrl)) return;
     }
-    // forward / backward substitution, column-oriented so that each step is parallel over the rows
-    for (int k = 0; k < ka; ++k) {
-        if (tid == 0) rhs[k] /= M[(size_t)k * ka + k];
-        __syncthreads();
-        const double rk = rhs[k];
-        for (int i = k + 1 + tid; i < ka; i += nt) rhs[i] -= M[(size_t)i * ka + k] * rk;
-        __syncthreads();
+    // ---- C: backward substitution L^T x = y by block rows ----
+    for (int kb = nb - 1; kb >= 0; --kb) {
+        if (bid == 0 || bid < kb) {
+            const double* Dg = M + (size_t)kb * kNcpTile * ld + kb * kNcpTile;
+            __syncthreads();
+            for (int t = tid; t < kNcpTile * kNcpTile; t += nt) {
+                const int r = t / kNcpTile, l = t % kNcpTile;
+                if (l <= r) sA[r * kNcpLd + l] = Dg[(size_t)r * ld + l];
+            }
+            if (tid < kNcpTile) sy[tid] = rhs[kb * kNcpTile + tid];
+            __syncthreads();
+            if (tid < 32) {
+                for (int j = kNcpTile - 1; j >= 0; --j) {
+                    if (lane == 0) sy[j] /= sA[j * kNcpLd + j];
+                    __syncwarp();
+                    const double xj = sy[j];
+                    for (int l = lane; l < j; l += 32) sy[l] -= sA[j * kNcpLd + l] * xj;
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            if (bid == 0 && tid < kNcpTile) c.xsol[kb * kNcpTile + tid] = sy[tid];
+            // rhs_p -= L[kb, p]^T x_kb for the block rows p < kb (rhs_kb itself is only read in this phase)
+            for (int p = bid; p < kb; p += G) {
+                if (tid < kNcpTile) {
+                    const double* Lkp = M + (size_t)kb * kNcpTile * ld + p * kNcpTile + tid;
+                    double s = 0.0;
+                    for (int i = 0; i < kNcpTile; ++i) s += Lkp[(size_t)i * ld] * sy[i];
+                    rhs[p * kNcpTile + tid] -= s;
+                }
+            }
+        }
+        if (!ncp_grid_sync(c.bar, ctrl)) return;
     }
-    for (int i = ka - 1; i >= 0; --i) {
-        if (tid == 0) rhs[i] /= M[(size_t)i * ka + i];
-        __syncthreads();
-        const double ri = rhs[i];
-        for (int k = tid; k < i; k += nt) rhs[k] -= M[(size_t)i * ka + k] * ri;
-        __syncthreads();
-    }
-    for (int a = tid; a < ka; a += nt) {
+    // ---- D: multipliers, Coulomb cone (forward_gpu.cpp:1255-1302), contact right-hand side ----
+    for (int a = gt; a < ka; a += nthr) {
         const int k = c.act[a];
-        double l = c.lam[k] + rhs[a];
+        double l = c.lam[k] + c.xsol[a];
         l = l < 0.0 ? 0.0 : (l > 1e8 ? 1e8 : l);
         c.lam[k] = l;
     }
-    __syncthreads();
-    // Coulomb cone (forward_gpu.cpp:1255-1302); non-active candidates have lambda = 0 and no friction
-    for (int k = tid; k < K; k += nt) c.ltmp[k] = 0.0;
-    __syncthreads();
-    for (int a = tid; a < ka; a += nt) {
+    for (int k = gt; k < K; k += nthr) c.lt1[k] = c.lt2[k] = 0.0;  // non-active candidates carry no friction
+    if (!ncp_grid_sync(c.bar, ctrl)) return;
+    for (int a = gw; a < ka; a += nwarps) {
         const int k = c.act[a];
         double t1v = 0.0, t2v = 0.0;
         if (c.mu > 0.0 && c.lam[k] > 0.0) {
-            const int node = c.cand[k];
-            double qn0 = c.ainvb[3 * a], qn1 = c.ainvb[3 * a + 1], qn2 = c.ainvb[3 * a + 2];
-            for (int b = 0; b < ka; ++b) {
+            const double* Gk = c.G + (size_t)k * K;
+            double f = 0.0;
+            for (int b = lane; b < ka; b += 32) {
                 const int kb = c.act[b];
-                const double f = c.omega[kb] * c.lam[kb] * c.G[(size_t)k * K + kb];
-                qn0 += f * n0;
-                qn1 += f * n1;
-                qn2 += f * n2;
+                f += c.omega[kb] * c.lam[kb] * Gk[kb];
             }
+            f = warp_sum_d(f);
+            const int node = c.cand[k];
+            const double qn0 = c.ainvb[3 * a] + f * n0, qn1 = c.ainvb[3 * a + 1] + f * n1,
+                         qn2 = c.ainvb[3 * a + 2] + f * n2;
             const double s0 = qn0 - q0[3 * node], s1 = qn1 - q0[3 * node + 1], s2 = qn2 - q0[3 * node + 2];
             const double sn = s0 * n0 + s1 * n1 + s2 * n2;
             const double u0 = s0 - sn * n0, u1 = s1 - sn * n1, u2 = s2 - sn * n2;
             const double ut1 = u0 * c.t1[0] + u1 * c.t1[1] + u2 * c.t1[2];
             const double ut2 = u0 * c.t2[0] + u1 * c.t2[1] + u2 * c.t2[2];
-            const double Gkk = c.G[(size_t)k * K + k];
-            const double det = Gkk * Gkk;
+            const double Gkk = Gk[k];
             double st1 = 0.0, st2 = 0.0;
-            if (fabs(det) > 1e-20) {
+            if (fabs(Gkk * Gkk) > 1e-20) {
                 st1 = -ut1 / Gkk;
                 st2 = -ut2 / Gkk;
             }
@@ -259,25 +470,18 @@ __global__ void __launch_bounds__(1024) k_ncp_solve(ContactDev c, const double* 
                 }
             }
         }
-        c.ltmp[k] = t1v;
-        c.ltmp[K + k] = t2v;
-    }
-    __syncthreads();
-    for (int k = tid; k < K; k += nt) {
-        c.lt1[k] = c.ltmp[k];
-        c.lt2[k] = c.ltmp[K + k];
-    }
-    __syncthreads();
-    // contact right-hand side J^T f at the active nodes (omega from this iteration times the new lambda)
-    for (int a = tid; a < ka; a += nt) {
-        const int k = c.act[a];
-        const double fn = c.omega[k] * c.lam[k];
-        const int node = c.cand[k], j = iperm[node];
-        const double r0 = r64 ? r64[3 * node] : 0.0, r1 = r64 ? r64[3 * node + 1] : 0.0,
-                     r2 = r64 ? r64[3 * node + 2] : 0.0;
-        vcon[j] = (T)(r0 + fn * n0 + c.lt1[k] * c.t1[0] + c.lt2[k] * c.t2[0]);
-        vcon[npad + j] = (T)(r1 + fn * n1 + c.lt1[k] * c.t1[1] + c.lt2[k] * c.t2[1]);
-        vcon[2 * (size_t)npad + j] = (T)(r2 + fn * n2 + c.lt1[k] * c.t1[2] + c.lt2[k] * c.t2[2]);
+        if (lane == 0) {
+            c.lt1[k] = t1v;
+            c.lt2[k] = t2v;
+            // contact right-hand side J^T f at the node (omega from this iteration times the new lambda)
+            const double fn = c.omega[k] * c.lam[k];
+            const int node = c.cand[k], j = iperm[node];
+            const double r0 = r64 ? r64[3 * node] : 0.0, r1 = r64 ? r64[3 * node + 1] : 0.0,
+                         r2 = r64 ? r64[3 * node + 2] : 0.0;
+            vcon[j] = (T)(r0 + fn * n0 + t1v * c.t1[0] + t2v * c.t2[0]);
+            vcon[npad + j] = (T)(r1 + fn * n1 + t1v * c.t1[1] + t2v * c.t2[1]);
+            vcon[2 * (size_t)npad + j] = (T)(r2 + fn * n2 + t1v * c.t1[2] + t2v * c.t2[2]);
+        }
     }
 }
 
@@ -301,6 +505,17 @@ __global__ void k_restitution(ContactDev c, double* __restrict__ q, const double
 
 }  // namespace
 
+int ncp_grid() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 148;
+}
+
+size_t ncp_matrix_capacity(int K) {
+    const size_t kp = ((size_t)K + kNcpTile - 1) / kNcpTile * kNcpTile;
+    return kp;
+}
+
 void launch_delassus(int K, const int64_t* off, const int* prow, const double* pval, double* G, cudaStream_t st) {
     const long long npairs = (long long)K * (K + 1) / 2;
     const long long blocks = (npairs * 32 + 255) / 256;
@@ -313,7 +528,25 @@ void launch_ncp_iteration(const ContactDev& c, const double* x, const T* y, int 
                           cudaStream_t st) {
     k_ncp_prepare<<<1, 1024, 0, st>>>(c, x, ctrl);
     k_ncp_ainvb<T><<<(c.K * 32 + 255) / 256, 256, 0, st>>>(c, y, npad, x_base, ctrl);
-    k_ncp_solve<T><<<1, 1024, 0, st>>>(c, q0, iperm, vcon, npad, r64, ctrl);
+    // one cooperative grid of one CTA per SM (the barrier needs every CTA resident)
+    const size_t smem = (size_t)(2 * kNcpTile * kNcpLd + kNcpTile) * sizeof(double);
+    static bool attr_set[2] = {false, false};
+    void (*kern)(ContactDev, const double*, const int*, T*, int, const double*, Ctrl*) = k_ncp_block_solve<T>;
+    if (!attr_set[sizeof(T) == 8]) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set[sizeof(T) == 8] = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ncp_grid());
+    cfg.blockDim = dim3(kNcpThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, c, q0, iperm, vcon, npad, r64, ctrl);
 }
 template void launch_ncp_iteration<double>(const ContactDev&, const double*, const double*, int, const double*,
                                            const double*, const int*, double*, const double*, Ctrl*, cudaStream_t);

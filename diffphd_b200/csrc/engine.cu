@@ -630,16 +630,22 @@ void Engine::build_contact(double dt) {
                          cudaMemcpyDeviceToHost));
     for (int k = 0; k < K; ++k) rp[k] = std::max(dt * dt * gdiag[k], 1e-10);
     dc_rprec.upload(rp);
-    for (DeviceBuffer* b : {&dc_lam, &dc_lt1, &dc_lt2, &dc_omega, &dc_E, &dc_h, &dc_rhs}) {
+    for (DeviceBuffer* b : {&dc_lam, &dc_lt1, &dc_lt2, &dc_omega, &dc_E, &dc_h}) {
         b->alloc((size_t)K * sizeof(double));
         CUDA_OK(cudaMemset(b->p, 0, b->bytes));
     }
-    dc_ltmp.alloc((size_t)2 * K * sizeof(double));
+    const size_t kcap = ncp_matrix_capacity(K);
+    for (DeviceBuffer* b : {&dc_rhs, &dc_xsol}) {
+        b->alloc(kcap * sizeof(double));
+        CUDA_OK(cudaMemset(b->p, 0, b->bytes));
+    }
+    dc_bar.alloc(4 * sizeof(unsigned int));
+    CUDA_OK(cudaMemset(dc_bar.p, 0, dc_bar.bytes));
     dc_act.alloc((size_t)K * sizeof(int));
     dc_kact.alloc(sizeof(int));
     CUDA_OK(cudaMemset(dc_kact.p, 0, sizeof(int)));
     dc_ainvb.alloc((size_t)3 * K * sizeof(double));
-    dc_M.alloc((size_t)K * K * sizeof(double));
+    dc_M.alloc(kcap * kcap * sizeof(double));
     c.cand = dc_cand.as<int>();
     c.off = dc_off.as<int64_t>();
     c.prow = dc_prow.as<int>();
@@ -657,7 +663,8 @@ void Engine::build_contact(double dt) {
     c.ainvb = dc_ainvb.as<double>();
     c.rhs = dc_rhs.as<double>();
     c.Mwork = dc_M.as<double>();
-    c.ltmp = dc_ltmp.as<double>();
+    c.xsol = dc_xsol.as<double>();
+    c.bar = dc_bar.as<unsigned int>();
 }
 
 void Engine::reset_warm_start() {
@@ -993,7 +1000,10 @@ static void init_ctrl(Ctrl* h, int mode, const Options& o, int max_iter, double 
 
 void Engine::check_status(const char* where) {
     if (h_ctrl_->status & kStatusSingularF) throw Error("Singular F.");
-    (void)where;
+    if (h_ctrl_->status & kStatusBarrierTimeout)
+        throw Error(std::string(where) + ": the contact solve's grid barrier timed out (CTAs not co-resident)");
+    if (h_ctrl_->status & kStatusNonFinite)
+        throw Error(std::string(where) + ": non-finite PD iterate (NaN or Inf in q, v, f_ext or the solve)");
 }
 
 void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st,
@@ -1019,6 +1029,7 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
                     graphs_[md] = nullptr;
                 }
         graph_mu_ = o.friction_mu;
+        CUDA_OK(cudaMemsetAsync(dc_bar.p, 0, dc_bar.bytes, st));  // clears an abort left by an earlier solve
         run_iterations(o.fp32_bulk ? 8 : 5, o, st);
     } else {
         run_iterations(o.fp32_bulk ? 1 : 0, o, st);

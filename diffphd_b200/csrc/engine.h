@@ -242,7 +242,7 @@ private:
     DeviceBuffer d_ws_err;       // set by the tcgen05 inference kernel when a tensor-core wait gave up
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
-        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_M, dc_ltmp, d_vcon, d_r64, d_q0;
+        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

@@ -19,6 +19,7 @@ enum StatusBits : int {
     kStatusNonFinite = 2,        // NaN/Inf in an iterate
     kStatusDiverged = 4,         // adjoint iterate exceeded the clip norm
     kStatusIndefinite = 8,       // conjugate-gradient curvature p^T (A - K) p <= 0
+    kStatusBarrierTimeout = 16,  // a grid-wide barrier of a cooperative kernel gave up waiting
 };
 
 // Device-resident control block of one fixed-point solve (forward PD loop or backbone adjoint).
@@ -222,10 +223,14 @@ struct ContactDev {
     int* act = nullptr;              // ordered active candidate list
     int* kact = nullptr;             // its length
     double* ainvb = nullptr;         // 3 per active candidate
-    double* rhs = nullptr;
-    double* Mwork = nullptr;         // active system, K x K capacity
-    double* ltmp = nullptr;          // 2K
+    double* rhs = nullptr;           // kcap: right-hand side, then the forward-substituted y
+    double* xsol = nullptr;          // kcap: the solution dlambda of the active system
+    double* Mwork = nullptr;         // active system, kcap x kcap capacity (kcap = K rounded up to 64)
+    unsigned int* bar = nullptr;     // grid barrier of the NCP solve: count, generation, abort
 };
+// Side of the padded active-system capacity for K candidates (K rounded up to the 64 x 64 tile).
+size_t ncp_matrix_capacity(int K);
+int ncp_grid();
 void launch_delassus(int K, const int64_t* off, const int* prow, const double* pval, double* G, cudaStream_t st);
 // One NCP iteration: y (T) holds S r for the iteration's right-hand side (S b in FP64; S (b - A x) in the
 // FP32 refinement form, where x_base = x adds the current iterate back).  vcon (T) receives J^T f; with r64
