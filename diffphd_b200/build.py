@@ -15,7 +15,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libdiffphd_b200.so"
-SOURCES = ["kernels.cu", "engine.cu", "setup.cpp", "capi.cpp", "noalloc.cu", "contact.cu", "mlp.cu", "mlp_tc.cu"]
+SOURCES = ["kernels.cu", "engine.cu", "setup.cpp", "capi.cpp", "noalloc.cu", "contact.cu", "mlp.cu", "mlp_tc.cu",
+           "sfactor_plan.cpp", "sfactor_gpu.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

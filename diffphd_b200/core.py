@@ -76,6 +76,9 @@ def load_library():
     L.dphd_kernel_launches.argtypes = [C.c_void_p]
     L.dphd_kernel_launches.restype = C.c_longlong
     L.dphd_device.argtypes = [C.c_void_p]
+    L.dphd_fp64_escalations.argtypes = [C.c_void_p]
+    L.dphd_debug_set_factor_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.dphd_factor_built_on_device.argtypes = [C.c_void_p]
     L.dphd_s_padded_values.argtypes = [C.c_void_p]
     L.dphd_s_padded_values.restype = C.c_longlong
     L.dphd_debug_time_ainv.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, _dp]
@@ -332,6 +335,18 @@ class Deformable:
 
     def reset_warm_start(self):
         self._check(self._L.dphd_reset_warm_start(self._h))
+
+    def set_factor_build(self, mode, small_subtree_max=0):
+        """0 automatic, 1 host, 2 device construction of the sparse-inverse factor (next build); in device mode the
+        etree subtrees of at most `small_subtree_max` nodes (512 when 0) are still built on the host."""
+        self._check(self._L.dphd_debug_set_factor_build(self._h, int(mode), int(small_subtree_max)))
+
+    def factor_built_on_device(self):
+        return int(self._L.dphd_factor_built_on_device(self._h)) == 1
+
+    def fp64_escalations(self):
+        """Mixed-precision frames that finished in FP64 after the FP32 iteration stalled."""
+        return int(self._L.dphd_fp64_escalations(self._h))
 
     def device(self):
         """CUDA device holding this deformable's GPU state (-1 before the first call that builds it)."""

@@ -377,6 +377,12 @@ int dphd_reset_warm_start(dphd_deformable* h) {
     return guard([&] { E(h).reset_warm_start(); });
 }
 
+int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_max) {
+    return guard([&] { E(h).set_factor_build(mode, small_subtree_max); });
+}
+int dphd_factor_built_on_device(const dphd_deformable* h) {
+    return h && h->eng ? h->eng->factor_built_on_device() : -1;
+}
 int dphd_device(const dphd_deformable* h) { return h && h->eng ? h->eng->device() : -2; }
 
 long long dphd_kernel_launches(const dphd_deformable* h) { return h && h->eng ? h->eng->kernel_launches() : -1; }
@@ -423,6 +429,7 @@ int dphd_reset_frame_stats(dphd_deformable* h) {
         E(h).stats.frame_converged.clear();
     });
 }
+int dphd_fp64_escalations(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.fp64_escalations : -1; }
 int dphd_last_backward_iters(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.last_bwd_iters : -1; }
 int dphd_last_filtered_samples(const dphd_deformable* h) {
     return h && h->eng ? h->eng->stats.last_filtered : -1;

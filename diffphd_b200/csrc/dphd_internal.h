@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -88,10 +89,47 @@ struct ContactPaths {
 };
 ContactPaths build_contact_paths(const SFactor& S, const std::vector<int>& cand_nodes);
 
+// Upper triangle (row <= col) of P A P^T by columns, in the factor's permuted order.
+struct PermUpper {
+    std::vector<int> Cp, Ci;
+    std::vector<double> Cx;
+};
+
+// Plan of the device construction of S (sfactor_plan.cpp, sfactor_gpu.cu).
+constexpr int kSbTile = 64;  // column tile of the S[s, D] product
+struct SBigSuper {
+    int a = 0, b = 0;   // rows [a, b) of an etree chain (permuted indices)
+    int lo = 0, ra = 0; // first column of the rows' segments, and its 4-aligned start in storage
+    int64_t B_off = 0;  // its B_s rows: plan.B[B_off .. B_off + nB)
+    int nB = 0;
+    int64_t ct_off = 0; // column tile t's contributing B positions: ct_p[ct_ptr[ct_off + t] .. ct_ptr[ct_off + t + 1])
+    int nct = 0;        // column tiles of kSbTile columns from ra up to a
+};
+struct SBuildPlan {
+    int small_max = 0;
+    std::vector<int> small_roots;   // roots of the host-built subtrees, ascending
+    std::vector<SBigSuper> sup;     // device-built supernodes in postorder
+    std::vector<int> B;
+    std::vector<int64_t> ct_ptr;
+    std::vector<int> ct_p;
+    std::vector<int64_t> a_rp;      // P A P^T, both triangles, by rows (permuted indices)
+    std::vector<int> a_ci;
+    std::vector<double> a_v;
+    int max_w = 0, max_nB = 0;
+    int64_t max_x = 0;              // largest [W | I] work array (rows padded to kSbTile) in doubles
+};
+SBuildPlan plan_sfactor_build(const struct SFactor& S, const struct PermUpper& U, int small_max);
+void sfactor_small_rows(const struct SFactor& S, const struct PermUpper& U, const std::vector<int>& roots, int threads,
+                        const std::function<double*(int)>& row_ptr);
+
 void init_samples(HostModel& M);
 double element_volume(const HostModel& M, int e);
 NodeMatrix assemble_A(const HostModel& M, double dt);
 std::vector<int> nested_dissection(const HostModel& M, const NodeMatrix& A);
 void build_sfactor(const NodeMatrix& A, const std::vector<int>& order, SFactor& S, int threads);
+// The symbolic half of build_sfactor: postorder permutation, etree, row ranges lo and row_ptr (no values) ...
+void sfactor_symbolic(const NodeMatrix& A, const std::vector<int>& order, SFactor& S, PermUpper& U);
+// ... and its numeric half on the host (up-looking LDL^T and the row recurrence into S.vals).
+void sfactor_numeric_host(const PermUpper& U, SFactor& S, int threads);
 
 }  // namespace dphd

@@ -67,6 +67,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.poll_chunk = std::max(1, (int)get("poll_chunk", 8));
     o.graph_while = (int)get("graph_while", 1);
     o.ws_tcgen05 = (int)get("ws_tcgen05", 1);
+    o.fp32_stall_window = std::max(0, (int)get("fp32_stall_window", 40));
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -209,6 +210,14 @@ long long Engine::s_memory_bytes() const {
            d_row_len.bytes + d_tile_ptr.bytes + d_tile_rows.bytes;
 }
 
+void Engine::set_factor_build(int mode, int small_subtree_max) {
+    DPHD_CHECK(mode >= 0 && mode <= 2, "factor build mode must be 0 (automatic), 1 (host) or 2 (device)");
+    const int sm = small_subtree_max > 0 ? small_subtree_max : 512;
+    if (mode != factor_mode_ || sm != small_subtree_max_) built_ = false;
+    factor_mode_ = mode;
+    small_subtree_max_ = sm;
+}
+
 void Engine::check_device() const {
     if (device_ < 0) return;
     int cur = -1;
@@ -235,7 +244,16 @@ void Engine::ensure_built(double dt, int threads) {
     A = assemble_A(M, dt);
     const std::vector<int> order = nested_dissection(M, A);
     S = SFactor();
-    build_sfactor(A, order, S, threads);
+    sb_upper_.reset(new PermUpper());
+    sfactor_symbolic(A, order, S, *sb_upper_);
+    factor_on_device_ = factor_mode_ == 2 || (factor_mode_ == 0 && S.nnz() > kDeviceBuildNnz);
+    if (factor_on_device_) {
+        sb_plan_.reset(new SBuildPlan(plan_sfactor_build(S, *sb_upper_, small_subtree_max_)));
+    } else {
+        sfactor_numeric_host(*sb_upper_, S, threads);
+        sb_upper_.reset();
+        sb_plan_.reset();
+    }
     built_ = true;
     built_dt_ = dt;
     device_ready_ = false;
@@ -259,12 +277,44 @@ void Engine::build_device(int threads) {
         rl[i] = ((i + 1 - ra[i]) + 3) & ~3;
         ro[i + 1] = ro[i] + rl[i];
     }
-    std::vector<double> v64(ro[n], 0.0);
-    for (int i = 0; i < n; ++i) {
-        const double* src = &S.vals[S.row_ptr[i]];
-        std::copy(src, src + (i - S.lo[i] + 1), &v64[ro[i] + (S.lo[i] - ra[i])]);
+    if (!factor_on_device_) {
+        std::vector<double> v64(ro[n], 0.0);
+        for (int i = 0; i < n; ++i) {
+            const double* src = &S.vals[S.row_ptr[i]];
+            std::copy(src, src + (i - S.lo[i] + 1), &v64[ro[i] + (S.lo[i] - ra[i])]);
+        }
+        std::vector<float> v32(v64.begin(), v64.end());
+        d_vals64.upload(v64);
+        d_vals32.upload(v32);
     }
-    std::vector<float> v32(v64.begin(), v64.end());
+    d_row_a.upload(ra);
+    d_row_len.upload(rl);
+    d_row_off.upload(ro);
+    if (factor_on_device_) {
+        DPHD_CHECK(sb_plan_ && sb_upper_, "device factor build: the symbolic plan is missing");
+        d_vals64.alloc((size_t)ro[n] * sizeof(double));
+        CUDA_OK(cudaMemsetAsync(d_vals64.p, 0, d_vals64.bytes, stream_));
+        // rows of the small subtrees: on the host into one zeroed staging array in the padded layout
+        const std::vector<int>& roots = sb_plan_->small_roots;
+        std::vector<int64_t> soff(roots.size() + 1, 0);
+        for (size_t q = 0; q < roots.size(); ++q) soff[q + 1] = soff[q] + (ro[roots[q] + 1] - ro[S.lo[roots[q]]]);
+        std::vector<double> staging(soff.back(), 0.0);
+        std::vector<int64_t> rowbase(n, 0);
+        for (size_t q = 0; q < roots.size(); ++q)
+            for (int i = S.lo[roots[q]]; i <= roots[q]; ++i) rowbase[i] = soff[q] - ro[S.lo[roots[q]]];
+        sfactor_small_rows(S, *sb_upper_, roots, threads,
+                           [&](int i) { return staging.data() + rowbase[i] + ro[i] + (S.lo[i] - ra[i]); });
+        for (size_t q = 0; q < roots.size(); ++q)
+            CUDA_OK(cudaMemcpyAsync(d_vals64.as<double>() + ro[S.lo[roots[q]]], staging.data() + soff[q],
+                                    (soff[q + 1] - soff[q]) * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        device_build_factor(*sb_plan_, S.lo, d_row_off.as<int64_t>(), d_row_a.as<int>(), d_row_len.as<int>(),
+                            d_vals64.as<double>(), stream_);
+        d_vals32.alloc((size_t)ro[n] * sizeof(float));
+        device_round_f32(d_vals64.as<double>(), d_vals32.as<float>(), (long long)ro[n], stream_);
+        CUDA_OK(cudaStreamSynchronize(stream_));
+        sb_plan_.reset();
+        sb_upper_.reset();
+    }
     // column tiles of S^T: rows whose padded segment meets the tile, ascending
     std::vector<int> tcnt(ntiles_ + 1, 0);
     for (int i = 0; i < n; ++i)
@@ -391,11 +441,6 @@ void Engine::build_device(int threads) {
     d_tile_chunk_ptr.upload(t_cptr);
     d_xpart64.alloc(c_tile.size() * 3 * kTileCols * sizeof(double));
     d_xpart32.alloc(c_tile.size() * 3 * kTileCols * sizeof(float));
-    d_row_a.upload(ra);
-    d_row_len.upload(rl);
-    d_row_off.upload(ro);
-    d_vals64.upload(v64);
-    d_vals32.upload(v32);
     d_tile_ptr.upload(tcnt);
     d_tile_rows.upload(trows);
     d_perm.upload(S.perm);
@@ -621,7 +666,14 @@ void Engine::build_contact(double dt) {
     dc_cand.upload(M.contact_nodes);
     dc_off.upload(P.off);
     dc_prow.upload(P.row);
-    dc_pval.upload(P.val);
+    if (!P.val.empty()) {
+        dc_pval.upload(P.val);
+    } else {  // device-built factor: gather the path values from the device copy of S
+        dc_pval.alloc(std::max<size_t>(1, P.row.size()) * sizeof(double));
+        device_path_vals(K, dc_off.as<int64_t>(), dc_prow.as<int>(), dc_cand.as<int>(), d_iperm.as<int>(),
+                         d_vals64.as<double>(), d_row_off.as<int64_t>(), d_row_a.as<int>(), dc_pval.as<double>(), 0);
+        CUDA_OK(cudaDeviceSynchronize());
+    }
     dc_G.alloc((size_t)K * K * sizeof(double));
     launch_delassus(K, dc_off.as<int64_t>(), dc_prow.as<int>(), dc_pval.as<double>(), dc_G.as<double>(), 0);
     CUDA_OK(cudaDeviceSynchronize());
@@ -996,6 +1048,7 @@ static void init_ctrl(Ctrl* h, int mode, const Options& o, int max_iter, double 
     h->rel_tol = o.rel_tol;
     h->abs_tol = o.abs_tol;
     h->clip = clip;
+    h->best_ratio = 1e300;
 }
 
 void Engine::check_status(const char* where) {
@@ -1030,12 +1083,29 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
                 }
         graph_mu_ = o.friction_mu;
         CUDA_OK(cudaMemsetAsync(dc_bar.p, 0, dc_bar.bytes, st));  // clears an abort left by an earlier solve
-        run_iterations(o.fp32_bulk ? 8 : 5, o, st);
-    } else {
-        run_iterations(o.fp32_bulk ? 1 : 0, o, st);
     }
+    const int mode64 = has_contact_ ? 5 : 0, mode32 = has_contact_ ? 8 : 1;
+    if (o.fp32_bulk && o.fp32_stall_window > 0) {
+        h_ctrl_->stall_window = o.fp32_stall_window;
+        CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    }
+    run_iterations(o.fp32_bulk ? mode32 : mode64, o, st);
     check_status("forward");
-    stats.frame_iters.push_back(h_ctrl_->iter);
+    int iters = h_ctrl_->iter;
+    if (o.fp32_bulk && h_ctrl_->stalled && !h_ctrl_->converged && iters < o.max_pd_iter) {
+        // the FP32 iteration stopped improving: the rest of the frame runs in FP64 from the current iterate, with a
+        // fresh Anderson history and the same gate (the iterations of both parts count against max_pd_iter)
+        Options o64 = o;
+        o64.max_pd_iter = o.max_pd_iter - iters;
+        CUDA_OK(cudaMemsetAsync(d_prev_pd.p, 0, n3 * sizeof(double), st));
+        init_ctrl(h_ctrl_, 0, o64, o64.max_pd_iter, 0.0);
+        CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+        run_iterations(mode64, o, st);  // o: the captured loop's iteration cap; the device gate stops at o64's
+        check_status("forward");
+        iters += h_ctrl_->iter;
+        stats.fp64_escalations++;
+    }
+    stats.frame_iters.push_back(iters);
     stats.frame_converged.push_back(h_ctrl_->converged);
     if (!h_ctrl_->converged && o.verbose >= 0)
         std::fprintf(stderr, "frame: %zu alg_phd: PD loop did not converge.\n", stats.frame_iters.size());
@@ -1712,6 +1782,7 @@ void Engine::host_sts_apply(double dt, const double* b, double* x) {
         built_dt_ = dt;
         device_ready_ = false;
     }
+    DPHD_CHECK(!S.vals.empty(), "the factor was built on the device: no host copy of S to apply");
     const int n = M.n;
     std::vector<unsigned char> fixed(n, 0);
     for (const auto& kv : M.dirichlet) fixed[kv.first / 3] = 1;

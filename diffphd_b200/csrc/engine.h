@@ -41,6 +41,8 @@ struct Options {
     int poll_chunk = 8;
     int graph_while = 1;         // device-side WHILE graph per solve (0: host polling every poll_chunk iterations)
     int ws_tcgen05 = 1;          // warm-start inference on tcgen05 MMAs with TMEM accumulators (0: mma.sync)
+    int fp32_stall_window = 40;  // mixed precision: iterations without the gate ratio halving before the rest of
+                                 // the frame continues in FP64 (0: never)
     static Options parse(const std::map<std::string, double>& m);
 };
 
@@ -63,6 +65,7 @@ struct DeviceBuffer {
 
 struct StepStats {
     std::vector<int> frame_iters, frame_converged;
+    int fp64_escalations = 0;  // mixed-precision frames finished in FP64 after the FP32 iteration stalled
     int last_bwd_iters = 0, last_filtered = 0, bwd_fallbacks = 0;
     // last backward's contact-aware material adjoint: frame source (0 no contact / skipped by option,
     // 1 forward tape, 2 replayed forward step, 3 tape miss without replay inputs), constraints, CG iterations
@@ -137,6 +140,11 @@ public:
     // time `reps` applications of the S^T S pair on the device; returns ms per application
     double time_ainv(double dt, int reps, bool fp32, bool flush_l2);
     long long kernel_launches() const { return launches_; }
+    // how the sparse-inverse factor is built: 0 automatic (on the device above kDeviceBuildNnz values, on the
+    // host below), 1 host, 2 device; a change takes effect at the next factor build
+    void set_factor_build(int mode, int small_subtree_max);
+    int factor_built_on_device() const { return factor_on_device_ ? 1 : 0; }
+    static constexpr long long kDeviceBuildNnz = 32ll << 20;
     // CUDA device that holds this handle's GPU state (-1 until the first call that builds it); every later
     // call must be made with that device current
     int device() const { return device_; }
@@ -190,6 +198,10 @@ private:
     void check_status(const char* where);
     void check_device() const;
     int device_ = -1;
+    int factor_mode_ = 0, small_subtree_max_ = 512;
+    bool factor_on_device_ = false;
+    std::unique_ptr<SBuildPlan> sb_plan_;   // device build: plan and the permuted upper triangle of A, kept from
+    std::unique_ptr<PermUpper> sb_upper_;   // the symbolic step until build_device runs the numeric one
 
     bool built_ = false;
     double built_dt_ = -1;

@@ -877,6 +877,16 @@ __global__ void __launch_bounds__(kThreads) k_aa_update(int n3, double* __restri
         ctrl->dq = dq; ctrl->rn = rn; ctrl->pdc = pdc; ctrl->pdr = pdr;
         conv = it > 0 && dq <= ctrl->rel_tol * rn + ctrl->abs_tol && pdc <= ctrl->rel_tol * pdr + ctrl->abs_tol;
         if (!(dq == dq) || !(pdc == pdc)) ctrl->status |= kStatusNonFinite;
+        if (!conv && it > 0 && ctrl->stall_window > 0) {
+            const double ratio = fmax(dq / (ctrl->rel_tol * rn + ctrl->abs_tol), pdc / (ctrl->rel_tol * pdr + ctrl->abs_tol));
+            if (ratio < 0.5 * ctrl->best_ratio) {
+                ctrl->best_ratio = ratio;
+                ctrl->best_it = it;
+            } else if (it - ctrl->best_it >= ctrl->stall_window) {
+                ctrl->stalled = 1;
+                ctrl->done = 1;
+            }
+        }
     } else {
         ctrl->dq = dq; ctrl->rn = xnorm;
         conv = it > 0 && ctrl->err < ctrl->rel_tol * xnorm + ctrl->abs_tol;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "devmath.cuh"
 
@@ -35,6 +36,10 @@ struct Ctrl {
     int pcg_init;
     unsigned int arrive[4];
     int loops;  // iterations run by the device-side while loop (k_loop_cond)
+    // stall detection of the forward loop (mixed precision): the solve stops with `stalled` set when the gate
+    // ratio max(|dq| / (rtol |q| + atol), |d pd| / (rtol |pd| + atol)) has not halved for stall_window iterations
+    int stall_window, stalled, best_it;
+    double best_ratio;
 };
 
 struct EnergyPack {
@@ -254,6 +259,15 @@ void launch_wb_project(int capacity, const int* count, const int* nodes, const d
                        double* u, T* vperm, const int* iperm, int npad, const Ctrl* ctrl, cudaStream_t st);
 void launch_gather_nodes(int K, const int* cand, const double* u, double* out, cudaStream_t st);
 void launch_diff_norms(int n, const double* a, const double* b, double* res, cudaStream_t st);
+
+// Device construction of the sparse-inverse factor (sfactor_gpu.cu): fills the device-built supernodes' rows of
+// d_vals (FP64, padded row layout; the small-subtree rows must already be there), then the FP32 copy.
+struct SBuildPlan;
+void device_build_factor(const SBuildPlan& P, const std::vector<int>& lo, const int64_t* d_ro, const int* d_ra,
+                         const int* d_rl, double* d_vals, cudaStream_t st);
+void device_round_f32(const double* d_in, float* d_out, long long n, cudaStream_t st);
+void device_path_vals(int K, const int64_t* d_off, const int* d_prow, const int* d_cand, const int* d_iperm,
+                      const double* d_vals, const int64_t* d_ro, const int* d_ra, double* d_pval, cudaStream_t st);
 
 // Device-side loop control of a graph WHILE node: counts the iteration and keeps looping while the gate has
 // not set `done` and fewer than `cap` iterations ran (cap > max_iter: a bound even if a gate kernel is skipped).

@@ -258,10 +258,11 @@ std::vector<int> etree(int n, const std::vector<int>& Cp, const std::vector<int>
 
 }  // namespace
 
-void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor& S, int threads) {
+void sfactor_symbolic(const NodeMatrix& A, const std::vector<int>& order0, SFactor& S, PermUpper& U) {
     const int n = A.n;
-    std::vector<int> Cp, Ci;
-    std::vector<double> Cx;
+    std::vector<int>& Cp = U.Cp;
+    std::vector<int>& Ci = U.Ci;
+    std::vector<double>& Cx = U.Cx;
     permuted_upper(A, order0, Cp, Ci, Cx);
     std::vector<int> par = etree(n, Cp, Ci);
     // postorder (children visited in increasing index order)
@@ -311,6 +312,21 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
         for (int j = n - 1; j >= 0; --j) depth[j] = S.parent[j] == -1 ? 0 : depth[S.parent[j]] + 1;
         S.max_depth = n ? *std::max_element(depth.begin(), depth.end()) : 0;
     }
+    S.row_ptr.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i) S.row_ptr[i + 1] = S.row_ptr[i] + (i - S.lo[i] + 1);
+}
+
+void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor& S, int threads) {
+    PermUpper U;
+    sfactor_symbolic(A, order0, S, U);
+    sfactor_numeric_host(U, S, threads);
+}
+
+void sfactor_numeric_host(const PermUpper& U, SFactor& S, int threads) {
+    const int n = S.n;
+    const std::vector<int>& Cp = U.Cp;
+    const std::vector<int>& Ci = U.Ci;
+    const std::vector<double>& Cx = U.Cx;
     // Up-looking LDL^T (Davis, ACM TOMS Algorithm 849): row k of L is computed from a sparse triangular
     // solve whose pattern is the row subtree of k.  Rows of L are kept for the L^-1 recurrence below.
     std::vector<int> lnz(n, 0), flag(n, -1);
@@ -370,8 +386,6 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
         D[k] = dk;
     }
     // S rows: row_i(L^-1) = e_i - sum_{k in row_i(L)} l_ik row_k(L^-1), each row dense on [lo_i, i].
-    S.row_ptr.assign(n + 1, 0);
-    for (int i = 0; i < n; ++i) S.row_ptr[i + 1] = S.row_ptr[i] + (i - S.lo[i] + 1);
     S.vals.assign(S.row_ptr[n], 0.0);
     S.Dinv_sqrt.resize(n);
     for (int i = 0; i < n; ++i) S.Dinv_sqrt[i] = 1.0 / std::sqrt(D[i]);
@@ -410,6 +424,8 @@ void build_sfactor(const NodeMatrix& A, const std::vector<int>& order0, SFactor&
     }
 }
 
+// Without a host copy of the S values (a device-built factor) only the path rows are filled; the values are
+// then gathered on the device.
 ContactPaths build_contact_paths(const SFactor& S, const std::vector<int>& cand_nodes) {
     ContactPaths P;
     const int K = (int)cand_nodes.size();
@@ -423,13 +439,13 @@ ContactPaths build_contact_paths(const SFactor& S, const std::vector<int>& cand_
         P.max_depth = std::max(P.max_depth, (int)paths[c].size());
     }
     P.row.resize(P.off[K]);
-    P.val.resize(P.off[K]);
+    if (!S.vals.empty()) P.val.resize(P.off[K]);
     for (int c = 0; c < K; ++c) {
         const int col = S.iperm[cand_nodes[c]];
         for (size_t k = 0; k < paths[c].size(); ++k) {
             const int r = paths[c][k];
             P.row[P.off[c] + k] = r;
-            P.val[P.off[c] + k] = S.vals[S.row_ptr[r] + (col - S.lo[r])];
+            if (!S.vals.empty()) P.val[P.off[c] + k] = S.vals[S.row_ptr[r] + (col - S.lo[r])];
         }
     }
     return P;

@@ -102,6 +102,14 @@ int dphd_reset_warm_start(dphd_deformable* h);
 
 /* Number of kernels this library launched on the GPU since the handle was created (graph nodes included). */
 long long dphd_kernel_launches(const dphd_deformable* h);
+/* Where the sparse-inverse factor S is built (the reference builds it on the host from an LDL^T and uploads it,
+ * forward_gpu.cpp:593-764): 0 automatic (on the device when S has more than 32 Mi values, else on the host),
+ * 1 host, 2 device (rows of etree subtrees of at most small_subtree_max nodes, 512 when <= 0, on the host; every
+ * larger separator chain on the GPU from the Schur complement of its descendants).  Takes effect at the next
+ * factor build.  No counterpart in the reference. */
+int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_max);
+/* 1 when the current factor was built on the device, 0 on the host, -1 for a null handle. */
+int dphd_factor_built_on_device(const dphd_deformable* h);
 /* CUDA device that holds this handle's GPU state: -1 until the first call that builds the factor (it records
  * the device current then), -2 for a null handle.  Later calls made while another device is current fail with
  * an error instead of mixing pointers of two devices.  No counterpart in the reference (fixed to device 0,
@@ -114,6 +122,10 @@ int dphd_num_frames(const dphd_deformable* h);
 int dphd_frame_stats(const dphd_deformable* h, int* frame_iters, int* frame_converged);
 int dphd_reset_frame_stats(dphd_deformable* h);
 int dphd_last_backward_iters(const dphd_deformable* h);
+/* Mixed-precision forward frames (option fp32_bulk) whose FP32 iteration stalled and that finished in FP64 from
+ * the FP32 iterate, since the handle was created (option fp32_stall_window: iterations without the gate ratio
+ * halving, default 40; 0 never switches).  No counterpart in the reference. */
+int dphd_fp64_escalations(const dphd_deformable* h);
 /* Samples whose 9x9 local Hessian the last backward call eigen-filtered (option bwd_eigen_filter 1 clamp /
  * 2 absolute value; the diagonal-dominance test of ProjectedNewtonMatrix, deformable_newton_forward.cpp:394-434). */
 int dphd_last_filtered_samples(const dphd_deformable* h);
