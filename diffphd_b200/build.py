@@ -16,7 +16,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libdiffphd_b200.so"
 SOURCES = ["kernels.cu", "engine.cu", "setup.cpp", "capi.cpp", "noalloc.cu", "contact.cu", "mlp.cu", "mlp_tc.cu",
-           "sfactor_plan.cpp", "sfactor_gpu.cu"]
+           "sfactor_plan.cpp", "sfactor_gpu.cu", "contact_precond.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -55,6 +55,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.bwd_mean_stiffness = (int)get("bwd_mean_stiffness", 0);
     o.bwd_cascade_cap = (int)get("bwd_cascade_cap", 1);
     o.bwd_eigen_filter = (int)get("bwd_eigen_filter", 0);
+    o.bwd_contact_precond = (int)get("bwd_contact_precond", 1);
     o.fp32_bulk = (int)get("fp32_bulk", 0);
     o.bwd_solver = (int)get("alg_phd_bwd_solver", 0);
     o.bwd_warm_start = (int)get("alg_phd_bwd_warm_start", 0);
@@ -68,6 +69,8 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.graph_while = (int)get("graph_while", 1);
     o.ws_tcgen05 = (int)get("ws_tcgen05", 1);
     o.fp32_stall_window = std::max(0, (int)get("fp32_stall_window", 40));
+    o.fp32_projection = (int)get("fp32_projection", -1);
+    o.ws_lambda = (int)get("ws_lambda", 1);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -721,6 +724,7 @@ void Engine::build_contact(double dt) {
 
 void Engine::reset_warm_start() {
     if (has_contact_ && dc_lam.p) CUDA_OK(cudaMemset(dc_lam.p, 0, dc_lam.bytes));
+    z_hist_ = 0;
     mu_prev_valid_ = false;
     mu_prev2_valid_ = false;
     mu_prev3_valid_ = false;
@@ -761,9 +765,14 @@ void Engine::enqueue_contact_iteration(cudaStream_t st, bool f32) {
         // CSR of A, also kept in FP64), y = S r in FP32; the NCP sees A^-1 b = x + S^T-path(y) at the
         // candidates and solves in FP64; the S input becomes r + J^T f (summed in FP64 at the candidates:
         // near the fixed point the two nearly cancel there), y = S (r + J^T f), x_raw = x + S^T y.
-        launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
-                               d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, M.vol / M.s, ep,
-                               d_elem_out64.as<double>(), c, st);
+        if (proj32_)
+            launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                   d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, M.vol / M.s, ep,
+                                   d_elem_out64.as<double>(), c, st);
+        else
+            launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                    d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, M.vol / M.s, ep,
+                                    d_elem_out64.as<double>(), c, st);
         launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
@@ -847,9 +856,14 @@ void Engine::enqueue_fwd_iteration(bool f32, cudaStream_t st) {
     const EnergyPack ep = energy_pack();
     Ctrl* c = d_ctrl.as<Ctrl>();
     if (f32) {
-        launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
-                               d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
-                               d_elem_out64.as<double>(), c, st);
+        if (proj32_)
+            launch_elem_fwd<float>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                   d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                                   d_elem_out64.as<double>(), c, st);
+        else
+            launch_elem_fwd<double>(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), d_qb.as<double>(),
+                                    d_elem_dir.as<unsigned char>(), dgrad.as<double>(), M.hex, vol_over_s, ep,
+                                    d_elem_out64.as<double>(), c, st);
         launch_gather_fwd<float>(n, d_node_ptr.as<int>(), d_node_inc.as<int>(), d_elem_out64.as<double>(),
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
@@ -891,7 +905,40 @@ void Engine::enqueue_bwd_iteration(cudaStream_t st) {
 }
 
 // One conjugate-gradient iteration of the adjoint (A - K_pd) mu = g_bar, preconditioned by S^T S.
-void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected) {
+void Engine::enqueue_contact_precond(bool f32, bool woodbury, cudaStream_t st) {
+    if (!woodbury) {
+        launch_ainv(f32, st);
+        return;
+    }
+    Ctrl* c = d_ctrl.as<Ctrl>();
+    const int K = contact_.K, ld = (int)ncp_matrix_capacity(K);
+    if (f32) {
+        launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
+        for (int stage = 0; stage < 2; ++stage)
+            launch_wbp_precond_parts<float>(stage, K, d_wb_count.as<int>(), d_wbp_cand.as<int>(), d_wbp_pos.as<int>(),
+                                            d_wbp_nb.as<int>(), contact_, wbp_dirs_, d_y32.as<float>(), npad_,
+                                            d_wbp_X.as<double>(), ld, d_wbp_u.as<double>(), d_wbp_w.as<double>(),
+                                            d_wbp_lam.as<double>(), d_iperm.as<int>(), d_vjac32.as<float>(), c, st);
+        SpmvPlan<float> acc = plan32_;
+        acc.y_accumulate = 1;
+        launch_s_only<float>(acc, d_vjac32.as<float>(), d_y32.as<float>(), c, st);
+        launch_st_only<float>(plan32_, d_y32.as<float>(), d_xraw.as<double>(), c, st);
+    } else {
+        launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
+        for (int stage = 0; stage < 2; ++stage)
+            launch_wbp_precond_parts<double>(stage, K, d_wb_count.as<int>(), d_wbp_cand.as<int>(),
+                                             d_wbp_pos.as<int>(), d_wbp_nb.as<int>(), contact_, wbp_dirs_,
+                                             d_y64.as<double>(), npad_, d_wbp_X.as<double>(), ld,
+                                             d_wbp_u.as<double>(), d_wbp_w.as<double>(), d_wbp_lam.as<double>(),
+                                             d_iperm.as<int>(), d_vjac64.as<double>(), c, st);
+        SpmvPlan<double> acc = plan64_;
+        acc.y_accumulate = 1;
+        launch_s_only<double>(acc, d_vjac64.as<double>(), d_y64.as<double>(), c, st);
+        launch_st_only<double>(plan64_, d_y64.as<double>(), d_xraw.as<double>(), c, st);
+    }
+}
+
+void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected, bool woodbury) {
     const int n = M.n, n3 = 3 * n;
     Ctrl* c = d_ctrl.as<Ctrl>();
     const int capK = has_contact_ ? contact_.K : 0;
@@ -915,8 +962,8 @@ void Engine::enqueue_pcg_iteration(bool f32, cudaStream_t st, bool projected) {
         launch_pcg_update1<double>(n, d_x.as<double>(), d_r.as<double>(), d_pp.as<double>(), d_wv.as<double>(),
                                    d_fixed_node.as<unsigned char>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_,
                                    d_part_upd.as<double>(), gather_blocks_, c, st);
-    if (projected) {  // z = P A^-1 P r, then the z-side update
-        launch_ainv(f32, st);
+    if (projected) {  // z = P M^-1 P r (M^-1 the preconditioner), then the z-side update
+        enqueue_contact_precond(f32, woodbury, st);
         launch_wb_project<double>(capK, d_wb_count.as<int>(), d_wb_nodes.as<int>(), d_wb_dirs.as<double>(),
                                   d_wb_ndir.as<int>(), d_xraw.as<double>(), nullptr, nullptr, npad_, c, st);
         launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(),
@@ -941,7 +988,8 @@ void Engine::enqueue_iteration(int mode, cudaStream_t cap) {
     if (mode == 2) enqueue_bwd_iteration(cap);
     else if (mode == 5 || mode == 8) enqueue_contact_iteration(cap, mode == 8);
     else if (mode == 6 || mode == 7) enqueue_pcg_iteration(mode == 7, cap, true);
-    else if (mode >= 3) enqueue_pcg_iteration(mode == 4, cap);
+    else if (mode == 9 || mode == 10) enqueue_pcg_iteration(mode == 10, cap, true, true);
+    else if (mode == 3 || mode == 4) enqueue_pcg_iteration(mode == 4, cap);
     else enqueue_fwd_iteration(mode == 1, cap);
 }
 
@@ -1071,6 +1119,17 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
         drop_graphs();
         graph_dt_ = h;
     }
+    // FP32 projections by default only without contact: with a contact set their rounding slows the coupled
+    // PD / NCP iteration (measured on the 64^3 contact block), so FP64 projections feed the FP32 S passes there
+    const bool want32 = o.fp32_projection < 0 ? !has_contact_ : o.fp32_projection != 0;
+    if (want32 != proj32_) {  // the projection precision is captured in the mixed graphs
+        proj32_ = want32;
+        for (int md : {1, 8})
+            if (graphs_[md]) {
+                cudaGraphExecDestroy(graphs_[md]);
+                graphs_[md] = nullptr;
+            }
+    }
     if (has_contact_) {
         contact_.mu = o.friction_mu;
         CUDA_OK(cudaMemsetAsync(dc_lt1.p, 0, dc_lt1.bytes, st));
@@ -1122,6 +1181,7 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     const int n3 = dofs();
     const double h2m = dt * dt / M.mass();
     const bool learned = !d_init && ws_net_;
+    ws_lambda_ = o.ws_lambda != 0;
     if (learned) d_init = ws_predict(dq, dv, df, dt, o.ws_tcgen05 != 0, st);
     // new-rollout detection of the contact tape (forward_gpu.cpp:437-449): the input must continue the last
     // frame; the comparison is read after the solve's own synchronisation
@@ -1217,6 +1277,11 @@ const double* Engine::ws_predict(const double* dq, const double* dv, const doubl
     }
     ws_apply(dt, base, d_ws_out.as<float>(), d_ws_qinit.as<double>(), st);
     launches_ += 1;
+    if (has_contact_ && ws_lambda_) {  // the predicted initial contact multipliers replace the previous frame's
+        launch_mlp_lambda_apply(contact_.K, dc_cand.as<int>(), d_ws_out.as<float>(), 1.0 / ws_lambda_scale(dt),
+                                dc_lam.as<double>(), st);
+        launches_ += 1;
+    }
     return d_ws_qinit.as<double>();
 }
 
@@ -1252,9 +1317,19 @@ void Engine::ws_features(double dt, const double* dq, const double* dqp, const d
     a.plane = M.has_plane ? 1 : 0;
     for (int d = 0; d < 3; ++d) a.pn[d] = M.plane_n[d];
     a.poff = M.plane_off;
-    launch_mlp_features(a, dq, dqp, dv, df, d_prev_base, X, d_base, st);
+    const float* lam_node = nullptr;
+    if (has_contact_ && dc_lam.p) {  // the current multipliers (the previous frame's) as the 16th feature
+        d_ws_lamnode.alloc((size_t)M.n * sizeof(float));
+        launch_mlp_lambda_nodes(M.n, contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), ws_lambda_scale(dt),
+                                d_ws_lamnode.as<float>(), st);
+        lam_node = d_ws_lamnode.as<float>();
+        launches_ += 2;
+    }
+    launch_mlp_features(a, dq, dqp, dv, df, d_prev_base, lam_node, X, d_base, st);
     launches_ += 1;
 }
+
+double Engine::ws_lambda_scale(double dt) const { return dt * dt / (M.mass() * ws_dx()); }
 
 void Engine::ws_apply(double dt, const double* d_base, const float* out, double* d_q_init, cudaStream_t st) {
     ensure_built(dt, 0);
@@ -1267,6 +1342,10 @@ void Engine::ws_target(double dt, const double* d_q_next, const double* d_base, 
     ensure_built(dt, 0);
     launch_mlp_target(dofs(), d_q_next, d_base, 1.0 / ws_dx(), Y, st);
     launches_ += 1;
+    if (has_contact_ && dc_lam.p) {  // the frame's final multipliers (the last forward call's) as column 3
+        launch_mlp_target_lambda(contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), ws_lambda_scale(dt), Y, st);
+        launches_ += 1;
+    }
 }
 
 void Engine::forward(const double* q, const double* v, const double* f_ext, double dt, const Options& o,
@@ -1442,6 +1521,19 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
     const int count = (int)nodes.size();
     stats.contact_constraints = (int)sel.size();
     if (count == 0) return;
+    // per direction b of the basis: its constrained candidates (the blocks of J A^-1 J^T), and each constrained
+    // node's position in them
+    std::vector<int> wcand, wpos, idx[3];
+    for (const auto& kv : per) {
+        if (M.dirichlet.count(3 * M.contact_nodes[kv.first])) continue;
+        int pos[3] = {-1, -1, -1};
+        for (int b : kv.second) {
+            pos[b] = (int)idx[b].size();
+            idx[b].push_back(kv.first);
+        }
+        wcand.push_back(kv.first);
+        for (int b = 0; b < 3; ++b) wpos.push_back(pos[b]);
+    }
     d_wb_nodes.alloc((size_t)K * sizeof(int));
     d_wb_ndir.alloc((size_t)K * sizeof(int));
     d_wb_dirs.alloc((size_t)9 * K * sizeof(double));
@@ -1454,6 +1546,35 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
     d_wb_mu.alloc(n3 * sizeof(double));
     CUDA_OK(cudaMemcpyAsync(d_wb_mu.p, d_x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     const bool f32 = o.fp32_bulk != 0;
+    const bool woodbury = o.bwd_contact_precond != 0;
+    if (woodbury) {
+        const size_t ld = ncp_matrix_capacity(K);
+        d_wbp_cand.alloc((size_t)K * sizeof(int));
+        d_wbp_pos.alloc((size_t)3 * K * sizeof(int));
+        d_wbp_nb.alloc(3 * sizeof(int));
+        d_wbp_idx.alloc((size_t)3 * K * sizeof(int));
+        d_wbp_X.alloc(3 * ld * ld * sizeof(double));
+        d_wbp_M.alloc(ld * ld * sizeof(double));
+        for (DeviceBuffer* b : {&d_wbp_u, &d_wbp_w, &d_wbp_lam}) b->alloc((size_t)3 * K * sizeof(double));
+        DeviceBuffer& vj = f32 ? d_vjac32 : d_vjac64;
+        vj.alloc((size_t)npad_ * 3 * (f32 ? sizeof(float) : sizeof(double)));
+        CUDA_OK(cudaMemsetAsync(vj.p, 0, vj.bytes, st));
+        CUDA_OK(cudaMemcpyAsync(d_wbp_cand.p, wcand.data(), wcand.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d_wbp_pos.p, wpos.data(), wpos.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        int nb[3] = {(int)idx[0].size(), (int)idx[1].size(), (int)idx[2].size()};
+        CUDA_OK(cudaMemcpyAsync(d_wbp_nb.p, nb, sizeof(nb), cudaMemcpyHostToDevice, st));
+        for (int b = 0; b < 3; ++b) {
+            for (int d = 0; d < 3; ++d) wbp_dirs_.d[b][d] = dirs3[b][d];
+            if (nb[b] == 0) continue;
+            int* db_idx = d_wbp_idx.as<int>() + (size_t)b * K;
+            CUDA_OK(cudaMemcpyAsync(db_idx, idx[b].data(), nb[b] * sizeof(int), cudaMemcpyHostToDevice, st));
+            const int npd = (nb[b] + 63) / 64 * 64;
+            double* Xb = d_wbp_X.as<double>() + (size_t)b * ld * ld;
+            launch_wbp_gather_g(nb[b], npd, db_idx, dc_G.as<double>(), K, d_wbp_M.as<double>(), Xb, (int)ld, st);
+            dense_chol_solve(d_wbp_M.as<double>(), npd, Xb, (int)ld, npd, st);  // X_b = L_b^-1
+        }
+        launches_ += 4;
+    }
     Ctrl* c = d_ctrl.as<Ctrl>();
     init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
     h_ctrl_->pcg_init = 1;
@@ -1469,7 +1590,10 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
                                       d_wb_ndir.as<int>(), u, reinterpret_cast<double*>(vperm), d_iperm.as<int>(),
                                       npad_, c, st);
     };
-    proj(d_x.as<double>(), nullptr);  // z_0 = P mu
+    // start: P mu, or (reverse sweeps, bwd_warm_start) P (mu + (z - mu) of the later step): the constraint
+    // correction carried over from the previous call (the projection makes any start admissible)
+    if (o.bwd_warm_start && z_hist_ > 0) launch_axpy(n3, 1.0, d_z1.as<double>(), d_x.as<double>(), st);
+    proj(d_x.as<double>(), nullptr);  // z_0 = P mu (or P (mu + correction))
     launch_kpd_elem(M.m, M.k, M.s, dE.as<int>(), d_x.as<double>(), dgrad.as<double>(), M.hex, d_J.as<double>(),
                     d_elem_out64.as<double>(), c, st);
     launch_pcg_gather(n, Acsr_, d_x.as<double>(), d_node_ptr.as<int>(), d_node_inc.as<int>(),
@@ -1484,17 +1608,22 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
         launch_pcg_init<double>(n, d_gbar.as<double>(), d_wv.as<double>(), d_fixed_node.as<unsigned char>(),
                                 d_iperm.as<int>(), d_r.as<double>(), d_vperm64.as<double>(), npad_, st);
     proj(d_r.as<double>(), vp);  // r_0 = P (g_bar - (A - K_pd) z_0)
-    launch_ainv(f32, st);
+    enqueue_contact_precond(f32, woodbury, st);
     proj(d_xraw.as<double>(), nullptr);
     launch_pcg_update2(n3, d_r.as<double>(), d_xraw.as<double>(), d_part_aa.as<double>(), d_part_upd.as<double>(),
                        gather_blocks_, red_blocks_, c, st);
     launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
     launches_ += 12;
-    run_iterations(f32 ? 7 : 6, o, st);
+    run_iterations(woodbury ? (f32 ? 10 : 9) : (f32 ? 7 : 6), o, st);
     stats.contact_iters = h_ctrl_->iter;
     if (h_ctrl_->status & (kStatusIndefinite | kStatusNonFinite | kStatusDiverged)) {
         CUDA_OK(cudaMemcpyAsync(d_x.p, d_wb_mu.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
         stats.bwd_fallbacks++;
+        z_hist_ = 0;
+    } else if (o.bwd_warm_start) {  // the constraint correction z - mu, for the next (earlier) step's start
+        d_z1.alloc(n3 * sizeof(double));
+        launch_sub(n3, d_x.as<double>(), d_wb_mu.as<double>(), d_z1.as<double>(), st);
+        z_hist_ = 1;
     }
 }
 

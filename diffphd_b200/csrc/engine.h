@@ -32,6 +32,8 @@ struct Options {
     int bwd_mean_stiffness = 0;  // reference backward semantics: mean stiffness inside K_pd
     int bwd_cascade_cap = 1;     // reference cap of the injected adjoint at |g_bar| + 1
     int bwd_eigen_filter = 0;    // 0 off (exact adjoint), 1 clamp, 2 abs
+    int bwd_contact_precond = 1; // contact-aware adjoint preconditioner: 1 exact inverse of A on the constrained
+                                 // subspace (Woodbury with the Delassus block), 0 P A^-1 P
     int fp32_bulk = 0;           // projection and S/S^T SpMVs in FP32
     int bwd_solver = 0;          // 0: Anderson-accelerated fixed point (reference), 1: preconditioned CG
     int bwd_warm_start = 0;      // CG adjoint starts from the previous backward call's solution (reverse sweeps)
@@ -41,6 +43,10 @@ struct Options {
     int poll_chunk = 8;
     int graph_while = 1;         // device-side WHILE graph per solve (0: host polling every poll_chunk iterations)
     int ws_tcgen05 = 1;          // warm-start inference on tcgen05 MMAs with TMEM accumulators (0: mma.sync)
+    int ws_lambda = 1;           // with a warm-start network and contact: start each frame's NCP from the
+                                 // network's predicted multipliers instead of the previous frame's
+    int fp32_projection = -1;    // mixed precision: 1 FP32 local projections, 0 FP64 projections with FP32 S
+                                 // passes, -1 automatic (FP32 without a contact set, FP64 with one)
     int fp32_stall_window = 40;  // mixed precision: iterations without the gate ratio halving before the rest of
                                  // the frame continues in FP64 (0: never)
     static Options parse(const std::map<std::string, double>& m);
@@ -121,6 +127,7 @@ public:
     void ws_apply(double dt, const double* d_base, const float* out, double* d_q_init, cudaStream_t st);
     void ws_target(double dt, const double* d_q_next, const double* d_base, float* Y, cudaStream_t st);
     double ws_dx() const;
+    double ws_lambda_scale(double dt) const;  // h^2 / (m dx): contact multipliers in the network's scale
     // Attach a trained warm-start network (device pointers; copied into engine memory) or detach (null): while
     // attached, every forward step whose caller gives no initial guess starts its PD loop from the network's
     // prediction.  The previous step's q and q_tilde are engine state (reset by reset_warm_start).
@@ -173,7 +180,10 @@ private:
     void run_forward_loop(const double* d_q, double h, const Options& o, cudaStream_t st,
                           const double* d_init = nullptr);
     void launch_ainv(bool fp32, cudaStream_t st, const double* x_base = nullptr);  // d_vperm -> d_xraw
-    void enqueue_pcg_iteration(bool fp32, cudaStream_t st, bool projected = false);
+    void enqueue_pcg_iteration(bool fp32, cudaStream_t st, bool projected = false, bool woodbury = false);
+    // x_raw = the contact-aware adjoint's preconditioner applied to the permuted S-pass input (P A^-1 P without
+    // the constrained-inverse correction, or the exact inverse of A on the constrained subspace with it)
+    void enqueue_contact_precond(bool fp32, bool woodbury, cudaStream_t st);
     void backward_core(const double* d_q_next, const double* d_gq, const double* d_gv, double dt, const Options& o,
                        double* d_dq, double* d_dv, double* d_df, double* d_dmat_w, double* d_dparams,
                        double* d_dstate_p, cudaStream_t st, const double* d_q, const double* d_v, const double* d_f);
@@ -186,6 +196,13 @@ private:
                      cudaStream_t st);
     void contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t st);
     DeviceBuffer d_wb_nodes, d_wb_dirs, d_wb_ndir, d_wb_count, d_wb_gath, d_wb_mu, d_cmp, d_rq, d_rv;
+    DeviceBuffer d_z1;  // constraint correction z - mu of the last contact-aware adjoint of a reverse sweep
+    // constrained-inverse preconditioner: per constrained node its candidate and its position in each direction's
+    // block, the block sizes, the blocks' inverse Cholesky factors, work vectors and the sparse S-pass input
+    DeviceBuffer d_wbp_cand, d_wbp_pos, d_wbp_nb, d_wbp_idx, d_wbp_X, d_wbp_M, d_wbp_u, d_wbp_w, d_wbp_lam;
+    DeviceBuffer d_vjac64, d_vjac32;
+    WbpDirs wbp_dirs_ = {};
+    int z_hist_ = 0;
     double* h_cmp_ = nullptr;
     void enqueue_contact_iteration(cudaStream_t st, bool f32);
     void enqueue_contact_iteration64(cudaStream_t st);
@@ -199,6 +216,7 @@ private:
     void check_device() const;
     int device_ = -1;
     int factor_mode_ = 0, small_subtree_max_ = 512;
+    bool proj32_ = true;  // precision of the projections captured in the mixed-precision iteration graphs
     bool factor_on_device_ = false;
     std::unique_ptr<SBuildPlan> sb_plan_;   // device build: plan and the permuted upper triangle of A, kept from
     std::unique_ptr<PermUpper> sb_upper_;   // the symbolic step until build_device runs the numeric one
@@ -211,7 +229,8 @@ private:
     double graph_dt_ = -1, graph_mu_ = 0;
     // 0 fwd64, 1 fwd mixed, 2 adjoint fixed point, 3/4 CG adjoint f64/f32, 5 contact f64, 6/7 projected CG
     // f64/f32, 8 contact mixed
-    static constexpr int kModes = 9;
+    // 9/10 projected CG f64/f32 with the constrained-inverse preconditioner
+    static constexpr int kModes = 11;
     cudaGraphExec_t graphs_[kModes] = {};
     size_t graph_nodes_[kModes] = {};
     bool graph_is_while_[kModes] = {};
@@ -252,6 +271,8 @@ private:
     int ws_which_ = 0;
     DeviceBuffer d_ws_master, d_ws_packed, d_ws_X, d_ws_out, d_ws_base0, d_ws_base1, d_ws_qprev, d_ws_qinit;
     DeviceBuffer d_ws_err;       // set by the tcgen05 inference kernel when a tensor-core wait gave up
+    DeviceBuffer d_ws_lamnode;   // node-indexed contact multipliers (the lambda feature)
+    bool ws_lambda_ = true;
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0;

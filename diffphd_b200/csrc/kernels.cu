@@ -1992,6 +1992,21 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap) {
     cudaGraphSetConditional(h, (!ctrl->done && loops < cap) ? 1u : 0u);
 }
 
+__global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += a * x[i];
+}
+__global__ void k_sub(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] - b[i];
+}
+void launch_axpy(int n, double a, const double* x, double* y, cudaStream_t st) {
+    if (n > 0) k_axpy<<<(n + 255) / 256, 256, 0, st>>>(n, a, x, y);
+}
+void launch_sub(int n, const double* a, const double* b, double* out, cudaStream_t st) {
+    if (n > 0) k_sub<<<(n + 255) / 256, 256, 0, st>>>(n, a, b, out);
+}
+
 void launch_loop_cond(cudaGraphConditionalHandle h, Ctrl* ctrl, int cap, cudaStream_t st) {
     k_loop_cond<<<1, 1, 0, st>>>(h, ctrl, cap);
 }

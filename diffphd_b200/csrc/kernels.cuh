@@ -195,6 +195,9 @@ void launch_pcg_update1(int n, double* mu, double* r, const double* p, const dou
 void launch_pcg_update2(int n3, const double* r, const double* z, double* part, const double* mu_part, int mu_blocks,
                         int blocks, Ctrl* ctrl, cudaStream_t st);
 void launch_pcg_p(int n3, double* p, const double* z, const Ctrl* ctrl, cudaStream_t st);
+// y += a x;  out = a - b
+void launch_axpy(int n, double a, const double* x, double* y, cudaStream_t st);
+void launch_sub(int n, const double* a, const double* b, double* out, cudaStream_t st);
 // out = 2 a - b (linear extrapolation of the last two adjoints for the next solve's start)
 void launch_extrapolate(int n3, const double* a, const double* b, double* out, cudaStream_t st);
 // out = 3 (a - b) + c (quadratic extrapolation of the last three adjoints)
@@ -233,6 +236,22 @@ struct ContactDev {
     double* Mwork = nullptr;         // active system, kcap x kcap capacity (kcap = K rounded up to 64)
     unsigned int* bar = nullptr;     // grid barrier of the NCP solve: count, generation, abort
 };
+// The preconditioner of the contact-aware adjoint (contact_precond.cu): the three unit directions of the
+// constraint basis, the parts of one application (stage 0: u = J A^-1 r from y = S r, lam = X^T X u per direction
+// block; stage 1: the S-pass input -J^T lam), and the set-up gather of G_b with an identity X_b.
+struct WbpDirs {
+    double d[3][3];
+};
+template <typename T>
+void launch_wbp_precond_parts(int stage, int cap, const int* count, const int* wcand, const int* wpos, const int* nb,
+                              const ContactDev& c, const WbpDirs& dirs, const T* y, int npad, const double* X, int ld,
+                              double* u, double* w, double* lam, const int* iperm, T* vjac, const Ctrl* ctrl,
+                              cudaStream_t st);
+void launch_wbp_gather_g(int n, int n_pad, const int* idx, const double* G, int K, double* M, double* X, int ldx,
+                         cudaStream_t st);
+// Dense Cholesky M = L L^T (n rows, a multiple of 64, identity-padded, ld n) with X <- L^-1 X (ldx, ncols), one
+// cooperative grid (sfactor_gpu.cu); throws on a barrier timeout or a non-positive pivot.
+void dense_chol_solve(double* M, int n, double* X, int ldx, int ncols, cudaStream_t st);
 // Side of the padded active-system capacity for K candidates (K rounded up to the 64 x 64 tile).
 size_t ncp_matrix_capacity(int K);
 int ncp_grid();
@@ -300,7 +319,13 @@ void mlp_adamw_flat(float* master, void* packed, const float* part, int nblocks,
                     float eps, float wd, int step, float* m, float* v, float* grad_out, float* loss_out,
                     cudaStream_t st);
 void launch_mlp_features(const FeatureArgs& a, const double* q, const double* qp, const double* v, const double* f,
-                         const double* prev_base, void* X, double* base, cudaStream_t st);
+                         const double* prev_base, const float* lam_node, void* X, double* base, cudaStream_t st);
+// contact multipliers <-> the network: node-indexed feature column, training target column 3 of Y [n][4], and the
+// predicted initial multipliers (scale = h^2 / (m dx))
+void launch_mlp_lambda_nodes(int n, int K, const int* cand, const double* lam, double scale, float* lam_node,
+                             cudaStream_t st);
+void launch_mlp_target_lambda(int K, const int* cand, const double* lam, double scale, float* Y, cudaStream_t st);
+void launch_mlp_lambda_apply(int K, const int* cand, const float* out, double inv_scale, double* lam, cudaStream_t st);
 void launch_mlp_apply(int n3, const double* base, const float* out, double dx, const unsigned char* fixed_dof,
                       const double* fval, double* q_init, cudaStream_t st);
 void launch_mlp_target(int n3, const double* q_next, const double* base, double inv_dx, float* Y, cudaStream_t st);

@@ -21,7 +21,7 @@
 
 namespace dphd {
 
-constexpr int kIn = 16, kHid = 128, kOut = 8, kOutUsed = 3;
+constexpr int kIn = 16, kHid = 128, kOut = 8, kOutUsed = 4;
 constexpr int kRowsPerCta = 128;
 // per-CTA gradient partial: W1 [16][128], W2 [128][128], W3 [128][8], b1, b2 [128], b3 [8], loss
 constexpr int kPartW1 = 0, kPartW2 = kPartW1 + kIn * kHid, kPartW3 = kPartW2 + kHid * kHid;
@@ -533,14 +533,15 @@ namespace dphd {
 
 namespace {
 
-// Per-node features (15 used of 16): displacement (q - X)/dx, last step (q - q_prev)/dx, the last step's
-// correction (q - q_tilde_prev)/dx (0 without a previous prediction), h^2/m f_ext/dx, height above the contact
-// plane /dx, log10 of the node's mean PD stiffness / 7, Dirichlet flag; also the inertial prediction
-// q_tilde = q + h v + h^2/m (f_ext + m g) (the warm start is q_tilde + dx * MLP).
+// Per-node features (16): displacement (q - X)/dx, last step (q - q_prev)/dx, the last step's correction
+// (q - q_tilde_prev)/dx (0 without a previous prediction), h^2/m f_ext/dx, height above the contact plane /dx,
+// log10 of the node's mean PD stiffness / 7, Dirichlet flag, and the node's current contact multiplier (the
+// previous frame's lambda) in the output's scale h^2/(m dx) (0 off the contact set); also the inertial
+// prediction q_tilde = q + h v + h^2/m (f_ext + m g) (the warm start is q_tilde + dx * MLP).
 __global__ void k_mlp_features(FeatureArgs a, const double* __restrict__ q, const double* __restrict__ qp,
                                const double* __restrict__ v, const double* __restrict__ f,
-                               const double* __restrict__ prev_base, __nv_bfloat16* __restrict__ X,
-                               double* __restrict__ base) {
+                               const double* __restrict__ prev_base, const float* __restrict__ lam_node,
+                               __nv_bfloat16* __restrict__ X, double* __restrict__ base) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     float feat[16];
@@ -559,7 +560,7 @@ __global__ void k_mlp_features(FeatureArgs a, const double* __restrict__ q, cons
                        : 0.f;
     feat[13] = a.wlog[i];
     feat[14] = a.fixed[i] ? 1.f : 0.f;
-    feat[15] = 0.f;
+    feat[15] = lam_node ? lam_node[i] : 0.f;
     for (int c = 0; c < 16; ++c) X[(size_t)i * 16 + c] = __float2bfloat16_rn(feat[c]);
 }
 
@@ -571,19 +572,59 @@ __global__ void k_mlp_apply(int n3, const double* __restrict__ base, const float
     q_init[k] = fixed_dof[k] ? fval[k] : base[k] + dx * (double)out[(size_t)(k / 3) * 8 + k % 3];
 }
 
+// Training targets, 4 per node: (q_next - q_tilde)/dx and the frame's contact multiplier in the scale h^2/(m dx)
+// (column 3: 0 here, the candidates' values are written by k_mlp_target_lambda after this kernel).
 __global__ void k_mlp_target(int n3, const double* __restrict__ q_next, const double* __restrict__ base,
                              double inv_dx, float* __restrict__ Y) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n3) return;
-    Y[k] = (float)((q_next[k] - base[k]) * inv_dx);
+    Y[(size_t)(k / 3) * 4 + k % 3] = (float)((q_next[k] - base[k]) * inv_dx);
+    if (k % 3 == 0) Y[(size_t)(k / 3) * 4 + 3] = 0.f;
+}
+
+__global__ void k_mlp_target_lambda(int K, const int* __restrict__ cand, const double* __restrict__ lam, double scale,
+                                    float* __restrict__ Y) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) Y[(size_t)cand[k] * 4 + 3] = (float)(lam[k] * scale);
+}
+
+// Node-indexed contact multipliers in the network's scale (the lambda feature): 0 off the candidate set.
+__global__ void k_mlp_lambda_zero(int n, float* __restrict__ lam_node) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) lam_node[i] = 0.f;
+}
+__global__ void k_mlp_lambda_scatter(int K, const int* __restrict__ cand, const double* __restrict__ lam, double scale,
+                                     float* __restrict__ lam_node) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) lam_node[cand[k]] = (float)(lam[k] * scale);
+}
+
+// The predicted initial contact multipliers: lambda_k = max(0, out[node_k][3]) / scale.
+__global__ void k_mlp_lambda_apply(int K, const int* __restrict__ cand, const float* __restrict__ out, double inv_scale,
+                                   double* __restrict__ lam) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const double v = (double)out[(size_t)cand[k] * 8 + 3];
+    lam[k] = v > 0.0 ? v * inv_scale : 0.0;
 }
 
 }  // namespace
 
 void launch_mlp_features(const FeatureArgs& a, const double* q, const double* qp, const double* v, const double* f,
-                         const double* prev_base, void* X, double* base, cudaStream_t st) {
-    k_mlp_features<<<(a.n + 255) / 256, 256, 0, st>>>(a, q, qp, v, f, prev_base, reinterpret_cast<__nv_bfloat16*>(X),
-                                                      base);
+                         const double* prev_base, const float* lam_node, void* X, double* base, cudaStream_t st) {
+    k_mlp_features<<<(a.n + 255) / 256, 256, 0, st>>>(a, q, qp, v, f, prev_base, lam_node,
+                                                      reinterpret_cast<__nv_bfloat16*>(X), base);
+}
+void launch_mlp_lambda_nodes(int n, int K, const int* cand, const double* lam, double scale, float* lam_node,
+                             cudaStream_t st) {
+    k_mlp_lambda_zero<<<(n + 255) / 256, 256, 0, st>>>(n, lam_node);
+    if (K > 0) k_mlp_lambda_scatter<<<(K + 255) / 256, 256, 0, st>>>(K, cand, lam, scale, lam_node);
+}
+void launch_mlp_target_lambda(int K, const int* cand, const double* lam, double scale, float* Y, cudaStream_t st) {
+    if (K > 0) k_mlp_target_lambda<<<(K + 255) / 256, 256, 0, st>>>(K, cand, lam, scale, Y);
+}
+void launch_mlp_lambda_apply(int K, const int* cand, const float* out, double inv_scale, double* lam, cudaStream_t st) {
+    if (K > 0) k_mlp_lambda_apply<<<(K + 255) / 256, 256, 0, st>>>(K, cand, out, inv_scale, lam);
 }
 void launch_mlp_apply(int n3, const double* base, const float* out, double dx, const unsigned char* fixed_dof,
                       const double* fval, double* q_init, cudaStream_t st) {

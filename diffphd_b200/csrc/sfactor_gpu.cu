@@ -442,6 +442,36 @@ void device_build_factor(const SBuildPlan& P, const std::vector<int>& lo, const 
     DPHD_CHECK(!(status & kSfbNotPositive), "PD matrix is not positive definite (device factor build)");
 }
 
+void dense_chol_solve(double* M, int n, double* X, int ldx, int ncols, cudaStream_t st) {
+    DPHD_CHECK(n % kT == 0, "dense_chol_solve: n must be a multiple of 64");
+    if (n == 0) return;
+    DeviceBuffer d_bar, d_status;
+    d_bar.alloc(4 * sizeof(unsigned int));
+    d_status.alloc(sizeof(int));
+    CUDA_OK(cudaMemsetAsync(d_bar.p, 0, d_bar.bytes, st));
+    CUDA_OK(cudaMemsetAsync(d_status.p, 0, sizeof(int), st));
+    const size_t chol_smem = (size_t)3 * kT * kLd * sizeof(double);
+    CUDA_OK(cudaFuncSetAttribute(k_sfb_chol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem));
+    const int nbw = n / kT, nxc = (ncols + kT - 1) / kT;
+    const int grid = std::max(1, std::min(device_sms(), nbw * std::max(nxc, 1)));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThr);
+    cfg.dynamicSmemBytes = chol_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_OK(cudaLaunchKernelEx(&cfg, k_sfb_chol, M, n, X, ldx, ncols, d_bar.as<unsigned int>(), d_status.as<int>()));
+    int status = 0;
+    CUDA_OK(cudaMemcpyAsync(&status, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    DPHD_CHECK(!(status & kSfbBarrierTimeout), "dense Cholesky: a grid barrier timed out");
+    DPHD_CHECK(!(status & kSfbNotPositive), "dense Cholesky: matrix is not positive definite");
+}
+
 void device_round_f32(const double* d_in, float* d_out, long long n, cudaStream_t st) {
     if (n <= 0) return;
     k_to_f32<<<4 * device_sms(), 256, 0, st>>>(d_in, d_out, n);

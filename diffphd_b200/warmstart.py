@@ -1,16 +1,18 @@
 """Learned warm start of the projective-dynamics fixed point.
 
-The reference starts every PD loop from the current positions q.  Here a per-node MLP (15 -> 128 -> 128 -> 3,
-GELU, BF16 tensor-core kernels with FP32 accumulation, diffphd_b200/csrc/mlp.cu) predicts the correction of the
-inertial prediction q_tilde = q + h v + h^2/m (f_ext + m g):
+The reference starts every PD loop from the current positions q and every NCP from the previous frame's contact
+multipliers.  Here a per-node MLP (16 -> 128 -> 128 -> 4, GELU, BF16 tensor-core kernels with FP32 accumulation,
+diffphd_b200/csrc/mlp.cu) predicts both: the correction of the inertial prediction
+q_tilde = q + h v + h^2/m (f_ext + m g) and, on the contact set, the frame's normal multiplier:
 
-    q_init = q_tilde + dx * MLP(features),     features per node (dphd_warmstart_features):
+    q_init = q_tilde + dx * MLP(features)[0:3],  lambda_init = max(0, MLP(features)[3]) * m dx / h^2,
+    features per node (dphd_warmstart_features):
         (q - X)/dx, (q - q_prev)/dx, (q - q_tilde_prev)/dx, h^2 f_ext/(m dx), height above the contact plane/dx,
-        log10(mean PD stiffness)/7, Dirichlet flag
+        log10(mean PD stiffness)/7, Dirichlet flag, the previous frame's multiplier * h^2/(m dx) (0 off contact)
 
 and the PD loop then runs from q_init to the same dual gate as the plain solver, so the network changes only
 the iteration count: a bad prediction costs iterations, never accuracy.  Training data are the plain solver's
-own rollouts (target (q_next - q_tilde)/dx); training runs on the GPU through the library's fused training
+own rollouts (targets (q_next - q_tilde)/dx and the frame's final multiplier * h^2/(m dx)); training runs on the GPU through the library's fused training
 kernel (forward, backward and weight gradients in one kernel, deterministic AdamW in a second).
 
     mlp = WarmStartMLP(device, seed=0)
@@ -39,7 +41,7 @@ def _sizes():
     return a.value, b.value, c.value, d.value
 
 
-N_IN, N_HID, N_OUT = 16, 128, 8
+N_IN, N_HID, N_OUT, N_USED = 16, 128, 8, 4
 
 
 class WarmStartMLP:
@@ -49,11 +51,10 @@ class WarmStartMLP:
         self.device = torch.device(device)
         self.n_master, self.n_packed, self.part_per_block, self.rows_per_block = _sizes()
         g = torch.Generator().manual_seed(int(seed))
-        W1 = torch.randn(N_IN, N_HID, generator=g, dtype=torch.float64) * math.sqrt(2.0 / 15.0)
-        W1[N_IN - 1] = 0
+        W1 = torch.randn(N_IN, N_HID, generator=g, dtype=torch.float64) * math.sqrt(2.0 / N_IN)
         W2 = torch.randn(N_HID, N_HID, generator=g, dtype=torch.float64) * math.sqrt(2.0 / N_HID)
         W3 = torch.randn(N_HID, N_OUT, generator=g, dtype=torch.float64) * (0.1 / math.sqrt(N_HID))
-        W3[:, 3:] = 0
+        W3[:, N_USED:] = 0
         flat = torch.cat([W1.ravel(), W2.ravel(), W3.ravel(), torch.zeros(2 * N_HID + N_OUT, dtype=torch.float64)])
         assert flat.numel() == self.n_master
         self.master = flat.to(torch.float32).to(self.device)
@@ -81,7 +82,7 @@ class WarmStartMLP:
         self.pack()
 
     def forward(self, X, out=None, tcgen05=True):
-        """X: BF16 [n][16] CUDA tensor -> FP32 [n][8] (columns 0..2 used).  tcgen05: the kernel on tcgen05 MMAs
+        """X: BF16 [n][16] CUDA tensor -> FP32 [n][8] (columns 0..3 used).  tcgen05: the kernel on tcgen05 MMAs
         with TMEM accumulators (dphd_mlp_forward_tc), else the mma.sync kernel (dphd_mlp_forward)."""
         n = X.shape[0]
         if out is None:
@@ -119,7 +120,7 @@ class WarmStartMLP:
         return self.loss_buf / n, grad
 
     def train_step(self, X, Y, lr, betas=(0.9, 0.999), eps=1e-8, weight_decay=1e-4, grad=None):
-        """One AdamW step on the rows X (BF16 [n][16]), Y (FP32 [n][3]); returns the mean loss (device tensor,
+        """One AdamW step on the rows X (BF16 [n][16]), Y (FP32 [n][4]); returns the mean loss (device tensor,
         before the update)."""
         n = X.shape[0]
         self.step_count += 1
@@ -186,7 +187,8 @@ class WarmStartStepper:
 
 def generate_dataset(make_scene, seeds, steps, device, options=None, method="pd_eigen_alg_phd", stream=0):
     """Rollouts of the plain solver (PD loop from q) on each seeded scene; per step and node the features and the
-    target (q_next - q_tilde)/dx.  Returns X (BF16 [N][16]) and Y (FP32 [N][3]) on `device`."""
+    targets (q_next - q_tilde)/dx and the frame's contact multiplier (scaled, 0 off the contact set).  Returns X
+    (BF16 [N][16]) and Y (FP32 [N][4]) on `device`."""
     Xs, Ys = [], []
     for seed in seeds:
         sc = make_scene(int(seed))
@@ -208,7 +210,7 @@ def generate_dataset(make_scene, seeds, steps, device, options=None, method="pd_
             base = bases[t % 2]
             d.warmstart_features(sc.dt, q, q_prev, v, f, prev_base, X, base, stream=stream)
             d.forward_device(method, q, v, f, sc.dt, opts, qn, vn, stream=stream)
-            Y = torch.empty(n3 // 3, 3, dtype=torch.float32, device=device)
+            Y = torch.empty(n3 // 3, N_USED, dtype=torch.float32, device=device)
             d.warmstart_target(sc.dt, qn, base, Y, stream=stream)
             Xs.append(X)
             Ys.append(Y)

@@ -21,7 +21,7 @@ import math
 
 import numpy as np
 
-N_IN, N_HID, N_OUT, N_USED = 16, 128, 8, 3
+N_IN, N_HID, N_OUT, N_USED = 16, 128, 8, 4
 OFF_W1 = 0
 OFF_W2 = OFF_W1 + N_IN * N_HID
 OFF_W3 = OFF_W2 + N_HID * N_HID
@@ -63,7 +63,7 @@ def unpack(master):
 
 
 def forward(master, X, emulate=True):
-    """Outputs [n][8] (columns 3..7 carry only b3) and the activations needed by the backward pass."""
+    """Outputs [n][8] (columns 4..7 carry only b3) and the activations needed by the backward pass."""
     W1, W2, W3, b1, b2, b3 = unpack(master)
     r = bf16 if emulate else (lambda a: np.asarray(a, dtype=np.float64))
     x = r(X)
@@ -76,7 +76,7 @@ def forward(master, X, emulate=True):
 
 
 def loss_and_grad(master, X, Y, emulate=True):
-    """loss = sum((out[:, :3] - Y)^2) / n and its gradient in the flat layout."""
+    """loss = sum((out[:, :4] - Y)^2) / n and its gradient in the flat layout."""
     W1, W2, W3, b1, b2, b3 = unpack(master)
     r = bf16 if emulate else (lambda a: np.asarray(a, dtype=np.float64))
     n = X.shape[0]

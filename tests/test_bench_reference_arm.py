@@ -24,4 +24,5 @@ def test_reference_arm_prints_the_contract_line():
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
-    assert line["config"]["workload"] == bench.WORKLOAD
+    assert line["config"]["workload"] == bench.WORKLOADS["contact64"]
+    assert line["steps"] == 1

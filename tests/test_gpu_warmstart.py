@@ -30,7 +30,7 @@ def _batch(n, seed=0):
     X = rng.standard_normal((n, 16))
     X[:, 15] = 0
     Xb = torch.as_tensor(X, dtype=torch.float32).to(torch.bfloat16).to(_dev())
-    Y = rng.standard_normal((n, 3)) * 0.2
+    Y = rng.standard_normal((n, 4)) * 0.2
     return Xb, torch.as_tensor(Y, dtype=torch.float32, device=_dev()), M.bf16(X), Y
 
 
@@ -93,15 +93,14 @@ def test_adamw_step_matches_oracle():
 
 
 def test_training_fits_a_smooth_map():
-    """Training through the fused kernels drives the loss of a smooth 15 -> 3 map down by an order of magnitude."""
+    """Training through the fused kernels drives the loss of a smooth 16 -> 4 map down by an order of magnitude."""
     import torch
     from diffphd_b200.warmstart import fit
     rng = np.random.default_rng(9)
     N = 60000
     X = rng.uniform(-1, 1, (N, 16))
-    X[:, 15] = 0
-    Y = np.stack([np.sin(2 * X[:, 0]) * X[:, 1], X[:, 2] ** 2 - X[:, 3], np.tanh(X[:, 4] + X[:, 5] * X[:, 6])],
-                 axis=1) * 0.1
+    Y = np.stack([np.sin(2 * X[:, 0]) * X[:, 1], X[:, 2] ** 2 - X[:, 3], np.tanh(X[:, 4] + X[:, 5] * X[:, 6]),
+                  np.maximum(X[:, 15], 0) * X[:, 7]], axis=1) * 0.1
     Xb = torch.as_tensor(X, dtype=torch.float32).to(torch.bfloat16).to(_dev())
     Yt = torch.as_tensor(Y, dtype=torch.float32, device=_dev())
     mlp = _mlp(10)
@@ -156,10 +155,11 @@ def test_features_base_and_target_kernels():
     assert np.array_equal(Xn[:, 14], exp[:, 14])
     assert np.all(Xn[:, 12] == 0) and np.all(Xn[:, 15] == 0)
     assert np.all(Xn[:, 13] > 0.5) and np.all(Xn[:, 13] < 1.1)  # log10(stiffness)/7 for 1e5..1e7 Pa
-    Y = torch.empty(nodes, 3, dtype=torch.float32, device=dev)
+    Y = torch.empty(nodes, 4, dtype=torch.float32, device=dev)
     d.warmstart_target(sc.dt, qn, base, Y)
-    np.testing.assert_allclose(Y.cpu().numpy().ravel(), ((qn.cpu().numpy() - base_ref) / dx).astype(np.float32),
-                               rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(Y.cpu().numpy()[:, :3].ravel(),
+                               ((qn.cpu().numpy() - base_ref) / dx).astype(np.float32), rtol=1e-6, atol=1e-7)
+    assert np.all(Y.cpu().numpy()[:, 3] == 0)  # no contact set: the multiplier target is zero
     # q_init = base + dx * out, Dirichlet dofs at their values
     out = torch.as_tensor(rng.standard_normal((nodes, 8)) * 0.1, dtype=torch.float32, device=dev)
     qi = torch.empty_like(q)

@@ -26,7 +26,7 @@ def test_fp64_gradient_matches_central_differences():
     n = 37
     X = rng.standard_normal((n, 16))
     X[:, 15] = 0.0
-    Y = rng.standard_normal((n, 3))
+    Y = rng.standard_normal((n, 4))
     p = _params(3)
     _, g = M.loss_and_grad(p, X, Y, emulate=False)
     used = M.used_mask()
@@ -87,7 +87,7 @@ def test_emulated_gradient_is_close_to_fp64():
     rng = np.random.default_rng(8)
     X = rng.standard_normal((300, 16))
     X[:, 15] = 0
-    Y = rng.standard_normal((300, 3)) * 0.1
+    Y = rng.standard_normal((300, 4)) * 0.1
     p = _params(9, 0.1)
     _, g64 = M.loss_and_grad(p, X, Y, emulate=False)
     _, g16 = M.loss_and_grad(p, X, Y, emulate=True)
