@@ -194,10 +194,14 @@ def train_warm_start(dev, args, workload):
     hist = fit(mlp, X, Y, steps=args.ws_fit_steps, batch=65536, lr=2e-3, log_every=max(1, args.ws_fit_steps - 1))
     torch.cuda.synchronize(dev)
     t2 = time.perf_counter()
+    # mean loss over a fixed sample of the rows after training (the last mini-batch's loss alone is noisy)
+    g = torch.Generator(device=X.device).manual_seed(1)
+    idx = torch.randint(0, X.shape[0], (min(262144, X.shape[0]),), device=X.device, generator=g)
+    eval_loss = float(mlp.gradient(X[idx].contiguous(), Y[idx].contiguous())[0])
     info = {"train_scene": make(seeds[0]).name + " (seeds %d..%d)" % (seeds[0], seeds[-1]),
             "rollout_steps_per_seed": args.ws_steps, "rows": int(X.shape[0]), "data_gen_s": round(t1 - t0, 2),
             "fit_s": round(t2 - t1, 2), "fit_steps": args.ws_fit_steps, "batch": 65536,
-            "loss_first_last": [h[1] for h in hist]}
+            "loss_first_last_batch": [h[1] for h in hist], "loss_after_fit_262k_rows": eval_loss}
     del X, Y
     return mlp, info
 
@@ -526,6 +530,42 @@ def run_ainv_only(args):
                       "stored_values": d.s_padded_values()}))
 
 
+def run_profile_step(args):
+    """Profiling mode: W untimed warm-up steps (FP64) of the workload, then one forward step and its adjoint in the
+    timed configuration (learned start excluded), inside the NVTX range "prof", with every iteration graph replayed
+    from the host so that each kernel is a separate launch a profiler can see."""
+    import torch
+    from diffphd_b200 import core
+    dev = torch.device("cuda", 0)
+    cells = tuple(args.cells) if args.cells else None
+    sc = build_scene(args.workload, cells)
+    d = core.from_scene(sc)
+    T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev).contiguous()
+    o64 = options(sc, "f64", host_loop=True)
+    o = options(sc, args.precision, warm=True, host_loop=True)
+    q, v, f = T(sc.q0), T(sc.v0), T(sc.f_ext)
+    for _ in range(args.warmup):
+        qn, vn = torch.empty_like(q), torch.empty_like(q)
+        d.forward_device(METHOD, q, v, f, sc.dt, o64, qn, vn)
+        q, v = qn, vn
+    g, z = T(np.ones(sc.dofs)), torch.zeros_like(q)
+    dq, dv, df = torch.empty_like(g), torch.empty_like(g), torch.empty_like(g)
+    # one untimed step of the profiled configuration first (its graphs are captured outside the range)
+    qn, vn = torch.empty_like(q), torch.empty_like(q)
+    d.forward_device(METHOD, q, v, f, sc.dt, o, qn, vn)
+    d.backward_device(METHOD, qn, g, z, sc.dt, o, dq, dv, df)
+    torch.cuda.synchronize()
+    d.reset_frame_stats()
+    torch.cuda.nvtx.range_push("prof")
+    d.forward_device(METHOD, q, v, f, sc.dt, o, qn, vn)
+    d.backward_device(METHOD, qn, g, z, sc.dt, o, dq, dv, df)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"workload": sc.name, "precision": args.precision, "pd_iters": d.frame_stats()[0].tolist(),
+                      "adjoint_iters": d._L.dphd_last_backward_iters(d._h),
+                      "contact_adjoint": d.contact_adjoint_stats()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -533,11 +573,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="contact64", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="mixed", choices=["f64", "mixed"], help="--ainv-reps mode only")
-    ap.add_argument("--cells", type=int, nargs=3, help="--ainv-reps mode: grid of the contact workload")
+    ap.add_argument("--precision", default="mixed", choices=["f64", "mixed"],
+                    help="--ainv-reps / --profile-step modes only")
+    ap.add_argument("--cells", type=int, nargs=3, help="--ainv-reps / --profile-step modes: grid of the contact workload")
     ap.add_argument("--ainv-reps", type=int, default=0,
                     help="profiling mode: only apply the S^T S pair this many times on the workload")
     ap.add_argument("--ablation", action="store_true", help="also time mixed precision without the warm starts")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="profiling mode: one forward step + adjoint (host-replayed graphs) in the NVTX range 'prof'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true", help="headline without the learned / adjoint starts")
     ap.add_argument("--host-loop", action="store_true",
@@ -551,6 +594,9 @@ def main():
         args.warmup = 3
     if args.ainv_reps > 0:
         run_ainv_only(args)
+        return
+    if args.profile_step:
+        run_profile_step(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

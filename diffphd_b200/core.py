@@ -76,7 +76,9 @@ def load_library():
     L.dphd_kernel_launches.argtypes = [C.c_void_p]
     L.dphd_kernel_launches.restype = C.c_longlong
     L.dphd_device.argtypes = [C.c_void_p]
+    L.dphd_debug_set_mma_wait_polls.argtypes = [C.c_longlong]
     L.dphd_fp64_escalations.argtypes = [C.c_void_p]
+    L.dphd_backward_fallbacks.argtypes = [C.c_void_p]
     L.dphd_debug_set_factor_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.dphd_factor_built_on_device.argtypes = [C.c_void_p]
     L.dphd_s_padded_values.argtypes = [C.c_void_p]
@@ -343,6 +345,10 @@ class Deformable:
 
     def factor_built_on_device(self):
         return int(self._L.dphd_factor_built_on_device(self._h)) == 1
+
+    def backward_fallbacks(self):
+        """Adjoint solves that fell back from CG (to the fixed point, or to the unconstrained adjoint)."""
+        return int(self._L.dphd_backward_fallbacks(self._h))
 
     def fp64_escalations(self):
         """Mixed-precision frames that finished in FP64 after the FP32 iteration stalled."""

@@ -377,6 +377,9 @@ int dphd_reset_warm_start(dphd_deformable* h) {
     return guard([&] { E(h).reset_warm_start(); });
 }
 
+int dphd_debug_set_mma_wait_polls(long long polls) {
+    return guard([&] { dphd::set_mma_wait_polls(polls); });
+}
 int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_max) {
     return guard([&] { E(h).set_factor_build(mode, small_subtree_max); });
 }
@@ -429,6 +432,7 @@ int dphd_reset_frame_stats(dphd_deformable* h) {
         E(h).stats.frame_converged.clear();
     });
 }
+int dphd_backward_fallbacks(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.bwd_fallbacks : -1; }
 int dphd_fp64_escalations(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.fp64_escalations : -1; }
 int dphd_last_backward_iters(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.last_bwd_iters : -1; }
 int dphd_last_filtered_samples(const dphd_deformable* h) {

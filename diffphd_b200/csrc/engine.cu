@@ -56,6 +56,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.bwd_cascade_cap = (int)get("bwd_cascade_cap", 1);
     o.bwd_eigen_filter = (int)get("bwd_eigen_filter", 0);
     o.bwd_contact_precond = (int)get("bwd_contact_precond", 1);
+    o.debug_force_bwd_fallback = (int)get("debug_force_bwd_fallback", 0);
     o.fp32_bulk = (int)get("fp32_bulk", 0);
     o.bwd_solver = (int)get("alg_phd_bwd_solver", 0);
     o.bwd_warm_start = (int)get("alg_phd_bwd_warm_start", 0);
@@ -1100,11 +1101,11 @@ static void init_ctrl(Ctrl* h, int mode, const Options& o, int max_iter, double 
 }
 
 void Engine::check_status(const char* where) {
+    if (h_ctrl_->status & kStatusNonFinite)  // first: a NaN input can also trip the singular-F test
+        throw Error(std::string(where) + ": non-finite PD iterate (NaN or Inf in q, v, f_ext or the solve)");
     if (h_ctrl_->status & kStatusSingularF) throw Error("Singular F.");
     if (h_ctrl_->status & kStatusBarrierTimeout)
         throw Error(std::string(where) + ": the contact solve's grid barrier timed out (CTAs not co-resident)");
-    if (h_ctrl_->status & kStatusNonFinite)
-        throw Error(std::string(where) + ": non-finite PD iterate (NaN or Inf in q, v, f_ext or the solve)");
 }
 
 void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st,
@@ -1723,8 +1724,9 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
         launch_pcg_p(n3, d_pp.as<double>(), d_xraw.as<double>(), c, st);
         launches_ += 8;
         run_iterations(f32 ? 4 : 3, o, st);
-        if (h_ctrl_->status & kStatusIndefinite) {
-            // negative curvature of (A - K_pd): fall back to the reference fixed point for this step
+        if ((h_ctrl_->status & kStatusIndefinite) || o.debug_force_bwd_fallback) {
+            // negative curvature of (A - K_pd): fall back to the reference fixed point for this step (the debug
+            // option takes this path without the curvature test failing, for the failure-path tests)
             init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);
             CUDA_OK(cudaMemcpyAsync(c, h_ctrl_, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
             CUDA_OK(cudaMemsetAsync(d_x.p, 0, n3 * sizeof(double), st));

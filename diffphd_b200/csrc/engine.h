@@ -32,6 +32,7 @@ struct Options {
     int bwd_mean_stiffness = 0;  // reference backward semantics: mean stiffness inside K_pd
     int bwd_cascade_cap = 1;     // reference cap of the injected adjoint at |g_bar| + 1
     int bwd_eigen_filter = 0;    // 0 off (exact adjoint), 1 clamp, 2 abs
+    int debug_force_bwd_fallback = 0;  // take the CG -> fixed-point fallback path (failure-path tests)
     int bwd_contact_precond = 1; // contact-aware adjoint preconditioner: 1 exact inverse of A on the constrained
                                  // subspace (Woodbury with the Delassus block), 0 P A^-1 P
     int fp32_bulk = 0;           // projection and S/S^T SpMVs in FP32

@@ -314,6 +314,9 @@ void mlp_forward_flat(float* master, void* packed, const void* X, int n, float* 
 // Same network on tcgen05 MMAs (mlp_tc.cu): BF16 operands in shared memory, FP32 accumulators in TMEM; *err is
 // set to 1 when a completion wait gave up (the outputs of that CTA's remaining rows are then not written).
 void mlp_forward_tc_flat(float* master, void* packed, const void* X, int n, float* out, int* err, cudaStream_t st);
+// Bound (polls) of the tcgen05 kernel's completion waits (0: every wait gives up at once); < 0 restores the
+// default (4M).  Process-wide.
+void set_mma_wait_polls(long long polls);
 int mlp_train_flat(float* master, void* packed, const void* X, const float* Y, int n, float* part, cudaStream_t st);
 void mlp_adamw_flat(float* master, void* packed, const float* part, int nblocks, float lr, float b1, float b2,
                     float eps, float wd, int step, float* m, float* v, float* grad_out, float* loss_out,

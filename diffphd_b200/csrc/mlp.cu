@@ -536,7 +536,7 @@ namespace {
 // Per-node features (16): displacement (q - X)/dx, last step (q - q_prev)/dx, the last step's correction
 // (q - q_tilde_prev)/dx (0 without a previous prediction), h^2/m f_ext/dx, height above the contact plane /dx,
 // log10 of the node's mean PD stiffness / 7, Dirichlet flag, and the node's current contact multiplier (the
-// previous frame's lambda) in the output's scale h^2/(m dx) (0 off the contact set); also the inertial
+// previous frame's lambda) in the output's scale h^2/(m dx), clipped at 4 (0 off the contact set); also the inertial
 // prediction q_tilde = q + h v + h^2/m (f_ext + m g) (the warm start is q_tilde + dx * MLP).
 __global__ void k_mlp_features(FeatureArgs a, const double* __restrict__ q, const double* __restrict__ qp,
                                const double* __restrict__ v, const double* __restrict__ f,
@@ -555,8 +555,10 @@ __global__ void k_mlp_features(FeatureArgs a, const double* __restrict__ q, cons
         feat[6 + d] = prev_base ? (float)((q[k] - prev_base[k]) * a.inv_dx) : 0.f;
         feat[9 + d] = (float)(a.h2m * f[k] * a.inv_dx);
     }
-    feat[12] = a.plane ? (float)((a.pn[0] * q[3 * i] + a.pn[1] * q[3 * i + 1] + a.pn[2] * q[3 * i + 2] + a.poff) *
-                                 a.inv_dx)
+    // height above the contact plane in cells, clamped to [-2, 2]: only the layer next to the plane is told apart
+    // (unclamped, the feature would grow with the body's size and leave the training range on larger meshes)
+    feat[12] = a.plane ? fminf(2.f, fmaxf(-2.f, (float)((a.pn[0] * q[3 * i] + a.pn[1] * q[3 * i + 1] +
+                                                         a.pn[2] * q[3 * i + 2] + a.poff) * a.inv_dx)))
                        : 0.f;
     feat[13] = a.wlog[i];
     feat[14] = a.fixed[i] ? 1.f : 0.f;
@@ -572,6 +574,10 @@ __global__ void k_mlp_apply(int n3, const double* __restrict__ base, const float
     q_init[k] = fixed_dof[k] ? fval[k] : base[k] + dx * (double)out[(size_t)(k / 3) * 8 + k % 3];
 }
 
+// The scaled multipliers are clipped at kLamClip in the feature and the target: impact frames reach tens of the
+// resting values, and a few such rows would dominate the squared loss of a warm start.
+constexpr double kLamClip = 4.0;
+
 // Training targets, 4 per node: (q_next - q_tilde)/dx and the frame's contact multiplier in the scale h^2/(m dx)
 // (column 3: 0 here, the candidates' values are written by k_mlp_target_lambda after this kernel).
 __global__ void k_mlp_target(int n3, const double* __restrict__ q_next, const double* __restrict__ base,
@@ -585,7 +591,7 @@ __global__ void k_mlp_target(int n3, const double* __restrict__ q_next, const do
 __global__ void k_mlp_target_lambda(int K, const int* __restrict__ cand, const double* __restrict__ lam, double scale,
                                     float* __restrict__ Y) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < K) Y[(size_t)cand[k] * 4 + 3] = (float)(lam[k] * scale);
+    if (k < K) Y[(size_t)cand[k] * 4 + 3] = (float)fmin(lam[k] * scale, kLamClip);
 }
 
 // Node-indexed contact multipliers in the network's scale (the lambda feature): 0 off the candidate set.
@@ -596,7 +602,7 @@ __global__ void k_mlp_lambda_zero(int n, float* __restrict__ lam_node) {
 __global__ void k_mlp_lambda_scatter(int K, const int* __restrict__ cand, const double* __restrict__ lam, double scale,
                                      float* __restrict__ lam_node) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < K) lam_node[cand[k]] = (float)(lam[k] * scale);
+    if (k < K) lam_node[cand[k]] = (float)fmin(lam[k] * scale, kLamClip);
 }
 
 // The predicted initial contact multipliers: lambda_k = max(0, out[node_k][3]) / scale.

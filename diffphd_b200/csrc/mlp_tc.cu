@@ -85,8 +85,8 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    for (long long i = 0; i < kWaitPolls; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, long long polls) {
+    for (long long i = 0; i < polls; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const __nv_bfloat16* __r
                                                         const float* __restrict__ b1, const float* __restrict__ b2,
                                                         const float* __restrict__ b3,
                                                         const __nv_bfloat16* __restrict__ X, int n,
-                                                        float* __restrict__ out, int* __restrict__ err) {
+                                                        float* __restrict__ out, int* __restrict__ err,
+                                                        long long wait_polls) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     SmemTc& s = *reinterpret_cast<SmemTc*>(smem_raw);
     const int t = threadIdx.x, warp = t >> 5;
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const __nv_bfloat16* __r
     // Waits for the MMAs committed to the barrier; the result is made CTA-uniform before any .sync.aligned
     // tcgen05.ld depends on it.
     auto wait_mma = [&]() -> bool {
-        const bool r = __syncthreads_and(mbar_wait(mbar, phase));
+        const bool r = __syncthreads_and(mbar_wait(mbar, phase, wait_polls));
         phase ^= 1u;
         fence_after_sync();
         return r;
@@ -286,7 +287,11 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const __nv_bfloat16* __r
         }
         // the next tile's X write and barrier (publish) order these TMEM reads before its layer-1 MMA
     }
-    if (!ok && t == 0) atomicExch(err, 1);
+    if (!ok) {
+        if (t == 0) atomicExch(err, 1);
+        // the MMAs of the wait that gave up may still be in flight: drain them (the full bound) before TMEM goes
+        __syncthreads_and(mbar_wait(mbar, phase ^ 1u, kWaitPolls));
+    }
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
@@ -303,6 +308,9 @@ static_assert(make_idesc(128, 128) == ((1u << 4) | (1u << 7) | (1u << 10) | (16u
 
 size_t mlp_tc_smem() { return sizeof(SmemTc) + 1024; }
 
+long long g_mma_wait_polls = kWaitPolls;  // bound of the completion waits (lowered only by a failure-path test)
+void set_mma_wait_polls(long long polls) { g_mma_wait_polls = polls >= 0 ? polls : kWaitPolls; }
+
 void launch_mlp_forward_tc(const void* W1T, const void* W2T, const void* W3T, const float* b1, const float* b2,
                            const float* b3, const void* X, int n, float* out, int* err, int max_ctas,
                            cudaStream_t st) {
@@ -314,7 +322,7 @@ void launch_mlp_forward_tc(const void* W1T, const void* W2T, const void* W3T, co
     k_mlp_forward_tc<<<grid, 128, smem, st>>>(
         reinterpret_cast<const __nv_bfloat16*>(W1T), reinterpret_cast<const __nv_bfloat16*>(W2T),
         reinterpret_cast<const __nv_bfloat16*>(W3T), b1, b2, b3, reinterpret_cast<const __nv_bfloat16*>(X), n, out,
-        err);
+        err, g_mma_wait_polls);
 }
 
 }  // namespace dphd

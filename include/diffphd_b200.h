@@ -102,6 +102,11 @@ int dphd_reset_warm_start(dphd_deformable* h);
 
 /* Number of kernels this library launched on the GPU since the handle was created (graph nodes included). */
 long long dphd_kernel_launches(const dphd_deformable* h);
+/* Bound, in polls, of the completion waits of the tcgen05 warm-start inference kernel (default 4M; 0 makes every
+ * wait give up at once; < 0 restores the default; process-wide).  A wait that runs out sets the kernel's error flag, drains the MMAs in flight, frees its
+ * TMEM and returns; the forward step then fails with an error.  For failure-path tests.  No counterpart in the
+ * reference. */
+int dphd_debug_set_mma_wait_polls(long long polls);
 /* Where the sparse-inverse factor S is built (the reference builds it on the host from an LDL^T and uploads it,
  * forward_gpu.cpp:593-764): 0 automatic (on the device when S has more than 32 Mi values, else on the host),
  * 1 host, 2 device (rows of etree subtrees of at most small_subtree_max nodes, 512 when <= 0, on the host; every
@@ -126,6 +131,10 @@ int dphd_last_backward_iters(const dphd_deformable* h);
  * the FP32 iterate, since the handle was created (option fp32_stall_window: iterations without the gate ratio
  * halving, default 40; 0 never switches).  No counterpart in the reference. */
 int dphd_fp64_escalations(const dphd_deformable* h);
+/* Adjoint solves that left the conjugate-gradient solver for the reference fixed point (negative curvature of
+ * A - K_pd) or, in the contact-aware solve, for the unconstrained adjoint, since the handle was created.  No
+ * counterpart in the reference. */
+int dphd_backward_fallbacks(const dphd_deformable* h);
 /* Samples whose 9x9 local Hessian the last backward call eigen-filtered (option bwd_eigen_filter 1 clamp /
  * 2 absolute value; the diagonal-dominance test of ProjectedNewtonMatrix, deformable_newton_forward.cpp:394-434). */
 int dphd_last_filtered_samples(const dphd_deformable* h);

@@ -79,3 +79,26 @@ def test_host_factor_matches_oracle_solve(oracle_lib, builder):
     xr[sc.dirichlet_dofs] = 0.0
     assert np.abs(x - xr).max() <= 1e-11 * np.abs(xr).max()
     assert d.s_nnz() > sc.n
+
+
+def test_malformed_and_truncated_mesh_files_are_rejected(tmp_path):
+    """The .bin reader (the reference's Mesh::Initialize, cpp/core/src/mesh/mesh.cpp:4-31) rejects a file with the
+    wrong header and a file cut short, with an error instead of reading past the data."""
+    import shutil
+    from pathlib import Path
+    gold = Path(__file__).resolve().parent / "golden" / "ref_hex_16x4x4.bin"
+    bad = tmp_path / "bad_header.bin"
+    data = bytearray(gold.read_bytes())
+    data[0:4] = (7).to_bytes(4, "little")  # vertex dimension 7
+    bad.write_bytes(bytes(data))
+    cut = tmp_path / "truncated.bin"
+    cut.write_bytes(gold.read_bytes()[: len(data) // 2])
+    ok = tmp_path / "ok.bin"
+    shutil.copy(gold, ok)
+    for path, msg in ((bad, "Corrupted mesh file"), (cut, "mesh"), (tmp_path / "missing.bin", "Cannot open")):
+        d = core.HexDeformable()
+        with pytest.raises(RuntimeError, match=msg):
+            d.Initialize(str(path), 1e3, "none", 1e6, 0.45)
+    d = core.HexDeformable()
+    d.Initialize(str(ok), 1e3, "none", 1e6, 0.45)
+    assert d.dofs() == 3 * 425

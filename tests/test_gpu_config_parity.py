@@ -1,0 +1,167 @@
+"""Parity at the configured sizes (not shrunken meshes), through the C ABI, against the FP64 oracle.
+
+  * the 32x16x16 Neo-Hookean tet block (40,960 tets) for 20 steps with the bench's options -- FP32 bulk, learned
+    PD warm start, adjoint warm start, Anderson window 5, the 1e-6 dual gate -- against the oracle's FP64 rollout
+    and reverse sweep at the same gate: relative position error <= 1e-6 after the rollout and gradient error
+    <= 1e-4 (the target's criteria);
+  * the 16x4x4 cantilever (425 nodes) for 100 steps: gradients w.r.t. q0, v0 and the per-element Young's moduli
+    (through the Lame chain of the per-element energy parameters) against central differences with eps 1e-7;
+  * the 24^3 contact drop (rotated block, Coulomb mu 0.5, every node a candidate) for 24 steps in FP64: the same
+    contact set as the oracle at every step;
+  * the reference's own backward (mean stiffness inside K_pd, deformable_projective_dynamics_backward.cpp:37-44,
+    option bwd_mean_stiffness) against the oracle in the same mode.
+"""
+import numpy as np
+import pytest
+
+from diffphd_b200 import core, scenes
+
+pytestmark = pytest.mark.gpu
+
+METHOD = "pd_eigen_alg_phd"
+
+
+def _T(a, dev):
+    import torch
+    return torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev).contiguous()
+
+
+def test_tet_block_bench_options_match_the_fp64_oracle(oracle_lib):
+    import torch
+    from diffphd_b200.warmstart import WarmStartMLP, fit, generate_dataset
+    dev = torch.device("cuda:0")
+    steps = 20
+    sc = scenes.nh_tet_block(steps=steps)  # 32 x 16 x 16 cells, 9,537 nodes
+    base = dict(sc.options, thread_ct=16)
+    mixed = dict(base, fp32_bulk=1, alg_phd_bwd_solver=1, alg_phd_bwd_warm_start=3)
+    # a briefly trained warm-start network (held-out material seeds), attached as in the bench
+    X, Y = generate_dataset(lambda s: scenes.nh_tet_block(seed=s), [1, 2], 8, dev, options=base)
+    mlp = WarmStartMLP(dev, seed=0)
+    fit(mlp, X, Y, steps=300, batch=32768, lr=2e-3)
+    d = core.from_scene(sc)
+    d.set_warm_start_network(mlp)
+    qs, vs = [_T(sc.q0, dev)], [_T(sc.v0, dev)]
+    f = _T(sc.f_ext, dev)
+    for _ in range(steps):
+        qn, vn = torch.empty_like(qs[0]), torch.empty_like(qs[0])
+        d.forward_device(METHOD, qs[-1], vs[-1], f, sc.dt, mixed, qn, vn)
+        qs.append(qn)
+        vs.append(vn)
+    assert np.all(d.frame_stats()[1] == 1)
+    r = sc.extra["loss_r"]
+    gq, gv = _T(r, dev), torch.zeros_like(qs[0])
+    gpar = np.zeros(d.NumOfPdParams())
+    dpar = torch.empty(d.NumOfPdParams(), dtype=torch.float64, device=dev)
+    for i in reversed(range(steps)):
+        dq, dv, df = torch.empty_like(gq), torch.empty_like(gq), torch.empty_like(gq)
+        d.backward_device(METHOD, qs[i + 1], gq, gv, sc.dt, mixed, dq, dv, df, dl_dparams=dpar)
+        gpar += dpar.cpu().numpy()
+        gq, gv = dq, dv
+    o = oracle_lib.OracleDeformable.from_scene(sc)
+    q, v = sc.q0.copy(), sc.v0.copy()
+    oq, ov = [q], [v]
+    for _ in range(steps):
+        q, v, _ = o.forward(q, v, sc.f_ext, sc.dt, base)
+        oq.append(q)
+        ov.append(v)
+    q_gpu = qs[-1].cpu().numpy()
+    pos_err = np.linalg.norm(q_gpu - oq[-1]) / np.linalg.norm(oq[-1])
+    disp_err = np.linalg.norm(q_gpu - oq[-1]) / np.linalg.norm(oq[-1] - sc.q0)
+    print(f"tet block 20 steps: position error {pos_err:.2e} (of the displacement {disp_err:.2e})")
+    assert pos_err <= 1e-6
+    g, g_v = r.copy(), np.zeros(sc.dofs)
+    opar = np.zeros(d.NumOfPdParams())
+    for i in reversed(range(steps)):
+        out = o.backward(oq[i], ov[i], sc.f_ext, sc.dt, oq[i + 1], g, g_v, base)
+        opar += np.concatenate(out["dl_dparams"])
+        g, g_v = out["dl_dq"], out["dl_dv"]
+    for name, a, b in (("dl_dq0", gq.cpu().numpy(), g), ("dl_dv0", gv.cpu().numpy(), g_v), ("dl_dparams", gpar, opar)):
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        print(f"  {name}: relative error {err:.2e}")
+        assert err <= 1e-4, (name, err)
+
+
+def _cantilever_loss(sim, sc, q0, v0, params, steps):
+    import torch
+    from diffphd_b200.autograd import Rollout
+    dev = q0.device
+    qT, _ = Rollout.apply(sim, q0, v0, params, _T(sc.f_ext, dev), steps, 10)
+    return (qT * _T(sc.extra["loss_r"], dev)).sum()
+
+
+def test_cantilever_100_steps_gradients_match_central_differences():
+    import torch
+    from diffphd_b200.autograd import DiffSim
+    dev = torch.device("cuda:0")
+    sc = scenes.cantilever(steps=100, heterogeneous=True)  # 16 x 4 x 4 hex cells, per-element E
+    opts = dict(sc.options, rel_tol=1e-12, abs_tol=1e-14, max_pd_iter=5000, alg_phd_bwd_solver=1)
+    sim = DiffSim(sc, opts)
+    q0 = _T(sc.q0, dev).requires_grad_(True)
+    v0 = _T(sc.v0, dev).requires_grad_(True)
+    p0 = sim.default_params().to(dev).requires_grad_(True)
+    L = _cantilever_loss(sim, sc, q0, v0, p0, sc.steps)
+    L.backward()
+    gq0, gv0, gp = q0.grad.cpu().numpy(), v0.grad.cpu().numpy(), p0.grad.cpu().numpy()
+    sizes = sim.sizes
+    dE, _ = scenes.chain_material_grad(sc, np.split(gp, np.cumsum(sizes)[:-1]))
+    rng = np.random.default_rng(3)
+    free = np.ones(sc.dofs, bool)
+    free[sc.dirichlet_dofs] = False
+    eps = 1e-7
+    with torch.no_grad():
+        def loss(q0n=sc.q0, v0n=sc.v0, E=sc.youngs):
+            params = np.concatenate([np.atleast_1d(p) for _, p, _ in scenes.energy_params_from_material(sc, E)])
+            return float(_cantilever_loss(sim, sc, _T(q0n, dev), _T(v0n, dev), _T(params, dev), sc.steps))
+        for name, grad, direction, fn in (
+                ("v0", gv0, rng.standard_normal(sc.dofs) * free, lambda t, dv: loss(v0n=sc.v0 + t * dv)),
+                ("q0", gq0, rng.standard_normal(sc.dofs) * free * 1e-3, lambda t, dq: loss(q0n=sc.q0 + t * dq)),
+                ("E", dE, rng.standard_normal(sc.m) * sc.youngs, lambda t, de: loss(E=sc.youngs + t * de))):
+            fd = (fn(eps, direction) - fn(-eps, direction)) / (2 * eps)
+            an = float(grad @ direction)
+            print(f"cantilever 100 steps, d/d{name}: adjoint {an:.9e}  FD {fd:.9e}")
+            assert abs(an - fd) <= 1e-4 * abs(fd), (name, an, fd)
+
+
+def test_contact_drop_24_cubed_has_the_oracles_contact_sets(oracle_lib):
+    sc = scenes.contact_drop(height=0.002, steps=24)  # 24^3 hex block, 15,625 candidates
+    opts = dict(sc.options, thread_ct=16)
+    d = core.from_scene(sc)
+    o = oracle_lib.OracleDeformable.from_scene(sc)
+    q, v = sc.q0.copy(), sc.v0.copy()
+    qo, vo = sc.q0.copy(), sc.v0.copy()
+    contact_steps = 0
+    for t in range(sc.steps):
+        qn, vn = np.zeros(sc.dofs), np.zeros(sc.dofs)
+        act = d.PyForward(METHOD, q, v, [], sc.f_ext, sc.dt, opts, qn, vn, [])
+        q, v = qn, vn
+        qo, vo, act_o = o.forward(qo, vo, sc.f_ext, sc.dt, opts)
+        lam = d.contact_lambda().cpu().numpy()
+        mine = set(np.asarray(sc.plane[1])[lam > 0].tolist())
+        assert mine == set(act_o.tolist()), (t, len(mine), len(act_o))
+        contact_steps += bool(mine)
+        assert np.linalg.norm(q - qo) / np.linalg.norm(qo) <= 1e-6
+    assert contact_steps >= 20
+    assert np.all(d.frame_stats()[1] == 1)
+
+
+def test_reference_mean_stiffness_backward_matches_the_oracle(oracle_lib):
+    sc = scenes.cantilever(cells=(8, 2, 2), dx=0.02, steps=1, heterogeneous=True)
+    opts = dict(sc.options, aa_window=0, rel_tol=1e-12, abs_tol=1e-14, max_pd_iter=5000, bwd_mean_stiffness=1)
+    d = core.from_scene(sc)
+    qn, vn = np.zeros(sc.dofs), np.zeros(sc.dofs)
+    d.PyForward(METHOD, sc.q0, sc.v0, [], sc.f_ext, sc.dt, opts, qn, vn, [])
+    g = np.random.default_rng(4).standard_normal(sc.dofs)
+    o = oracle_lib.OracleDeformable.from_scene(sc)
+    qo, _, _ = o.forward(sc.q0, sc.v0, sc.f_ext, sc.dt, opts)
+    for solver in (0, 1):
+        out = d.backward(METHOD, sc.q0, sc.v0, [], sc.f_ext, sc.dt, qn, vn, [], g, 0 * g,
+                         dict(opts, alg_phd_bwd_solver=solver))
+        ref = o.backward(sc.q0, sc.v0, sc.f_ext, sc.dt, qo, g, 0 * g, opts)
+        for k in ("dl_dq", "dl_dv", "dl_df_ext"):
+            assert np.abs(out[k] - ref[k]).max() <= 1e-7 * np.abs(ref[k]).max(), (solver, k)
+        a, b = np.asarray(out["dl_dparams"]).ravel(), np.concatenate(ref["dl_dparams"])
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), solver
+        # the mean-stiffness adjoint is not the exact one: it differs from the default (per-element) adjoint
+        exact = d.backward(METHOD, sc.q0, sc.v0, [], sc.f_ext, sc.dt, qn, vn, [], g, 0 * g,
+                           dict(opts, bwd_mean_stiffness=0, alg_phd_bwd_solver=solver))
+        assert np.abs(exact["dl_dv"] - out["dl_dv"]).max() > 1e-6 * np.abs(out["dl_dv"]).max()
