@@ -25,10 +25,11 @@ from . import core
 class DiffSim:
     """A scene whose PD energy parameters can be replaced by a tensor (per-element materials)."""
 
-    def __init__(self, scene, options=None, method="pd_eigen_alg_phd"):
+    def __init__(self, scene, options=None, method="pd_eigen_alg_phd", warm_start_network=None):
         self.scene = scene
         self.options = dict(options or scene.options)
         self.method = method
+        self.warm_start_network = warm_start_network  # attached to every deformable this object builds
         self._d = None
         self._params = None
         self.sizes = [int(np.size(p)) for _, p, _ in scene.energies]
@@ -51,6 +52,8 @@ class DiffSim:
             d.AddStateForce("gravity", sc.gravity)
         if sc.plane is not None:
             d.SetFrictionalBoundary("planar", sc.plane[0], sc.plane[1])
+        if self.warm_start_network is not None:
+            d.set_warm_start_network(self.warm_start_network)
         self._d, self._params = d, params.copy()
         return d
 
@@ -72,12 +75,15 @@ class Rollout(torch.autograd.Function):
         q, v = q0.detach().contiguous(), v0.detach().contiguous()
         f = f_ext.detach().contiguous()
         k = max(1, int(checkpoint_every))
-        # a checkpoint holds (q, v) and the contact multipliers that warm-start the next frame's NCP
-        ckpts = {0: (q.clone(), v.clone(), d.contact_lambda(stream=stream).clone())}
+        # a checkpoint holds (q, v), the contact multipliers that warm-start the next frame's NCP and the learned
+        # start's previous-step state, so that a recomputed segment repeats the forward pass bit for bit
+        def snapshot():
+            return (q.clone(), v.clone(), d.contact_lambda(stream=stream).clone(), d.warm_start_state(stream=stream))
+        ckpts = {0: snapshot()}
         for t in range(steps):
             q, v = _step(d, sim, q, v, f, stream)
             if (t + 1) % k == 0 and t + 1 < steps:
-                ckpts[t + 1] = (q.clone(), v.clone(), d.contact_lambda(stream=stream).clone())
+                ckpts[t + 1] = snapshot()
         ctx.sim, ctx.steps, ctx.k, ctx.p_np = sim, steps, k, p_np
         ctx.ckpts = ckpts
         ctx.save_for_backward(f)
@@ -99,9 +105,11 @@ class Rollout(torch.autograd.Function):
         starts = sorted(ctx.ckpts)
         for s in reversed(starts):
             e = min(s + k, steps)
-            # recompute the segment's states from its checkpoint (and its contact multipliers)
-            q, v, lam = ctx.ckpts[s]
+            # recompute the segment's states from its checkpoint (its contact multipliers and learned-start state
+            # included); the adjoint history of the later segments is kept: it warm-starts this segment's solves
+            q, v, lam, ws = ctx.ckpts[s]
             d.set_contact_lambda(lam, stream=stream)
+            d.set_warm_start_state(ws, stream=stream)
             qs = [q]
             for _ in range(s, e):
                 q, v = _step(d, sim, q, v, f, stream)

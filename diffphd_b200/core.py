@@ -78,6 +78,7 @@ def load_library():
     L.dphd_device.argtypes = [C.c_void_p]
     L.dphd_debug_set_mma_wait_polls.argtypes = [C.c_longlong]
     L.dphd_fp64_escalations.argtypes = [C.c_void_p]
+    L.dphd_warm_start_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_void_p]
     L.dphd_backward_fallbacks.argtypes = [C.c_void_p]
     L.dphd_debug_set_factor_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.dphd_factor_built_on_device.argtypes = [C.c_void_p]
@@ -345,6 +346,21 @@ class Deformable:
 
     def factor_built_on_device(self):
         return int(self._L.dphd_factor_built_on_device(self._h)) == 1
+
+    def warm_start_state(self, stream=0):
+        """(valid, 2*3n float64 CUDA tensor): the learned start's previous-step state (for checkpoints)."""
+        import torch
+        buf = torch.zeros(2 * self.dofs(), dtype=torch.float64, device="cuda")
+        valid = C.c_int(0)
+        self._check(self._L.dphd_warm_start_state(self._h, C.c_void_p(buf.data_ptr()), C.byref(valid), 0,
+                                                  C.c_void_p(int(stream))))
+        return valid.value, buf
+
+    def set_warm_start_state(self, state, stream=0):
+        valid, buf = state
+        v = C.c_int(int(valid))
+        self._check(self._L.dphd_warm_start_state(self._h, C.c_void_p(buf.data_ptr()), C.byref(v), 1,
+                                                  C.c_void_p(int(stream))))
 
     def backward_fallbacks(self):
         """Adjoint solves that fell back from CG (to the fixed point, or to the unconstrained adjoint)."""

@@ -1233,6 +1233,26 @@ void Engine::set_s_units(bool on) {
 
 double Engine::ws_dx() const { return std::pow(M.vol, 1.0 / 3.0); }
 
+void Engine::ws_state(double* d_buf, int* valid, bool set, cudaStream_t st) {
+    const size_t n3 = (size_t)3 * M.n;
+    DPHD_CHECK(d_buf && valid, "warm-start state: null pointer");
+    if (!set) {
+        *valid = ws_prev_valid_ ? 1 : 0;
+        if (ws_prev_valid_) {
+            CUDA_OK(cudaMemcpyAsync(d_buf, d_ws_qprev.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            const DeviceBuffer& pb = ws_which_ ? d_ws_base0 : d_ws_base1;  // the next step's prev_base
+            CUDA_OK(cudaMemcpyAsync(d_buf + n3, pb.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        }
+        return;
+    }
+    ws_prev_valid_ = *valid != 0;
+    if (!ws_prev_valid_) return;
+    for (DeviceBuffer* b : {&d_ws_qprev, &d_ws_base0, &d_ws_base1}) b->alloc(n3 * sizeof(double));
+    CUDA_OK(cudaMemcpyAsync(d_ws_qprev.p, d_buf, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    DeviceBuffer& pb = ws_which_ ? d_ws_base0 : d_ws_base1;
+    CUDA_OK(cudaMemcpyAsync(pb.p, d_buf + n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+}
+
 void Engine::set_ws_net(const float* d_master, const void* d_packed) {
     if (!d_master) {
         ws_net_ = false;

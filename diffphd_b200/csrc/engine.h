@@ -137,6 +137,10 @@ public:
     int contact_candidates() const;
     void contact_lambda_device(double* d_buf, bool set, cudaStream_t st);
     bool ws_net_attached() const { return ws_net_; }
+    // the learned start's frame-to-frame state (whether a previous step exists, its q and its q_tilde): copied to
+    // (set = false) or from (set = true) a device array of 2 * 3n doubles, so that a checkpointed rollout can
+    // recompute a segment exactly as the forward pass ran it
+    void ws_state(double* d_buf, int* valid, bool set, cudaStream_t st);
     // selects the row-group or the one-warp-per-item kernel of the FP32 y = S v pass (overriding the choice
     // timed at factor build); drops the captured iteration graphs
     void set_s_units(bool on);

@@ -127,6 +127,11 @@ int dphd_num_frames(const dphd_deformable* h);
 int dphd_frame_stats(const dphd_deformable* h, int* frame_iters, int* frame_converged);
 int dphd_reset_frame_stats(dphd_deformable* h);
 int dphd_last_backward_iters(const dphd_deformable* h);
+/* The learned start's frame-to-frame state: *valid (a previous step exists) and, when valid, the previous step's
+ * q and q_tilde in d_buf (device, 2 * 3n FP64), copied out (set = 0) or restored (set = 1) on `stream`.  A
+ * checkpointed rollout saves it with each checkpoint (with the contact multipliers) so that recomputing a segment
+ * repeats the forward pass exactly.  No counterpart in the reference. */
+int dphd_warm_start_state(dphd_deformable* h, double* d_buf, int* valid, int set, void* stream);
 /* Mixed-precision forward frames (option fp32_bulk) whose FP32 iteration stalled and that finished in FP64 from
  * the FP32 iterate, since the handle was created (option fp32_stall_window: iterations without the gate ratio
  * halving, default 40; 0 never switches).  No counterpart in the reference. */

@@ -93,3 +93,30 @@ def test_checkpointed_contact_rollout_is_exact():
     for g in grads[1:]:
         for a, b in zip(g, grads[0]):
             assert np.array_equal(a, b)
+
+
+def test_checkpointed_rollout_with_learned_start_recomputes_exactly():
+    """With a warm-start network attached, every checkpoint also holds the learned start's previous-step state, so
+    recomputed segments repeat the forward pass bit for bit: gradients are identical for every checkpoint
+    interval."""
+    import torch
+    from diffphd_b200.autograd import DiffSim
+    from diffphd_b200.warmstart import WarmStartMLP
+    sc = scenes.cantilever(cells=(4, 2, 2), dx=0.02, steps=7, heterogeneous=True)
+    opts = dict(sc.options)
+    opts.update(rel_tol=1e-8, abs_tol=1e-12, max_pd_iter=2000)
+    dev = torch.device("cuda")
+    sim = DiffSim(sc, opts, warm_start_network=WarmStartMLP(dev, seed=4))
+    T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev)
+    r = T(np.random.default_rng(8).standard_normal(sc.dofs))
+    grads = []
+    for ck in (1, 3, 7):
+        q0 = T(sc.q0).requires_grad_(True)
+        v0 = T(sc.v0).requires_grad_(True)
+        params = sim.default_params().to("cuda").requires_grad_(True)
+        L = _loss(sim, sc, T, q0, v0, params, T(sc.f_ext), r, ck)
+        L.backward()
+        grads.append((float(L), v0.grad.cpu().numpy(), params.grad.cpu().numpy()))
+    for g in grads[1:]:
+        assert g[0] == grads[0][0]
+        assert np.array_equal(g[1], grads[0][1]) and np.array_equal(g[2], grads[0][2])
