@@ -532,8 +532,8 @@ def run_ainv_only(args):
 
 def run_profile_step(args):
     """Profiling mode: W untimed warm-up steps (FP64) of the workload, then one forward step and its adjoint in the
-    timed configuration (learned start excluded), inside the NVTX range "prof", with every iteration graph replayed
-    from the host so that each kernel is a separate launch a profiler can see."""
+    timed configuration (learned start excluded), inside the NVTX ranges "prof_fwd" and "prof_bwd", with every
+    iteration graph replayed from the host so that each kernel is a separate launch a profiler can see."""
     import torch
     from diffphd_b200 import core
     dev = torch.device("cuda", 0)
@@ -556,8 +556,11 @@ def run_profile_step(args):
     d.backward_device(METHOD, qn, g, z, sc.dt, o, dq, dv, df)
     torch.cuda.synchronize()
     d.reset_frame_stats()
-    torch.cuda.nvtx.range_push("prof")
+    torch.cuda.nvtx.range_push("prof_fwd")
     d.forward_device(METHOD, q, v, f, sc.dt, o, qn, vn)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.nvtx.range_push("prof_bwd")
     d.backward_device(METHOD, qn, g, z, sc.dt, o, dq, dv, df)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
@@ -580,7 +583,8 @@ def main():
                     help="profiling mode: only apply the S^T S pair this many times on the workload")
     ap.add_argument("--ablation", action="store_true", help="also time mixed precision without the warm starts")
     ap.add_argument("--profile-step", action="store_true",
-                    help="profiling mode: one forward step + adjoint (host-replayed graphs) in the NVTX range 'prof'")
+                    help="profiling mode: one forward step + adjoint (host-replayed graphs) in the NVTX ranges "
+                         "'prof_fwd' and 'prof_bwd'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true", help="headline without the learned / adjoint starts")
     ap.add_argument("--host-loop", action="store_true",

@@ -16,7 +16,8 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libdiffphd_b200.so"
 SOURCES = ["kernels.cu", "engine.cu", "setup.cpp", "capi.cpp", "noalloc.cu", "contact.cu", "mlp.cu", "mlp_tc.cu",
-           "sfactor_plan.cpp", "sfactor_gpu.cu", "contact_precond.cu"]
+           "sfactor_plan.cpp", "sfactor_gpu.cu", "contact_precond.cu",
+           "ncp_cached.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

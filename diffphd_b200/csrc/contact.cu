@@ -310,13 +310,20 @@ k_ncp_block_solve(ContactDev c, const double* __restrict__ q0, const int* __rest
                     sB[r * kNcpLd + l] = Pg[(size_t)r * ld + l];
                 }
                 __syncthreads();
-                if (tid < kNcpTile) {
+                if (tid < kNcpTile) {  // row tid: x L_kk^T = m, four independent partial sums per dot
                     double* row = sB + tid * kNcpLd;
                     for (int j = 0; j < kNcpTile; ++j) {
-                        double x = row[j];
                         const double* Lj = sA + j * kNcpLd;
-                        for (int l = 0; l < j; ++l) x -= row[l] * Lj[l];
-                        row[j] = x / Lj[j];
+                        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                        int l = 0;
+                        for (; l + 4 <= j; l += 4) {
+                            s0 += row[l] * Lj[l];
+                            s1 += row[l + 1] * Lj[l + 1];
+                            s2 += row[l + 2] * Lj[l + 2];
+                            s3 += row[l + 3] * Lj[l + 3];
+                        }
+                        for (; l < j; ++l) s0 += row[l] * Lj[l];
+                        row[j] = (row[j] - ((s0 + s1) + (s2 + s3))) / Lj[j];
                     }
                 }
                 __syncthreads();
@@ -382,9 +389,14 @@ k_ncp_block_solve(ContactDev c, const double* __restrict__ q0, const int* __rest
                 if (tid < kNcpTile) {
                     const double* Li = M + (size_t)(i * kNcpTile + tid) * ld + kb * kNcpTile;
                     const double* y = rhs + kb * kNcpTile;
-                    double s = 0.0;
-                    for (int k = 0; k < kNcpTile; ++k) s += Li[k] * y[k];
-                    rhs[i * kNcpTile + tid] -= s;
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    for (int k = 0; k < kNcpTile; k += 4) {
+                        s0 += Li[k] * y[k];
+                        s1 += Li[k + 1] * y[k + 1];
+                        s2 += Li[k + 2] * y[k + 2];
+                        s3 += Li[k + 3] * y[k + 3];
+                    }
+                    rhs[i * kNcpTile + tid] -= (s0 + s1) + (s2 + s3);
                 }
             }
         }
@@ -416,9 +428,14 @@ k_ncp_block_solve(ContactDev c, const double* __restrict__ q0, const int* __rest
             for (int p = bid; p < kb; p += G) {
                 if (tid < kNcpTile) {
                     const double* Lkp = M + (size_t)kb * kNcpTile * ld + p * kNcpTile + tid;
-                    double s = 0.0;
-                    for (int i = 0; i < kNcpTile; ++i) s += Lkp[(size_t)i * ld] * sy[i];
-                    rhs[p * kNcpTile + tid] -= s;
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    for (int i = 0; i < kNcpTile; i += 4) {
+                        s0 += Lkp[(size_t)i * ld] * sy[i];
+                        s1 += Lkp[(size_t)(i + 1) * ld] * sy[i + 1];
+                        s2 += Lkp[(size_t)(i + 2) * ld] * sy[i + 2];
+                        s3 += Lkp[(size_t)(i + 3) * ld] * sy[i + 3];
+                    }
+                    rhs[p * kNcpTile + tid] -= (s0 + s1) + (s2 + s3);
                 }
             }
         }
@@ -528,6 +545,10 @@ void launch_ncp_iteration(const ContactDev& c, const double* x, const T* y, int 
                           cudaStream_t st) {
     k_ncp_prepare<<<1, 1024, 0, st>>>(c, x, ctrl);
     k_ncp_ainvb<T><<<(c.K * 32 + 255) / 256, 256, 0, st>>>(c, y, npad, x_base, ctrl);
+    if (c.cached) {
+        launch_ncp_cached_solve<T>(c, q0, iperm, vcon, npad, r64, ctrl, st);
+        return;
+    }
     // one cooperative grid of one CTA per SM (the barrier needs every CTA resident)
     const size_t smem = (size_t)(2 * kNcpTile * kNcpLd + kNcpTile) * sizeof(double);
     static bool attr_set[2] = {false, false};

@@ -69,21 +69,40 @@ __global__ void __launch_bounds__(256) k_wbp_trmv(const int* __restrict__ nb, co
     if (lane == 0) w[(size_t)b * cap + i] = s;
 }
 
-// lam_b = X_b^T w_b; one thread per column (coalesced over the columns of each row).
-__global__ void __launch_bounds__(256) k_wbp_trmvt(const int* __restrict__ nb, const double* __restrict__ X, int ld,
+// lam_b = X_b^T w_b from the stored transpose Xt_b (row j holds column j of X_b from its diagonal on); one warp
+// per row.
+__global__ void __launch_bounds__(256) k_wbp_trmvt(const int* __restrict__ nb, const double* __restrict__ Xt, int ld,
                                                    const double* __restrict__ w, double* __restrict__ lam, int cap,
                                                    const Ctrl* ctrl) {
     if (ctrl->done) return;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = (int)(t / cap), j = (int)(t % cap);
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int b = (int)(gw / cap), j = (int)(gw % cap);
     if (b >= 3) return;
     const int n = nb[b];
     if (j >= n) return;
-    const double* Xb = X + (size_t)b * ld * ld;
+    const double* Xj = Xt + (size_t)b * ld * ld + (size_t)j * ld;
     const double* wb = w + (size_t)b * cap;
     double s = 0.0;
-    for (int i = j; i < n; ++i) s += Xb[(size_t)i * ld + j] * wb[i];
-    lam[(size_t)b * cap + j] = s;
+    for (int i = j + lane; i < n; i += 32) s += Xj[i] * wb[i];
+    s = wsum(s);
+    if (lane == 0) lam[(size_t)b * cap + j] = s;
+}
+
+// Xt = the transpose of the lower triangle of X (n x n, leading dimension ld), 32 x 32 tiles through shared memory.
+__global__ void k_wbp_transpose(int n, const double* __restrict__ X, double* __restrict__ Xt, int ld) {
+    __shared__ double tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // source rows by.., columns bx..
+    if (bx > by + 31) return;                              // entirely above the diagonal: nothing to copy
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = by + r, j = bx + threadIdx.x;
+        tile[r][threadIdx.x] = (i < n && j < n && j <= i) ? X[(size_t)i * ld + j] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = bx + r, j = by + threadIdx.x;  // destination row i (= source column), column j (= source row)
+        if (i < n && j < n && j >= i) Xt[(size_t)i * ld + j] = tile[threadIdx.x][r];
+    }
 }
 
 // The S-pass input -J^T lam at the constrained nodes (the vector is zero elsewhere).
@@ -125,10 +144,11 @@ void launch_wbp_precond_parts(int stage, int cap, const int* count, const int* w
                               double* u, double* w, double* lam, const int* iperm, T* vjac, const Ctrl* ctrl,
                               cudaStream_t st) {
     if (cap <= 0) return;
-    if (stage == 0) {  // u = J A^-1 r, lam = (J A^-1 J^T)^-1 u
+    if (stage == 0) {  // u = J A^-1 r, lam = (J A^-1 J^T)^-1 u (X: three blocks, then their three transposes)
+        const double* Xt = X + (size_t)3 * ld * ld;
         k_wbp_jdot<T><<<(cap * 32 + 255) / 256, 256, 0, st>>>(count, wcand, wpos, c, y, npad, dirs, cap, u, ctrl);
         k_wbp_trmv<<<(unsigned)(((long long)3 * cap * 32 + 255) / 256), 256, 0, st>>>(nb, X, ld, u, w, cap, ctrl);
-        k_wbp_trmvt<<<(3 * cap + 255) / 256, 256, 0, st>>>(nb, X, ld, w, lam, cap, ctrl);
+        k_wbp_trmvt<<<(unsigned)(((long long)3 * cap * 32 + 255) / 256), 256, 0, st>>>(nb, Xt, ld, w, lam, cap, ctrl);
     } else {  // the S-pass input -J^T lam
         k_wbp_scatter<T><<<(cap + 255) / 256, 256, 0, st>>>(count, wcand, wpos, c, dirs, cap, lam, iperm, vjac, npad,
                                                              ctrl);
@@ -142,6 +162,12 @@ template void launch_wbp_precond_parts<float>(int, int, const int*, const int*, 
                                               const ContactDev&, const WbpDirs&, const float*, int, const double*,
                                               int, double*, double*, double*, const int*, float*, const Ctrl*,
                                               cudaStream_t);
+
+void launch_wbp_transpose(int n, const double* X, double* Xt, int ld, cudaStream_t st) {
+    if (n <= 0) return;
+    const int nt = (n + 31) / 32;
+    k_wbp_transpose<<<dim3(nt, nt), dim3(32, 8), 0, st>>>(n, X, Xt, ld);
+}
 
 void launch_wbp_gather_g(int n, int n_pad, const int* idx, const double* G, int K, double* M, double* X, int ldx,
                          cudaStream_t st) {

@@ -71,7 +71,8 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.ws_tcgen05 = (int)get("ws_tcgen05", 1);
     o.fp32_stall_window = std::max(0, (int)get("fp32_stall_window", 40));
     o.fp32_projection = (int)get("fp32_projection", -1);
-    o.ws_lambda = (int)get("ws_lambda", 1);
+    o.ws_lambda = (int)get("ws_lambda", 0);
+    o.ncp_solver = (int)get("ncp_solver", 1);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -697,6 +698,14 @@ void Engine::build_contact(double dt) {
     }
     dc_bar.alloc(4 * sizeof(unsigned int));
     CUDA_OK(cudaMemset(dc_bar.p, 0, dc_bar.bytes));
+    dc_Xinv.alloc(kcap * kcap * sizeof(double));
+    dc_Xt.alloc(kcap * kcap * sizeof(double));
+    dc_pcg.alloc((4 * kcap + 1024) * sizeof(double));
+    dc_actref.alloc((size_t)K * sizeof(int));
+    dc_flags.alloc(4 * sizeof(int));
+    CUDA_OK(cudaMemset(dc_flags.p, 0, dc_flags.bytes));
+    dc_stats.alloc(2 * sizeof(unsigned long long));
+    CUDA_OK(cudaMemset(dc_stats.p, 0, dc_stats.bytes));
     dc_act.alloc((size_t)K * sizeof(int));
     dc_kact.alloc(sizeof(int));
     CUDA_OK(cudaMemset(dc_kact.p, 0, sizeof(int)));
@@ -721,6 +730,20 @@ void Engine::build_contact(double dt) {
     c.Mwork = dc_M.as<double>();
     c.xsol = dc_xsol.as<double>();
     c.bar = dc_bar.as<unsigned int>();
+    c.kcap = kcap;
+    c.Xinv = dc_Xinv.as<double>();
+    c.Xt = dc_Xt.as<double>();
+    c.pcg = dc_pcg.as<double>();
+    c.act_ref = dc_actref.as<int>();
+    c.ncp_flags = dc_flags.as<int>();
+    c.ncp_stats = dc_stats.as<unsigned long long>();
+}
+
+void Engine::ncp_stats(long long* cached, long long* refactors) {
+    unsigned long long h[2] = {0, 0};
+    if (has_contact_ && dc_stats.p) CUDA_OK(cudaMemcpy(h, dc_stats.p, sizeof(h), cudaMemcpyDeviceToHost));
+    *cached = (long long)h[0];
+    *refactors = (long long)h[1];
 }
 
 void Engine::reset_warm_start() {
@@ -1133,6 +1156,14 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
     }
     if (has_contact_) {
         contact_.mu = o.friction_mu;
+        if ((o.ncp_solver != 0) != (contact_.cached != 0)) {  // the NCP solver is captured in the contact graphs
+            contact_.cached = o.ncp_solver != 0 ? 1 : 0;
+            for (int md : {5, 8})
+                if (graphs_[md]) {
+                    cudaGraphExecDestroy(graphs_[md]);
+                    graphs_[md] = nullptr;
+                }
+        }
         CUDA_OK(cudaMemsetAsync(dc_lt1.p, 0, dc_lt1.bytes, st));
         CUDA_OK(cudaMemsetAsync(dc_lt2.p, 0, dc_lt2.bytes, st));
         if (graph_mu_ != o.friction_mu)  // the friction coefficient is captured in the contact iteration graphs
@@ -1340,6 +1371,8 @@ void Engine::ws_features(double dt, const double* dq, const double* dqp, const d
     a.poff = M.plane_off;
     const float* lam_node = nullptr;
     if (has_contact_ && dc_lam.p) {  // the current multipliers (the previous frame's) as the 16th feature
+        d_ws_lamprev.alloc((size_t)contact_.K * sizeof(double));  // kept for the training target's change
+        CUDA_OK(cudaMemcpyAsync(d_ws_lamprev.p, dc_lam.p, d_ws_lamprev.bytes, cudaMemcpyDeviceToDevice, st));
         d_ws_lamnode.alloc((size_t)M.n * sizeof(float));
         launch_mlp_lambda_nodes(M.n, contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), ws_lambda_scale(dt),
                                 d_ws_lamnode.as<float>(), st);
@@ -1363,8 +1396,11 @@ void Engine::ws_target(double dt, const double* d_q_next, const double* d_base, 
     ensure_built(dt, 0);
     launch_mlp_target(dofs(), d_q_next, d_base, 1.0 / ws_dx(), Y, st);
     launches_ += 1;
-    if (has_contact_ && dc_lam.p) {  // the frame's final multipliers (the last forward call's) as column 3
-        launch_mlp_target_lambda(contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), ws_lambda_scale(dt), Y, st);
+    if (has_contact_ && dc_lam.p) {  // column 3: the multipliers' change over the frame (final - at the features)
+        const double* prev = d_ws_lamprev.bytes == (size_t)contact_.K * sizeof(double) ? d_ws_lamprev.as<double>()
+                                                                                        : nullptr;
+        launch_mlp_target_lambda(contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), prev, ws_lambda_scale(dt), Y,
+                                 st);
         launches_ += 1;
     }
 }
@@ -1574,7 +1610,7 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
         d_wbp_pos.alloc((size_t)3 * K * sizeof(int));
         d_wbp_nb.alloc(3 * sizeof(int));
         d_wbp_idx.alloc((size_t)3 * K * sizeof(int));
-        d_wbp_X.alloc(3 * ld * ld * sizeof(double));
+        d_wbp_X.alloc(6 * ld * ld * sizeof(double));  // the three X_b, then their transposes
         d_wbp_M.alloc(ld * ld * sizeof(double));
         for (DeviceBuffer* b : {&d_wbp_u, &d_wbp_w, &d_wbp_lam}) b->alloc((size_t)3 * K * sizeof(double));
         DeviceBuffer& vj = f32 ? d_vjac32 : d_vjac64;
@@ -1593,6 +1629,7 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
             double* Xb = d_wbp_X.as<double>() + (size_t)b * ld * ld;
             launch_wbp_gather_g(nb[b], npd, db_idx, dc_G.as<double>(), K, d_wbp_M.as<double>(), Xb, (int)ld, st);
             dense_chol_solve(d_wbp_M.as<double>(), npd, Xb, (int)ld, npd, st);  // X_b = L_b^-1
+            launch_wbp_transpose(nb[b], Xb, d_wbp_X.as<double>() + (size_t)(3 + b) * ld * ld, (int)ld, st);
         }
         launches_ += 4;
     }

@@ -44,8 +44,11 @@ struct Options {
     int poll_chunk = 8;
     int graph_while = 1;         // device-side WHILE graph per solve (0: host polling every poll_chunk iterations)
     int ws_tcgen05 = 1;          // warm-start inference on tcgen05 MMAs with TMEM accumulators (0: mma.sync)
-    int ws_lambda = 1;           // with a warm-start network and contact: start each frame's NCP from the
-                                 // network's predicted multipliers instead of the previous frame's
+    int ncp_solver = 1;          // NCP dense solve: 1 CG preconditioned by a cached factor (refactored when the
+                                 // active list changes or CG stalls), 0 a fresh Cholesky every PD iteration
+    int ws_lambda = 0;           // with a warm-start network and contact: 1 starts each frame's NCP from the
+                                 // network's predicted multipliers instead of the previous frame's (measured
+                                 // slower on the 64^3 contact rollout, so off by default)
     int fp32_projection = -1;    // mixed precision: 1 FP32 local projections, 0 FP64 projections with FP32 S
                                  // passes, -1 automatic (FP32 without a contact set, FP64 with one)
     int fp32_stall_window = 40;  // mixed precision: iterations without the gate ratio halving before the rest of
@@ -136,6 +139,8 @@ public:
     // contact candidates and their normal multipliers (the lambda warm start carried across frames)
     int contact_candidates() const;
     void contact_lambda_device(double* d_buf, bool set, cudaStream_t st);
+    // NCP solves by the cached factor and refactorisations since the contact set-up
+    void ncp_stats(long long* cached, long long* refactors);
     bool ws_net_attached() const { return ws_net_; }
     // the learned start's frame-to-frame state (whether a previous step exists, its q and its q_tilde): copied to
     // (set = false) or from (set = true) a device array of 2 * 3n doubles, so that a checkpointed rollout can
@@ -277,10 +282,12 @@ private:
     DeviceBuffer d_ws_master, d_ws_packed, d_ws_X, d_ws_out, d_ws_base0, d_ws_base1, d_ws_qprev, d_ws_qinit;
     DeviceBuffer d_ws_err;       // set by the tcgen05 inference kernel when a tensor-core wait gave up
     DeviceBuffer d_ws_lamnode;   // node-indexed contact multipliers (the lambda feature)
+    DeviceBuffer d_ws_lamprev;   // the multipliers at the last features call (the training target's baseline)
     bool ws_lambda_ = true;
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
-        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0;
+        dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0, dc_Xinv, dc_Xt, dc_pcg,
+        dc_actref, dc_flags, dc_stats;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

@@ -235,7 +235,21 @@ struct ContactDev {
     double* xsol = nullptr;          // kcap: the solution dlambda of the active system
     double* Mwork = nullptr;         // active system, kcap x kcap capacity (kcap = K rounded up to 64)
     unsigned int* bar = nullptr;     // grid barrier of the NCP solve: count, generation, abort
+    // cached-factor solve (ncp_cached.cu): kcap = padded capacity; X = L_ref^-1 (lower) and its transpose for the
+    // active list act_ref; CG work vectors and per-CTA partials; flags (factor valid, its ka, list differs);
+    // stats (solves by the cached factor, refactorisations)
+    size_t kcap = 0;
+    double* Xinv = nullptr;
+    double* Xt = nullptr;
+    double* pcg = nullptr;
+    int* act_ref = nullptr;
+    int* ncp_flags = nullptr;
+    unsigned long long* ncp_stats = nullptr;
+    int cached = 1;                  // 1: the cached-factor solve, 0: a fresh factorisation every PD iteration
 };
+template <typename T>
+void launch_ncp_cached_solve(const ContactDev& c, const double* q0, const int* iperm, T* vcon, int npad,
+                             const double* r64, Ctrl* ctrl, cudaStream_t st);
 // The preconditioner of the contact-aware adjoint (contact_precond.cu): the three unit directions of the
 // constraint basis, the parts of one application (stage 0: u = J A^-1 r from y = S r, lam = X^T X u per direction
 // block; stage 1: the S-pass input -J^T lam), and the set-up gather of G_b with an identity X_b.
@@ -249,6 +263,8 @@ void launch_wbp_precond_parts(int stage, int cap, const int* count, const int* w
                               cudaStream_t st);
 void launch_wbp_gather_g(int n, int n_pad, const int* idx, const double* G, int K, double* M, double* X, int ldx,
                          cudaStream_t st);
+// Xt = transpose of the lower triangle of X (n x n, leading dimension ld)
+void launch_wbp_transpose(int n, const double* X, double* Xt, int ld, cudaStream_t st);
 // Dense Cholesky M = L L^T (n rows, a multiple of 64, identity-padded, ld n) with X <- L^-1 X (ldx, ncols), one
 // cooperative grid (sfactor_gpu.cu); throws on a barrier timeout or a non-positive pivot.
 void dense_chol_solve(double* M, int n, double* X, int ldx, int ncols, cudaStream_t st);
@@ -327,7 +343,8 @@ void launch_mlp_features(const FeatureArgs& a, const double* q, const double* qp
 // predicted initial multipliers (scale = h^2 / (m dx))
 void launch_mlp_lambda_nodes(int n, int K, const int* cand, const double* lam, double scale, float* lam_node,
                              cudaStream_t st);
-void launch_mlp_target_lambda(int K, const int* cand, const double* lam, double scale, float* Y, cudaStream_t st);
+void launch_mlp_target_lambda(int K, const int* cand, const double* lam, const double* lam_prev, double scale,
+                              float* Y, cudaStream_t st);
 void launch_mlp_lambda_apply(int K, const int* cand, const float* out, double inv_scale, double* lam, cudaStream_t st);
 void launch_mlp_apply(int n3, const double* base, const float* out, double dx, const unsigned char* fixed_dof,
                       const double* fval, double* q_init, cudaStream_t st);

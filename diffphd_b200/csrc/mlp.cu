@@ -588,10 +588,14 @@ __global__ void k_mlp_target(int n3, const double* __restrict__ q_next, const do
     if (k % 3 == 0) Y[(size_t)(k / 3) * 4 + 3] = 0.f;
 }
 
-__global__ void k_mlp_target_lambda(int K, const int* __restrict__ cand, const double* __restrict__ lam, double scale,
-                                    float* __restrict__ Y) {
+// Column 3: the change of the multiplier over the frame, (lambda_final - lambda_prev) * scale, clipped to
+// [-kLamClip, kLamClip] (the network predicts a correction of the previous frame's multiplier).
+__global__ void k_mlp_target_lambda(int K, const int* __restrict__ cand, const double* __restrict__ lam,
+                                    const double* __restrict__ lam_prev, double scale, float* __restrict__ Y) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < K) Y[(size_t)cand[k] * 4 + 3] = (float)fmin(lam[k] * scale, kLamClip);
+    if (k >= K) return;
+    const double d = (lam[k] - (lam_prev ? lam_prev[k] : 0.0)) * scale;
+    Y[(size_t)cand[k] * 4 + 3] = (float)fmax(-kLamClip, fmin(d, kLamClip));
 }
 
 // Node-indexed contact multipliers in the network's scale (the lambda feature): 0 off the candidate set.
@@ -605,13 +609,14 @@ __global__ void k_mlp_lambda_scatter(int K, const int* __restrict__ cand, const 
     if (k < K) lam_node[cand[k]] = (float)fmin(lam[k] * scale, kLamClip);
 }
 
-// The predicted initial contact multipliers: lambda_k = max(0, out[node_k][3]) / scale.
+// The predicted initial contact multipliers: lambda_k <- max(0, lambda_k + out[node_k][3] / scale), the previous
+// frame's multiplier corrected by the network.
 __global__ void k_mlp_lambda_apply(int K, const int* __restrict__ cand, const float* __restrict__ out, double inv_scale,
                                    double* __restrict__ lam) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
-    const double v = (double)out[(size_t)cand[k] * 8 + 3];
-    lam[k] = v > 0.0 ? v * inv_scale : 0.0;
+    const double v = lam[k] + (double)out[(size_t)cand[k] * 8 + 3] * inv_scale;
+    lam[k] = v > 0.0 ? v : 0.0;
 }
 
 }  // namespace
@@ -626,8 +631,9 @@ void launch_mlp_lambda_nodes(int n, int K, const int* cand, const double* lam, d
     k_mlp_lambda_zero<<<(n + 255) / 256, 256, 0, st>>>(n, lam_node);
     if (K > 0) k_mlp_lambda_scatter<<<(K + 255) / 256, 256, 0, st>>>(K, cand, lam, scale, lam_node);
 }
-void launch_mlp_target_lambda(int K, const int* cand, const double* lam, double scale, float* Y, cudaStream_t st) {
-    if (K > 0) k_mlp_target_lambda<<<(K + 255) / 256, 256, 0, st>>>(K, cand, lam, scale, Y);
+void launch_mlp_target_lambda(int K, const int* cand, const double* lam, const double* lam_prev, double scale,
+                              float* Y, cudaStream_t st) {
+    if (K > 0) k_mlp_target_lambda<<<(K + 255) / 256, 256, 0, st>>>(K, cand, lam, lam_prev, scale, Y);
 }
 void launch_mlp_lambda_apply(int K, const int* cand, const float* out, double inv_scale, double* lam, cudaStream_t st) {
     if (K > 0) k_mlp_lambda_apply<<<(K + 255) / 256, 256, 0, st>>>(K, cand, out, inv_scale, lam);

@@ -201,13 +201,20 @@ __global__ void __launch_bounds__(kThr, 1) k_sfb_chol(double* __restrict__ M, in
                 double* Pg = M + (size_t)(kb + 1 + item) * kT * n + kb * kT;
                 for (int t = tid; t < kT * kT; t += nt) sA[(t / kT) * kLd + t % kT] = Pg[(size_t)(t / kT) * n + t % kT];
                 __syncthreads();
-                if (tid < kT) {
+                if (tid < kT) {  // row tid: x L_kk^T = m, four independent partial sums per dot
                     double* row = sA + tid * kLd;
                     for (int j = 0; j < kT; ++j) {
-                        double x = row[j];
                         const double* Lj = sD + j * kLd;
-                        for (int l = 0; l < j; ++l) x -= row[l] * Lj[l];
-                        row[j] = x / Lj[j];
+                        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                        int l = 0;
+                        for (; l + 4 <= j; l += 4) {
+                            s0 += row[l] * Lj[l];
+                            s1 += row[l + 1] * Lj[l + 1];
+                            s2 += row[l + 2] * Lj[l + 2];
+                            s3 += row[l + 3] * Lj[l + 3];
+                        }
+                        for (; l < j; ++l) s0 += row[l] * Lj[l];
+                        row[j] = (row[j] - ((s0 + s1) + (s2 + s3))) / Lj[j];
                     }
                 }
                 __syncthreads();
@@ -220,12 +227,19 @@ __global__ void __launch_bounds__(kThr, 1) k_sfb_chol(double* __restrict__ M, in
                     sA[r * kLd + c] = (c0 + c < ncols) ? Xg[(size_t)r * ldx + c] : 0.0;
                 }
                 __syncthreads();
-                if (tid < kT) {  // column tid: forward substitution with L_kk
+                if (tid < kT) {  // column tid: forward substitution with L_kk (four partial sums per dot)
                     for (int r = 0; r < kT; ++r) {
-                        double x = sA[r * kLd + tid];
                         const double* Lr = sD + r * kLd;
-                        for (int l = 0; l < r; ++l) x -= Lr[l] * sA[l * kLd + tid];
-                        sA[r * kLd + tid] = x / Lr[r];
+                        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                        int l = 0;
+                        for (; l + 4 <= r; l += 4) {
+                            s0 += Lr[l] * sA[l * kLd + tid];
+                            s1 += Lr[l + 1] * sA[(l + 1) * kLd + tid];
+                            s2 += Lr[l + 2] * sA[(l + 2) * kLd + tid];
+                            s3 += Lr[l + 3] * sA[(l + 3) * kLd + tid];
+                        }
+                        for (; l < r; ++l) s0 += Lr[l] * sA[l * kLd + tid];
+                        sA[r * kLd + tid] = (sA[r * kLd + tid] - ((s0 + s1) + (s2 + s3))) / Lr[r];
                     }
                 }
                 __syncthreads();

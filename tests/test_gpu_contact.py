@@ -96,3 +96,22 @@ def test_contact_mixed_precision_vs_fp64():
     print("worst per-step mixed vs FP64 difference / displacement from rest:", worst)
     assert touched > 0
     assert worst <= 2e-4
+
+
+def test_cached_factor_ncp_solve_matches_fresh_factorisation():
+    """The NCP's dense solve by CG preconditioned with a cached factor (ncp_solver 1, the default) against a fresh
+    Cholesky at every PD iteration (ncp_solver 0, the reference's scheme): the same active sets and the same
+    rollout to the CG tolerance, on a block whose whole bottom face rests on the ground."""
+    sc = scenes.hetero_contact(cells=(12, 12, 12), dx=0.01, steps=16, height=5e-4)
+    out = []
+    for solver in (0, 1):
+        d = core.from_scene(sc)
+        opts = dict(sc.options, ncp_solver=solver, rel_tol=1e-10, abs_tol=1e-14, max_pd_iter=3000)
+        q, v, acts = _roll_gpu(d, sc, sc.steps, opts)
+        out.append((q, acts, d.ncp_solve_stats()))
+    (q0, a0, s0), (q1, a1, s1) = out
+    assert a0 == a1 and len(a1[-1]) == 13 * 13
+    assert s0[0] == 0 and s0[1] > 0          # fresh factorisations only
+    assert s1[0] > 3 * s1[1]                 # mostly solved by the cached factor
+    disp = np.abs(q0 - sc.q0).max()
+    assert np.abs(q1 - q0).max() <= 1e-9 * disp
