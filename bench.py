@@ -280,6 +280,7 @@ def run_arm(arm, d, sc, state, args, dev, stream, mlp, clock=None):
     restore()
     d.reset_frame_stats()
     esc0 = d.fp64_escalations()
+    ncp0 = np.array(d.ncp_solve_stats(detail=True))
     torch.cuda.synchronize()
     q_out = [(torch.empty_like(q0), torch.empty_like(q0)) for _ in range(args.steps)]
     g_out = [(torch.empty_like(q0), torch.empty_like(q0), torch.empty_like(q0)) for _ in range(args.steps)]
@@ -323,6 +324,9 @@ def run_arm(arm, d, sc, state, args, dev, stream, mlp, clock=None):
            "contact_adjoint_iters_per_step": float(np.mean(contact_iters)) if contact_iters else None,
            "forward_converged_frac": float(np.mean(conv)) if len(conv) else None,
            "fp64_escalations": d.fp64_escalations() - esc0,
+           "pd_iters": [int(x) for x in fwd_iters],
+           "ncp_solves": dict(zip(("cached", "refactored", "cg_iters", "cg_fallbacks"),
+                                  (np.array(d.ncp_solve_stats(detail=True)) - ncp0).tolist())),
            "fwd_ms": [round(a.elapsed_time(b), 2) for a, b in ev[:args.steps]],
            "bwd_ms": [round(a.elapsed_time(b), 2) for a, b in ev[args.steps:]],
            "q_final": qs[-1]}

@@ -78,7 +78,7 @@ def load_library():
     L.dphd_device.argtypes = [C.c_void_p]
     L.dphd_debug_set_mma_wait_polls.argtypes = [C.c_longlong]
     L.dphd_fp64_escalations.argtypes = [C.c_void_p]
-    L.dphd_ncp_solve_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    L.dphd_ncp_solve_stats.argtypes = [C.c_void_p] + [C.POINTER(C.c_longlong)] * 4
     L.dphd_warm_start_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_void_p]
     L.dphd_backward_fallbacks.argtypes = [C.c_void_p]
     L.dphd_debug_set_factor_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -367,11 +367,13 @@ class Deformable:
         """Adjoint solves that fell back from CG (to the fixed point, or to the unconstrained adjoint)."""
         return int(self._L.dphd_backward_fallbacks(self._h))
 
-    def ncp_solve_stats(self):
-        """(solves by the cached factor, refactorisations) of the NCP's dense system since the contact set-up."""
-        a, b = C.c_longlong(0), C.c_longlong(0)
-        self._check(self._L.dphd_ncp_solve_stats(self._h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+    def ncp_solve_stats(self, detail=False):
+        """(solves by the cached factor, refactorisations) of the NCP's dense system since the contact set-up;
+        with detail=True also (CG iterations of the cached solves, CG attempts that fell back to a factorisation)."""
+        v = [C.c_longlong(0) for _ in range(4)]
+        self._check(self._L.dphd_ncp_solve_stats(self._h, *[C.byref(x) for x in v]))
+        out = tuple(x.value for x in v)
+        return out if detail else out[:2]
 
     def fp64_escalations(self):
         """Mixed-precision frames that finished in FP64 after the FP32 iteration stalled."""

@@ -436,8 +436,9 @@ int dphd_backward_fallbacks(const dphd_deformable* h) { return h && h->eng ? h->
 int dphd_warm_start_state(dphd_deformable* h, double* d_buf, int* valid, int set, void* stream) {
     return guard([&] { E(h).ws_state(d_buf, valid, set != 0, static_cast<cudaStream_t>(stream)); });
 }
-int dphd_ncp_solve_stats(dphd_deformable* h, long long* cached, long long* refactors) {
-    return guard([&] { E(h).ncp_stats(cached, refactors); });
+int dphd_ncp_solve_stats(dphd_deformable* h, long long* cached, long long* refactors, long long* cg_iters,
+                         long long* cg_fallbacks) {
+    return guard([&] { E(h).ncp_stats(cached, refactors, cg_iters, cg_fallbacks); });
 }
 int dphd_fp64_escalations(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.fp64_escalations : -1; }
 int dphd_last_backward_iters(const dphd_deformable* h) { return h && h->eng ? h->eng->stats.last_bwd_iters : -1; }

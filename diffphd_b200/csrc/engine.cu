@@ -700,11 +700,16 @@ void Engine::build_contact(double dt) {
     CUDA_OK(cudaMemset(dc_bar.p, 0, dc_bar.bytes));
     dc_Xinv.alloc(kcap * kcap * sizeof(double));
     dc_Xt.alloc(kcap * kcap * sizeof(double));
-    dc_pcg.alloc((4 * kcap + 1024) * sizeof(double));
+    dc_X32.alloc(kcap * kcap * sizeof(float));
+    dc_Xt32.alloc(kcap * kcap * sizeof(float));
+    dc_pcg.alloc((6 * kcap + 1024) * sizeof(double));
     dc_actref.alloc((size_t)K * sizeof(int));
+    dc_refpos.alloc((size_t)K * sizeof(int));
+    CUDA_OK(cudaMemset(dc_refpos.p, 0xff, dc_refpos.bytes));  // -1: no candidate is in a cached list yet
+    dc_refinv.alloc(kcap * sizeof(int));
     dc_flags.alloc(4 * sizeof(int));
     CUDA_OK(cudaMemset(dc_flags.p, 0, dc_flags.bytes));
-    dc_stats.alloc(2 * sizeof(unsigned long long));
+    dc_stats.alloc(4 * sizeof(unsigned long long));
     CUDA_OK(cudaMemset(dc_stats.p, 0, dc_stats.bytes));
     dc_act.alloc((size_t)K * sizeof(int));
     dc_kact.alloc(sizeof(int));
@@ -733,17 +738,23 @@ void Engine::build_contact(double dt) {
     c.kcap = kcap;
     c.Xinv = dc_Xinv.as<double>();
     c.Xt = dc_Xt.as<double>();
+    c.X32 = dc_X32.as<float>();
+    c.Xt32 = dc_Xt32.as<float>();
     c.pcg = dc_pcg.as<double>();
     c.act_ref = dc_actref.as<int>();
+    c.ref_pos = dc_refpos.as<int>();
+    c.ref_inv = dc_refinv.as<int>();
     c.ncp_flags = dc_flags.as<int>();
     c.ncp_stats = dc_stats.as<unsigned long long>();
 }
 
-void Engine::ncp_stats(long long* cached, long long* refactors) {
-    unsigned long long h[2] = {0, 0};
+void Engine::ncp_stats(long long* cached, long long* refactors, long long* cg_iters, long long* cg_fallbacks) {
+    unsigned long long h[4] = {0, 0, 0, 0};
     if (has_contact_ && dc_stats.p) CUDA_OK(cudaMemcpy(h, dc_stats.p, sizeof(h), cudaMemcpyDeviceToHost));
-    *cached = (long long)h[0];
-    *refactors = (long long)h[1];
+    if (cached) *cached = (long long)h[0];
+    if (refactors) *refactors = (long long)h[1];
+    if (cg_iters) *cg_iters = (long long)h[2];
+    if (cg_fallbacks) *cg_fallbacks = (long long)h[3];
 }
 
 void Engine::reset_warm_start() {
@@ -1174,6 +1185,9 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
                 }
         graph_mu_ = o.friction_mu;
         CUDA_OK(cudaMemsetAsync(dc_bar.p, 0, dc_bar.bytes, st));  // clears an abort left by an earlier solve
+        // every frame starts without a cached NCP factor, so that a frame's result depends on its inputs (and the
+        // multipliers' warm start) alone: a recomputed frame repeats the original bit for bit
+        CUDA_OK(cudaMemsetAsync(dc_flags.p, 0, dc_flags.bytes, st));
     }
     const int mode64 = has_contact_ ? 5 : 0, mode32 = has_contact_ ? 8 : 1;
     if (o.fp32_bulk && o.fp32_stall_window > 0) {

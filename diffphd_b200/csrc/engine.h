@@ -140,7 +140,7 @@ public:
     int contact_candidates() const;
     void contact_lambda_device(double* d_buf, bool set, cudaStream_t st);
     // NCP solves by the cached factor and refactorisations since the contact set-up
-    void ncp_stats(long long* cached, long long* refactors);
+    void ncp_stats(long long* cached, long long* refactors, long long* cg_iters, long long* cg_fallbacks);
     bool ws_net_attached() const { return ws_net_; }
     // the learned start's frame-to-frame state (whether a previous step exists, its q and its q_tilde): copied to
     // (set = false) or from (set = true) a device array of 2 * 3n doubles, so that a checkpointed rollout can
@@ -287,7 +287,7 @@ private:
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0, dc_Xinv, dc_Xt, dc_pcg,
-        dc_actref, dc_flags, dc_stats;
+        dc_actref, dc_flags, dc_stats, dc_X32, dc_Xt32, dc_refpos, dc_refinv;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

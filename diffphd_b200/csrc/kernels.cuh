@@ -236,13 +236,19 @@ struct ContactDev {
     double* Mwork = nullptr;         // active system, kcap x kcap capacity (kcap = K rounded up to 64)
     unsigned int* bar = nullptr;     // grid barrier of the NCP solve: count, generation, abort
     // cached-factor solve (ncp_cached.cu): kcap = padded capacity; X = L_ref^-1 (lower) and its transpose for the
-    // active list act_ref; CG work vectors and per-CTA partials; flags (factor valid, its ka, list differs);
-    // stats (solves by the cached factor, refactorisations)
+    // active list act_ref, with FP32 copies for the CG preconditioner; ref_pos[k] = the position of candidate k
+    // in act_ref (-1: not in it), ref_inv[a] = the position of act_ref[a] in the current list (-1: dropped); CG
+    // work vectors and per-CTA partials; flags (factor valid, its ka, candidates new to the list this launch);
+    // stats (solves by the cached factor, refactorisations, CG iterations, CG attempts that fell back)
     size_t kcap = 0;
     double* Xinv = nullptr;
     double* Xt = nullptr;
+    float* X32 = nullptr;
+    float* Xt32 = nullptr;
     double* pcg = nullptr;
     int* act_ref = nullptr;
+    int* ref_pos = nullptr;
+    int* ref_inv = nullptr;
     int* ncp_flags = nullptr;
     unsigned long long* ncp_stats = nullptr;
     int cached = 1;                  // 1: the cached-factor solve, 0: a fresh factorisation every PD iteration

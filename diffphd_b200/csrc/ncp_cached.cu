@@ -1,14 +1,18 @@
 // The NCP's dense solve M dlambda = rhs (M = Omega G Omega + E over the ka active candidates) with a cached
 // factor: the reference factors M at every PD iteration (forward_gpu.cpp:1238-1240).  Here one cooperative
 // launch per PD iteration
-//   A  assembles M (full rows, identity-padded to a multiple of 64) and the right-hand side, and marks whether the
-//      active list differs from the one the cached factor was built for;
-//   B  when a cached factor X = L_ref^-1 of a recent M_ref (same active list) exists: conjugate gradients on M
-//      preconditioned by X^T X, to |r| <= 1e-13 |rhs|, at most kNcpPcgIters iterations.  Near the fixed point
-//      Omega and E change little between PD iterations, so M_ref^-1 M is close to I and a few iterations suffice;
-//   C  otherwise (a new active list, or CG not converged): the blocked Cholesky of M with the triangular solve of
-//      the identity folded in (X = L^-1, only the lower blocks, kept as the new cached factor), then
-//      dlambda = X^T (X rhs);
+//   A  assembles M (full rows, identity-padded to a multiple of 64) and the right-hand side, and counts the active
+//      candidates that are not in the list act_ref the cached factor was built for;
+//   B  when a cached factor X = L_ref^-1 of an earlier M_ref of this frame exists and the two lists differ in at
+//      most kNcpMaxListChange candidates: conjugate gradients on M to |r| <= 1e-13 |rhs|, preconditioned by
+//      P = (X^T X restricted to the candidates in both lists) (+) diag(M)^-1 on the new ones.  X^T X restricted to a
+//      subset of its list is the inverse of a Schur complement of M_ref, so P M differs from I by the change of
+//      Omega and E between the PD iterations plus a term of rank <= (dropped + 2 x new candidates); near the fixed
+//      point a few iterations suffice.  X is applied from FP32 copies (the preconditioner only has to be
+//      symmetric positive definite; the residual and the iterate are FP64);
+//   C  otherwise (no factor, a large change of the list, or CG not converged): the blocked Cholesky of M with the
+//      triangular solve of the identity folded in (X = L^-1, only the lower blocks, kept as the new cached factor),
+//      then dlambda = X^T (X rhs);
 //   D  clamp, Coulomb cone and the contact right-hand side, as k_ncp_block_solve.
 // Both paths solve the same system to rounding (the CG tolerance is 1e-13), so the iterates match the
 // refactor-every-iteration solve (option ncp_solver = 0) to that level.
@@ -23,7 +27,8 @@ namespace {
 constexpr int kT = 64;
 constexpr int kLd = kT + 1;
 constexpr int kThr = 256;
-constexpr int kNcpPcgIters = 40;
+constexpr int kNcpPcgIters = 40;       // CG iteration cap for an unchanged list; + 2 per changed candidate
+constexpr int kNcpMaxListChange = 32;  // larger changes of the active list refactor at once
 constexpr double kNcpPcgTol = 1e-13;
 constexpr long long kSpins = 1ll << 24;
 
@@ -169,20 +174,27 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
     double* M = c.Mwork;
     double* rhs = c.rhs;
     double* x = c.xsol;
-    double* part = c.pcg + 4 * (size_t)ldx;  // per-CTA partial sums
-    int* flags = c.ncp_flags;                // [0] cached factor valid, [1] its ka, [2] list differs (this launch)
-    const bool have = flags[0] != 0 && flags[1] == ka;
-    // ---- A: M (full rows), rhs, and whether the active list matches the cached factor's ----
-    int differs = 0;
+    double* dg = c.pcg + 5 * (size_t)ldx;    // diag(M)
+    double* part = c.pcg + 6 * (size_t)ldx;  // per-CTA partial sums
+    int* flags = c.ncp_flags;  // [0] cached factor valid, [1] its ka, [2] candidates not in its list (this launch)
+    const bool have = flags[0] != 0;
+    const int ka_ref = have ? flags[1] : 0;
+    const int ld_ref = (ka_ref + kT - 1) / kT * kT;
+    // ---- A: M (full rows), diag(M), rhs, and the active candidates that are new to the cached factor's list ----
+    for (int a = gt; a < ka_ref; a += nthr) c.ref_inv[a] = -1;
+    int n_new_w = 0;
     for (int a = gw; a < ld; a += nwarps) {
         double* Ma = M + (size_t)a * ld;
         if (a >= ka) {
             for (int b = lane; b < ld; b += 32) Ma[b] = (a == b) ? 1.0 : 0.0;
-            if (lane == 0) rhs[a] = 0.0;
+            if (lane == 0) {
+                rhs[a] = 0.0;
+                dg[a] = 1.0;
+            }
             continue;
         }
         const int k = c.act[a];
-        if (have && lane == 0 && c.act_ref[a] != k) differs = 1;
+        if (have && lane == 0 && c.ref_pos[k] < 0) ++n_new_w;
         const double om = c.omega[k];
         const double* Gk = c.G + (size_t)k * K;
         double g0 = 0.0, g1 = 0.0, g2 = 0.0;
@@ -198,7 +210,9 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             g0 += Gab * (fn * n0 + f1 * c.t1[0] + f2 * c.t2[0]);
             g1 += Gab * (fn * n1 + f1 * c.t1[1] + f2 * c.t2[1]);
             g2 += Gab * (fn * n2 + f1 * c.t1[2] + f2 * c.t2[2]);
-            Ma[b] = om * Gab * c.omega[kb] + (a == b ? c.Ediag[k] : 0.0);
+            const double m = om * Gab * c.omega[kb] + (a == b ? c.Ediag[k] : 0.0);
+            Ma[b] = m;
+            if (a == b) dg[a] = m;
         }
         g0 = wsum(g0);
         g1 = wsum(g1);
@@ -210,16 +224,27 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             rhs[a] = c.hvec[k] - om * (n0 * g0 + n1 * g1 + n2 * g2);
         }
     }
-    if (differs) atomicOr(flags + 2, 1);
+    if (n_new_w) atomicAdd(flags + 2, n_new_w);
     if (!gsync(c.bar, ctrl)) return;
+    // lists sorted by candidate index: no new candidate and the same count means the same list, position for position
+    const int n_new = have ? __ldcg(flags + 2) : 0;
+    const int n_chg = n_new + (ka_ref - (ka - n_new));
+    const bool same = have && n_chg == 0;
     bool solved = false;
-    if (have && __ldcg(flags + 2) == 0) {
-        // ---- B: CG on M, preconditioned by X^T X (X = L_ref^-1, lower, ld ldx) ----
+    if (have && n_chg <= kNcpMaxListChange) {
+        // ---- B: CG on M, preconditioned by the cached factor on the common candidates, diag(M) on the new ----
         double* r = c.pcg;
         double* p = c.pcg + ldx;
         double* w = c.pcg + 2 * (size_t)ldx;
         double* t = c.pcg + 3 * (size_t)ldx;
-        const double* X = c.Xinv;
+        double* zr = c.pcg + 4 * (size_t)ldx;  // X^T X r over the cached list (a changed list only)
+        if (!same) {
+            for (int a = gt; a < ka; a += nthr) {
+                const int pr = c.ref_pos[c.act[a]];
+                if (pr >= 0) c.ref_inv[pr] = a;
+            }
+            if (!gsync(c.bar, ctrl)) return;
+        }
         // r = rhs, x = 0, |rhs|^2
         double acc = 0.0;
         for (int a = gt; a < ld; a += nthr) {
@@ -235,26 +260,51 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         double rz = 0.0;
         int it = 0;
         bool conv = rhs2 == 0.0;
-        while (!conv && it < kNcpPcgIters) {
-            // t = X r (one warp per row)
-            for (int a = gw; a < ld; a += nwarps) {
-                const double* Xa = X + (size_t)a * ldx;
+        const int cap = kNcpPcgIters + 2 * n_chg;
+        while (!conv && it < cap) {
+            // t = X r_ref over the cached list (one warp per row; r_ref = r at the common candidates, 0 at dropped)
+            for (int a = gw; a < ld_ref; a += nwarps) {
+                const float* Xa = c.X32 + (size_t)a * ldx;
                 double s = 0.0;
-                for (int b = lane; b <= a; b += 32) s += Xa[b] * __ldcg(r + b);
+                if (same) {
+                    for (int b = lane; b <= a; b += 32) s += (double)Xa[b] * __ldcg(r + b);
+                } else {
+                    for (int b = lane; b <= a && b < ka_ref; b += 32) {
+                        const int nb_ = __ldcg(c.ref_inv + b);
+                        if (nb_ >= 0) s += (double)Xa[b] * __ldcg(r + nb_);
+                    }
+                }
                 s = wsum(s);
                 if (lane == 0) t[a] = s;
             }
             if (!gsync(c.bar, ctrl)) return;
             // z = X^T t (one warp per row of the stored transpose), rz_new = r . z; z kept in w
             acc = 0.0;
-            for (int b = gw; b < ld; b += nwarps) {
-                const double* Xb = c.Xt + (size_t)b * ldx;
+            for (int b = gw; b < ld_ref; b += nwarps) {
+                const float* Xb = c.Xt32 + (size_t)b * ldx;
                 double s = 0.0;
-                for (int a = b + lane; a < ld; a += 32) s += Xb[a] * __ldcg(t + a);
+                for (int a = b + lane; a < ld_ref; a += 32) s += (double)Xb[a] * __ldcg(t + a);
                 s = wsum(s);
                 if (lane == 0) {
-                    w[b] = s;
-                    acc += __ldcg(r + b) * s;
+                    if (same) {
+                        w[b] = s;
+                        acc += __ldcg(r + b) * s;
+                    } else {
+                        zr[b] = s;
+                    }
+                }
+            }
+            if (!same) {  // z on the current list: the cached factor's value, or r / M_aa on a new candidate
+                if (!gsync(c.bar, ctrl)) return;
+                for (int a = gt; a < ld; a += nthr) {
+                    const double ra = __ldcg(r + a);
+                    double z = ra;
+                    if (a < ka) {
+                        const int pr = c.ref_pos[c.act[a]];
+                        z = pr >= 0 ? __ldcg(zr + pr) : (dg[a] > 0.0 ? ra / dg[a] : ra);
+                    }
+                    w[a] = z;
+                    acc += ra * z;
                 }
             }
             cta_partial(wsum(acc), part);
@@ -295,10 +345,15 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             if (!gsync(c.bar, ctrl)) return;
         }
         solved = conv;
+        if (gt == 0) {
+            c.ncp_stats[2] += it;         // CG iterations
+            if (!conv) c.ncp_stats[3] += 1;  // CG attempts that fall back to a factorisation
+        }
     }
     if (!solved) {
         // ---- C: blocked Cholesky of M with X = L^-1 (identity solved in place), then x = X^T X rhs ----
         double* X = c.Xinv;
+        for (int k = gt; k < K; k += nthr) c.ref_pos[k] = -1;  // read no more in this launch (after its CG)
         for (size_t e = (size_t)gt; e < (size_t)ld * ld; e += (size_t)nthr) {
             const int a = (int)(e / ld), b = (int)(e % ld);
             X[(size_t)a * ldx + b] = a == b ? 1.0 : 0.0;
@@ -430,7 +485,12 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         // the transpose of X (its lower triangle), for row-wise X^T products; then x = X^T (X rhs)
         for (size_t e = (size_t)gt; e < (size_t)ld * ld; e += (size_t)nthr) {
             const int a = (int)(e / ld), b = (int)(e % ld);
-            if (b <= a) c.Xt[(size_t)b * ldx + a] = X[(size_t)a * ldx + b];
+            if (b <= a) {
+                const double v = X[(size_t)a * ldx + b];
+                c.Xt[(size_t)b * ldx + a] = v;
+                c.X32[(size_t)a * ldx + b] = (float)v;
+                c.Xt32[(size_t)b * ldx + a] = (float)v;
+            }
         }
         double* t = c.pcg + 3 * (size_t)ldx;
         for (int a = gw; a < ld; a += nwarps) {
@@ -448,8 +508,11 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             s = wsum(s);
             if (lane == 0) x[b] = s;
         }
-        // the new cached factor: its active list
-        for (int a = gt; a < ka; a += nthr) c.act_ref[a] = c.act[a];
+        // the new cached factor: its active list and the candidates' positions in it
+        for (int a = gt; a < ka; a += nthr) {
+            c.act_ref[a] = c.act[a];
+            c.ref_pos[c.act[a]] = a;
+        }
         if (gt == 0) {
             flags[0] = 1;
             flags[1] = ka;

@@ -132,11 +132,14 @@ int dphd_last_backward_iters(const dphd_deformable* h);
  * checkpointed rollout saves it with each checkpoint (with the contact multipliers) so that recomputing a segment
  * repeats the forward pass exactly.  No counterpart in the reference. */
 int dphd_warm_start_state(dphd_deformable* h, double* d_buf, int* valid, int set, void* stream);
-/* The NCP's dense solves since the contact set-up: by conjugate gradients preconditioned with the cached factor
- * of an earlier PD iteration's system (same active list), and by a fresh factorisation (option ncp_solver 1,
- * the default; ncp_solver 0 factors at every PD iteration as the reference does, forward_gpu.cpp:1238-1240).
- * No counterpart in the reference. */
-int dphd_ncp_solve_stats(dphd_deformable* h, long long* cached, long long* refactors);
+/* The NCP's dense solves since the contact set-up (option ncp_solver 1, the default; ncp_solver 0 factors at
+ * every PD iteration as the reference does, forward_gpu.cpp:1238-1240): solves by conjugate gradients
+ * preconditioned with the cached factor of an earlier PD iteration's system of the same frame (its active list
+ * may differ by a few candidates), fresh factorisations, the CG iterations of all cached solves, and the CG
+ * attempts that did not converge and fell back to a factorisation.  Any pointer may be NULL.  No counterpart in
+ * the reference. */
+int dphd_ncp_solve_stats(dphd_deformable* h, long long* cached, long long* refactors, long long* cg_iters,
+                         long long* cg_fallbacks);
 /* Mixed-precision forward frames (option fp32_bulk) whose FP32 iteration stalled and that finished in FP64 from
  * the FP32 iterate, since the handle was created (option fp32_stall_window: iterations without the gate ratio
  * halving, default 40; 0 never switches).  No counterpart in the reference. */
