@@ -383,6 +383,9 @@ int dphd_debug_set_mma_wait_polls(long long polls) {
 int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_max) {
     return guard([&] { E(h).set_factor_build(mode, small_subtree_max); });
 }
+int dphd_debug_set_st_schedule(dphd_deformable* h, int chunk_rows, int rows_in_flight) {
+    return guard([&] { E(h).set_st_schedule(chunk_rows, rows_in_flight); });
+}
 int dphd_factor_built_on_device(const dphd_deformable* h) {
     return h && h->eng ? h->eng->factor_built_on_device() : -1;
 }

@@ -574,6 +574,45 @@ template void launch_ncp_iteration<double>(const ContactDev&, const double*, con
 template void launch_ncp_iteration<float>(const ContactDev&, const double*, const float*, int, const double*,
                                           const double*, const int*, float*, const double*, Ctrl*, cudaStream_t);
 
+namespace {
+__global__ void k_permute_r64(int n, const double* __restrict__ r64, const int* __restrict__ iperm,
+                              double* __restrict__ v, int npad, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int j = iperm[i];
+        v[j] = r64[3 * i];
+        v[npad + j] = r64[3 * i + 1];
+        v[2 * (size_t)npad + j] = r64[3 * i + 2];
+    } else if (i < npad) {  // padding rows of the permuted vector
+        v[i] = 0.0;
+        v[npad + i] = 0.0;
+        v[2 * (size_t)npad + i] = 0.0;
+    }
+}
+
+__global__ void k_cand_to_f32(ContactDev c, const int* __restrict__ iperm, const double* __restrict__ v64,
+                              float* __restrict__ v32, int npad, const Ctrl* ctrl) {
+    if (ctrl->done) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c.K) return;
+    const int j = iperm[c.cand[k]];
+    v32[j] = (float)v64[j];
+    v32[npad + j] = (float)v64[npad + j];
+    v32[2 * (size_t)npad + j] = (float)v64[2 * (size_t)npad + j];
+}
+}  // namespace
+
+void launch_permute_r64(int n, const double* r64, const int* iperm, double* vperm64, int npad, const Ctrl* ctrl,
+                        cudaStream_t st) {
+    k_permute_r64<<<(npad + 255) / 256, 256, 0, st>>>(n, r64, iperm, vperm64, npad, ctrl);
+}
+
+void launch_cand_to_f32(const ContactDev& c, const int* iperm, const double* vcon64, float* vperm32, int npad,
+                        const Ctrl* ctrl, cudaStream_t st) {
+    if (c.K > 0) k_cand_to_f32<<<(c.K + 255) / 256, 256, 0, st>>>(c, iperm, vcon64, vperm32, npad, ctrl);
+}
+
 void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,
                         double slop, cudaStream_t st) {
     if (c.K > 0) k_restitution<<<(c.K + 255) / 256, 256, 0, st>>>(c, q, q0, v0, h, e, slop);

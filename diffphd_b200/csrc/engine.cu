@@ -73,6 +73,7 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.fp32_projection = (int)get("fp32_projection", -1);
     o.ws_lambda = (int)get("ws_lambda", 0);
     o.ncp_solver = (int)get("ncp_solver", 1);
+    o.ncp_input_fp64 = (int)get("ncp_input_fp64", 0);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -223,6 +224,14 @@ void Engine::set_factor_build(int mode, int small_subtree_max) {
     small_subtree_max_ = sm;
 }
 
+void Engine::set_st_schedule(int chunk_rows, int rows_in_flight) {
+    DPHD_CHECK(chunk_rows >= 8 && chunk_rows <= 4096, "S^T chunk rows must lie in [8, 4096]");
+    DPHD_CHECK(rows_in_flight == 4 || rows_in_flight == 8, "S^T rows in flight must be 4 or 8");
+    if (chunk_rows != st_chunk_rows_ || rows_in_flight != st_rows_) built_ = false;
+    st_chunk_rows_ = chunk_rows;
+    st_rows_ = rows_in_flight;
+}
+
 void Engine::check_device() const {
     if (device_ < 0) return;
     int cur = -1;
@@ -360,13 +369,13 @@ void Engine::build_device(int threads) {
         std::vector<int> pos(r_ptr.begin(), r_ptr.end() - 1);
         for (size_t t = 0; t < it_row.size(); ++t) r_items[pos[it_row[t]]++] = (int)t;
     }
-    // x = S^T y schedule: each tile's row list in chunks of kChunkRows rows
+    // x = S^T y schedule: each tile's row list in chunks of st_chunk_rows_ rows
     std::vector<int> c_tile, c_p0, c_p1, t_cptr(ntiles_ + 1, 0);
     for (int t = 0; t < ntiles_; ++t) {
-        for (int p0 = tcnt[t]; p0 < tcnt[t + 1]; p0 += kChunkRows) {
+        for (int p0 = tcnt[t]; p0 < tcnt[t + 1]; p0 += st_chunk_rows_) {
             c_tile.push_back(t);
             c_p0.push_back(p0);
-            c_p1.push_back(std::min(p0 + kChunkRows, tcnt[t + 1]));
+            c_p1.push_back(std::min(p0 + st_chunk_rows_, tcnt[t + 1]));
         }
         if (tcnt[t] == tcnt[t + 1]) {  // keep every tile covered so stage 2 writes zeros
             c_tile.push_back(t);
@@ -470,6 +479,7 @@ void Engine::build_device(int threads) {
         P.row_item_ptr = d_row_item_ptr.as<int>();
         P.row_items = d_row_items.as<int>();
         P.n_chunks = (int)c_tile.size();
+        P.st_rows = st_rows_;
         P.ntiles = ntiles_;
         P.chunk_tile = d_chunk_tile.as<int>();
         P.chunk_p0 = d_chunk_p0.as<int>();
@@ -812,10 +822,22 @@ void Engine::enqueue_contact_iteration(cudaStream_t st, bool f32) {
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
                                  gather_blocks_, Acsr_, d_x.as<double>(), 1, c, st, d_r64.as<double>());
-        launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
-        launch_ncp_iteration<float>(contact_, d_x.as<double>(), d_y32.as<float>(), npad_, d_x.as<double>(),
-                                    d_q0.as<double>(), d_iperm.as<int>(), d_vperm32.as<float>(),
-                                    d_r64.as<double>(), c, st);
+        if (ncp64in_) {
+            // the NCP's input A^-1 b = x + S^T-path(S r) from an FP64 S pass: r is not small at the candidates
+            // (it carries -J^T f there), so its FP32 image would leave rounding noise in the contact gaps
+            launch_permute_r64(n, d_r64.as<double>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_, c, st);
+            launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
+            launch_ncp_iteration<double>(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, d_x.as<double>(),
+                                         d_q0.as<double>(), d_iperm.as<int>(), d_vcon.as<double>(),
+                                         d_r64.as<double>(), c, st);
+            launch_cand_to_f32(contact_, d_iperm.as<int>(), d_vcon.as<double>(), d_vperm32.as<float>(), npad_, c,
+                               st);
+        } else {
+            launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
+            launch_ncp_iteration<float>(contact_, d_x.as<double>(), d_y32.as<float>(), npad_, d_x.as<double>(),
+                                        d_q0.as<double>(), d_iperm.as<int>(), d_vperm32.as<float>(),
+                                        d_r64.as<double>(), c, st);
+        }
         launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
         SpmvPlan<float> ref = plan32_;
         ref.x_base = d_x.as<double>();
@@ -1164,6 +1186,13 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
                 cudaGraphExecDestroy(graphs_[md]);
                 graphs_[md] = nullptr;
             }
+    }
+    if (has_contact_ && (o.ncp_input_fp64 != 0) != ncp64in_) {  // captured in the mixed contact graph
+        ncp64in_ = o.ncp_input_fp64 != 0;
+        if (graphs_[8]) {
+            cudaGraphExecDestroy(graphs_[8]);
+            graphs_[8] = nullptr;
+        }
     }
     if (has_contact_) {
         contact_.mu = o.friction_mu;

@@ -51,6 +51,8 @@ struct Options {
                                  // slower on the 64^3 contact rollout, so off by default)
     int fp32_projection = -1;    // mixed precision: 1 FP32 local projections, 0 FP64 projections with FP32 S
                                  // passes, -1 automatic (FP32 without a contact set, FP64 with one)
+    int ncp_input_fp64 = 0;      // mixed precision with contact: 1 computes the NCP's A^-1 b at the candidates
+                                 // with an FP64 S pass (the other S / S^T passes of the iteration stay FP32)
     int fp32_stall_window = 40;  // mixed precision: iterations without the gate ratio halving before the rest of
                                  // the frame continues in FP64 (0: never)
     static Options parse(const std::map<std::string, double>& m);
@@ -160,6 +162,9 @@ public:
     // how the sparse-inverse factor is built: 0 automatic (on the device above kDeviceBuildNnz values, on the
     // host below), 1 host, 2 device; a change takes effect at the next factor build
     void set_factor_build(int mode, int small_subtree_max);
+    // the S^T pass's schedule: rows per chunk CTA and rows in flight per warp (4 or 8); takes effect at the next
+    // factor build
+    void set_st_schedule(int chunk_rows, int rows_in_flight);
     int factor_built_on_device() const { return factor_on_device_ ? 1 : 0; }
     static constexpr long long kDeviceBuildNnz = 32ll << 20;
     // CUDA device that holds this handle's GPU state (-1 until the first call that builds it); every later
@@ -226,7 +231,9 @@ private:
     void check_device() const;
     int device_ = -1;
     int factor_mode_ = 0, small_subtree_max_ = 512;
+    int st_chunk_rows_ = kChunkRows, st_rows_ = 4;
     bool proj32_ = true;  // precision of the projections captured in the mixed-precision iteration graphs
+    bool ncp64in_ = false;  // FP64 NCP input captured in the mixed-precision contact graph
     bool factor_on_device_ = false;
     std::unique_ptr<SBuildPlan> sb_plan_;   // device build: plan and the permuted upper triangle of A, kept from
     std::unique_ptr<PermUpper> sb_upper_;   // the symbolic step until build_device runs the numeric one

@@ -537,9 +537,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
 // to xpart[chunk] and summed in chunk order by stage 2.  Each warp takes every 8th row of the chunk and keeps
 // kStRows rows in flight.  FROM_ITEMS: y_r is summed here from the S pass's row-contiguous item partials (in
 // slot order, as the S fix-up kernel would), so the pair needs no separate fix-up launch.
-constexpr int kStRows = 4;
-
-template <typename T, bool FROM_ITEMS>
+template <typename T, bool FROM_ITEMS, int kStRows>
 __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __restrict__ y, int ch, const Ctrl* ctrl) {
     __shared__ T red[8][3][kTileCols];
     const int done = ctrl->done;  // in flight together with the chunk's bounds; the same in every thread
@@ -623,10 +621,10 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
     __syncthreads();  // `red` is reused by the next chunk of a persistent CTA
 }
 
-template <typename T, bool FROM_ITEMS>
+template <typename T, bool FROM_ITEMS, int kStRows>
 __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
     pdl_enter();
-    st_part_body<T, FROM_ITEMS>(p, y, blockIdx.x, ctrl);
+    st_part_body<T, FROM_ITEMS, kStRows>(p, y, blockIdx.x, ctrl);
 }
 
 // x = S^T y, stage 2: per tile column, sum the chunk partials in order and scatter to node-major x.
@@ -1700,6 +1698,13 @@ void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const do
                                                      v_perm, npad, prev_pd, part, A, q, zero_dirichlet, r_out, ctrl);
 }
 
+// stage 1 of x = S^T y with the plan's rows in flight per warp
+template <typename T, bool FROM_ITEMS>
+static void launch_st_part(const SpmvPlan<T>& p, const T* y, const Ctrl* ctrl, cudaStream_t st) {
+    if (p.st_rows == 8) launch_k(k_spmv_ST_part<T, FROM_ITEMS, 8>, p.n_chunks, 256, 0, st, p, y, ctrl);
+    else launch_k(k_spmv_ST_part<T, FROM_ITEMS, 4>, p.n_chunks, 256, 0, st, p, y, ctrl);
+}
+
 // stage 1 of y = S v: the row-group kernel for FP32 factors with a unit schedule, else one warp per item
 template <typename T>
 static void launch_s_items(const SpmvPlan<T>& p, const T* v, const Ctrl* ctrl, cudaStream_t st) {
@@ -1717,9 +1722,9 @@ void launch_sts(const SpmvPlan<T>& p, const T* v, T* y, double* x_out, const Ctr
     launch_s_items(p, v, ctrl, st);
     if (p.y_accumulate) {
         launch_k(k_spmv_S_fin<T>, blocks_for(p.n, kThreads), kThreads, 0, st, p, y, ctrl);
-        launch_k(k_spmv_ST_part<T, false>, p.n_chunks, 256, 0, st, p, y, ctrl);
+        launch_st_part<T, false>(p, y, ctrl, st);
     } else {
-        launch_k(k_spmv_ST_part<T, true>, p.n_chunks, 256, 0, st, p, nullptr, ctrl);
+        launch_st_part<T, true>(p, nullptr, ctrl, st);
     }
     launch_k(k_spmv_ST_fin<T>, blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st, p, x_out, ctrl);
 }
@@ -1899,7 +1904,7 @@ template <typename T>
 void launch_sts_cg(const SpmvPlan<T>& p, const T* v, double* z, const double* r, double* part, const double* mu_part,
                    int mu_blocks, Ctrl* ctrl, cudaStream_t st) {
     launch_s_items(p, v, ctrl, st);
-    launch_k(k_spmv_ST_part<T, true>, p.n_chunks, 256, 0, st, p, nullptr, ctrl);
+    launch_st_part<T, true>(p, nullptr, ctrl, st);
     launch_k(k_spmv_ST_fin_cg<T>, blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st, 
         p, z, r, part, mu_part, mu_blocks, ctrl);
 }
@@ -1978,7 +1983,7 @@ void launch_s_only(const SpmvPlan<T>& p, const T* v, T* y, const Ctrl* ctrl, cud
 }
 template <typename T>
 void launch_st_only(const SpmvPlan<T>& p, const T* y, double* x_out, const Ctrl* ctrl, cudaStream_t st) {
-    launch_k(k_spmv_ST_part<T, false>, p.n_chunks, 256, 0, st, p, y, ctrl);
+    launch_st_part<T, false>(p, y, ctrl, st);
     launch_k(k_spmv_ST_fin<T>, blocks_for((long long)p.ntiles * 3 * kTileCols, kThreads), kThreads, 0, st, p, x_out, ctrl);
 }
 template void launch_s_only<double>(const SpmvPlan<double>&, const double*, double*, const Ctrl*, cudaStream_t);

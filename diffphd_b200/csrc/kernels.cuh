@@ -93,8 +93,9 @@ struct SpmvPlan {
     const int* row_item_ptr = nullptr;
     const int* row_items = nullptr;
     T* ypart = nullptr;
-    // x = S^T y: column tiles of kTileCols, each tile's row list split into chunks (one CTA each)
-    int n_chunks = 0, ntiles = 0;
+    // x = S^T y: column tiles of kTileCols, each tile's row list split into chunks (one CTA each); st_rows: rows
+    // in flight per warp (4 or 8)
+    int n_chunks = 0, ntiles = 0, st_rows = 4;
     const int* chunk_tile = nullptr;
     const int* chunk_p0 = nullptr;
     const int* chunk_p1 = nullptr;
@@ -123,7 +124,7 @@ struct SpmvPlan {
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
-constexpr int kChunkRows = 64;       // rows per S^T chunk CTA
+constexpr int kChunkRows = 64;       // rows per S^T chunk CTA (default of the schedule)
 constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 constexpr int kGatherMaxThreads = 512;  // block-size bound of the node gathers
 
@@ -285,6 +286,12 @@ template <typename T>
 void launch_ncp_iteration(const ContactDev& c, const double* x, const T* y, int npad, const double* x_base,
                           const double* q0, const int* iperm, T* vcon, const double* r64, Ctrl* ctrl,
                           cudaStream_t st);
+// Mixed precision with an FP64 NCP input: r (node order, FP64) into the permuted FP64 S-pass input, and the
+// candidates' FP64 S-pass inputs r + J^T f (written by the FP64 NCP step) into the FP32 S-pass input.
+void launch_permute_r64(int n, const double* r64, const int* iperm, double* vperm64, int npad, const Ctrl* ctrl,
+                        cudaStream_t st);
+void launch_cand_to_f32(const ContactDev& c, const int* iperm, const double* vcon64, float* vperm32, int npad,
+                        const Ctrl* ctrl, cudaStream_t st);
 void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,
                         double slop, cudaStream_t st);
 // y (+)= S v only (first half of the pair), and x = S^T y only (second half).

@@ -176,7 +176,8 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
     double* x = c.xsol;
     double* dg = c.pcg + 5 * (size_t)ldx;    // diag(M)
     double* part = c.pcg + 6 * (size_t)ldx;  // per-CTA partial sums
-    int* flags = c.ncp_flags;  // [0] cached factor valid, [1] its ka, [2] candidates not in its list (this launch)
+    // [0] cached factor valid, [1] its ka, [2] candidates not in its list (this launch), [3] the last CG fell back
+    int* flags = c.ncp_flags;
     const bool have = flags[0] != 0;
     const int ka_ref = have ? flags[1] : 0;
     const int ld_ref = (ka_ref + kT - 1) / kT * kT;
@@ -260,7 +261,8 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         double rz = 0.0;
         int it = 0;
         bool conv = rhs2 == 0.0;
-        const int cap = kNcpPcgIters + 2 * n_chg;
+        // after an attempt that fell back, the next one gets a quarter of the cap (a system far from the cached one)
+        const int cap = (__ldcg(flags + 3) != 0 ? kNcpPcgIters / 4 : kNcpPcgIters) + 2 * n_chg;
         while (!conv && it < cap) {
             // t = X r_ref over the cached list (one warp per row; r_ref = r at the common candidates, 0 at dropped)
             for (int a = gw; a < ld_ref; a += nwarps) {
@@ -348,6 +350,7 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         if (gt == 0) {
             c.ncp_stats[2] += it;         // CG iterations
             if (!conv) c.ncp_stats[3] += 1;  // CG attempts that fall back to a factorisation
+            flags[3] = conv ? 0 : 1;
         }
     }
     if (!solved) {
