@@ -225,7 +225,8 @@ void Engine::set_factor_build(int mode, int small_subtree_max) {
 }
 
 void Engine::set_st_schedule(int chunk_rows, int rows_in_flight) {
-    DPHD_CHECK(chunk_rows >= 8 && chunk_rows <= 4096, "S^T chunk rows must lie in [8, 4096]");
+    DPHD_CHECK(chunk_rows >= 8 && chunk_rows <= kStChunkMax,
+               "S^T chunk rows must lie in [8, " + std::to_string(kStChunkMax) + "]");
     DPHD_CHECK(rows_in_flight == 4 || rows_in_flight == 8, "S^T rows in flight must be 4 or 8");
     if (chunk_rows != st_chunk_rows_ || rows_in_flight != st_rows_) built_ = false;
     st_chunk_rows_ = chunk_rows;
@@ -712,7 +713,7 @@ void Engine::build_contact(double dt) {
     dc_Xt.alloc(kcap * kcap * sizeof(double));
     dc_X32.alloc(kcap * kcap * sizeof(float));
     dc_Xt32.alloc(kcap * kcap * sizeof(float));
-    dc_pcg.alloc((6 * kcap + 1024) * sizeof(double));
+    dc_pcg.alloc((8 * kcap + 1024) * sizeof(double));
     dc_actref.alloc((size_t)K * sizeof(int));
     dc_refpos.alloc((size_t)K * sizeof(int));
     CUDA_OK(cudaMemset(dc_refpos.p, 0xff, dc_refpos.bytes));  // -1: no candidate is in a cached list yet

@@ -534,12 +534,17 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
 }
 
 // x = S^T y, stage 1: one CTA per (column tile, chunk of the tile's row list); partial tile sums are written
-// to xpart[chunk] and summed in chunk order by stage 2.  Each warp takes every 8th row of the chunk and keeps
-// kStRows rows in flight.  FROM_ITEMS: y_r is summed here from the S pass's row-contiguous item partials (in
-// slot order, as the S fix-up kernel would), so the pair needs no separate fix-up launch.
+// to xpart[chunk] and summed in chunk order by stage 2.  The CTA first stages the chunk's row descriptors (first
+// column, length, S offset) and y values in shared memory -- one coalesced pass, so that the S loads below do
+// not wait on a descriptor load each -- then each warp takes every 8th row and keeps kStRows rows in flight.
+// FROM_ITEMS: y_r is summed here from the S pass's row-contiguous item partials (in slot order, as the S fix-up
+// kernel would), so the pair needs no separate fix-up launch.
 template <typename T, bool FROM_ITEMS, int kStRows>
 __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __restrict__ y, int ch, const Ctrl* ctrl) {
     __shared__ T red[8][3][kTileCols];
+    __shared__ int2 s_cl[kStChunkMax];        // per row of the chunk: first column, length of its padded segment
+    __shared__ long long s_off[kStChunkMax];  // S offset of the row's first value
+    __shared__ T s_y[3][kStChunkMax];
     const int done = ctrl->done;  // in flight together with the chunk's bounds; the same in every thread
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tile = __ldg(p.chunk_tile + ch);
@@ -552,57 +557,62 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
         for (int q = 0; q < 4; ++q) acc[d][q] = T(0);
     const int pe = __ldg(p.chunk_p1 + ch), p0 = __ldg(p.chunk_p0 + ch);
     if (done) return;
-    for (int pp = p0 + wid; pp < pe; pp += 8 * kStRows) {
-        int4 dsc[kStRows];
-        int64_t off[kStRows];
-#pragma unroll
-        for (int u = 0; u < kStRows; ++u) {
-            const int q = pp + 8 * u;
-            dsc[u] = make_int4(0, 0, 0, 0);
-            off[u] = 0;
-            if (q < pe) {
-                dsc[u] = __ldg(p.trow_desc + q);
-                off[u] = __ldg(p.trow_off + q);
+    const int cnt = pe - p0;  // <= kStChunkMax (the schedule's chunk rows)
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const int q = p0 + t;
+        const int4 dd = __ldg(p.trow_desc + q);
+        s_cl[t] = make_int2(dd.x, dd.y);
+        s_off[t] = __ldg(p.trow_off + q);
+        T y0 = T(0), y1 = T(0), y2 = T(0);
+        if (FROM_ITEMS) {
+            if (p.yrow) {  // one load per row: the item partial, or the row total of a multi-item row
+                if (dd.z < dd.w) {
+                    const T* src = (dd.w - dd.z > 1 ? p.yrow : p.ypart) + 3 * (size_t)dd.z;
+                    y0 = __ldg(src);
+                    y1 = __ldg(src + 1);
+                    y2 = __ldg(src + 2);
+                }
+            } else {
+                for (int k = dd.z; k < dd.w; ++k) {
+                    y0 += __ldg(p.ypart + 3 * (size_t)k);
+                    y1 += __ldg(p.ypart + 3 * (size_t)k + 1);
+                    y2 += __ldg(p.ypart + 3 * (size_t)k + 2);
+                }
             }
+        } else {
+            const int i = __ldg(p.tile_rows + q);
+            y0 = __ldg(y + i);
+            y1 = __ldg(y + npad + i);
+            y2 = __ldg(y + 2 * (size_t)npad + i);
         }
+        s_y[0][t] = y0;
+        s_y[1][t] = y1;
+        s_y[2][t] = y2;
+    }
+    __syncthreads();
+    for (int b = wid; b < cnt; b += 8 * kStRows) {
         Vec4<T> sv[kStRows];
-        T yv[kStRows][3];
         bool in[kStRows];
 #pragma unroll
         for (int u = 0; u < kStRows; ++u) {
-            in[u] = dsc[u].y > 0 && c >= dsc[u].x && c + 4 <= dsc[u].x + dsc[u].y;
-            if (in[u]) sv[u].load_s(p.vals + off[u] + (c - dsc[u].x), p.keep_in_l2);
-            yv[u][0] = yv[u][1] = yv[u][2] = T(0);
-            if (FROM_ITEMS) {
-                if (p.yrow) {  // one load per row: the item partial, or the row total of a multi-item row
-                    if (dsc[u].z < dsc[u].w) {
-                        const T* src = (dsc[u].w - dsc[u].z > 1 ? p.yrow : p.ypart) + 3 * (size_t)dsc[u].z;
-                        yv[u][0] = __ldg(src);
-                        yv[u][1] = __ldg(src + 1);
-                        yv[u][2] = __ldg(src + 2);
-                    }
-                } else {
-                    for (int k = dsc[u].z; k < dsc[u].w; ++k) {
-                        yv[u][0] += __ldg(p.ypart + 3 * (size_t)k);
-                        yv[u][1] += __ldg(p.ypart + 3 * (size_t)k + 1);
-                        yv[u][2] += __ldg(p.ypart + 3 * (size_t)k + 2);
-                    }
-                }
-            } else if (pp + 8 * u < pe) {
-                const int i = __ldg(p.tile_rows + pp + 8 * u);
-                yv[u][0] = __ldg(y + i);
-                yv[u][1] = __ldg(y + npad + i);
-                yv[u][2] = __ldg(y + 2 * (size_t)npad + i);
+            const int t = b + 8 * u;
+            in[u] = false;
+            if (t < cnt) {
+                const int2 cl = s_cl[t];
+                in[u] = cl.y > 0 && c >= cl.x && c + 4 <= cl.x + cl.y;
+                if (in[u]) sv[u].load_s(p.vals + s_off[t] + (c - cl.x), p.keep_in_l2);
             }
         }
 #pragma unroll
         for (int u = 0; u < kStRows; ++u)
             if (in[u]) {
+                const int t = b + 8 * u;
+                const T y0 = s_y[0][t], y1 = s_y[1][t], y2 = s_y[2][t];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    acc[0][q] += sv[u].v[q] * yv[u][0];
-                    acc[1][q] += sv[u].v[q] * yv[u][1];
-                    acc[2][q] += sv[u].v[q] * yv[u][2];
+                    acc[0][q] += sv[u].v[q] * y0;
+                    acc[1][q] += sv[u].v[q] * y1;
+                    acc[2][q] += sv[u].v[q] * y2;
                 }
             }
     }

@@ -125,6 +125,7 @@ struct SpmvPlan {
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
 constexpr int kChunkRows = 64;       // rows per S^T chunk CTA (default of the schedule)
+constexpr int kStChunkMax = 512;     // largest S^T chunk (its row descriptors are staged in shared memory)
 constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 constexpr int kGatherMaxThreads = 512;  // block-size bound of the node gathers
 

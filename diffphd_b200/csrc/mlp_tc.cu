@@ -1,4 +1,5 @@
-// Warm-start MLP inference (15 -> 128 -> 128 -> 3, GELU) on the 5th-generation tensor cores: tcgen05.mma with
+// Warm-start MLP inference (16 -> 128 -> 128 -> 8, GELU; the first 4 outputs are used) on the 5th-generation
+// tensor cores: tcgen05.mma with
 // BF16 operands in shared memory, FP32 accumulators in tensor memory (TMEM), read back with tcgen05.ld.
 //
 // One CTA of 128 threads works on tiles of 128 rows (nodes); thread t owns row t, which is TMEM lane t of every

@@ -29,6 +29,7 @@ constexpr int kLd = kT + 1;
 constexpr int kThr = 256;
 constexpr int kNcpPcgIters = 40;       // CG iteration cap for an unchanged list; + 2 per changed candidate
 constexpr int kNcpMaxListChange = 32;  // larger changes of the active list refactor at once
+constexpr double kOmegaMin = 1e-6;     // |omega| below this: the candidate's row is decoupled (E only)
 constexpr double kNcpPcgTol = 1e-13;
 constexpr long long kSpins = 1ll << 24;
 
@@ -175,7 +176,7 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
     double* rhs = c.rhs;
     double* x = c.xsol;
     double* dg = c.pcg + 5 * (size_t)ldx;    // diag(M)
-    double* part = c.pcg + 6 * (size_t)ldx;  // per-CTA partial sums
+    double* part = c.pcg + 8 * (size_t)ldx;  // per-CTA partial sums (omega_ref, kept with the factor, at 7 ldx)
     // [0] cached factor valid, [1] its ka, [2] candidates not in its list (this launch), [3] the last CG fell back
     int* flags = c.ncp_flags;
     const bool have = flags[0] != 0;
@@ -227,25 +228,37 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
     }
     if (n_new_w) atomicAdd(flags + 2, n_new_w);
     if (!gsync(c.bar, ctrl)) return;
-    // lists sorted by candidate index: no new candidate and the same count means the same list, position for position
+    // candidates whose positions changed: new to the list, or dropped from it
     const int n_new = have ? __ldcg(flags + 2) : 0;
     const int n_chg = n_new + (ka_ref - (ka - n_new));
-    const bool same = have && n_chg == 0;
     bool solved = false;
     if (have && n_chg <= kNcpMaxListChange) {
-        // ---- B: CG on M, preconditioned by the cached factor on the common candidates, diag(M) on the new ----
+        // ---- B: CG on M, preconditioned by the cached factor on the common candidates, diag(M) on the others ----
+        // M = Omega G Omega + E and M_ref = Omega_r G Omega_r + E_r, so with D = Omega Omega_r^-1 (diagonal)
+        // M = D M_ref D + (E - D^2 E_r): the preconditioner D^-1 X^T X D^-1 follows the change of Omega between PD
+        // iterations exactly and leaves only the diagonal change of E (small for resting contacts) to CG.
+        // Candidates with omega or omega_ref near 0 (decoupled rows E only) take the diagonal preconditioner.
         double* r = c.pcg;
         double* p = c.pcg + ldx;
         double* w = c.pcg + 2 * (size_t)ldx;
         double* t = c.pcg + 3 * (size_t)ldx;
-        double* zr = c.pcg + 4 * (size_t)ldx;  // X^T X r over the cached list (a changed list only)
-        if (!same) {
-            for (int a = gt; a < ka; a += nthr) {
-                const int pr = c.ref_pos[c.act[a]];
-                if (pr >= 0) c.ref_inv[pr] = a;
+        double* zr = c.pcg + 4 * (size_t)ldx;  // X^T X (D^-1 r) over the cached list
+        double* sc = c.pcg + 6 * (size_t)ldx;  // omega_ref / omega at a scaled common candidate, else 0
+        const double* om_ref = c.pcg + 7 * (size_t)ldx;
+        for (int a = gt; a < ld; a += nthr) {
+            double f = 0.0;
+            if (a < ka) {
+                const int k = c.act[a];
+                const int pr = c.ref_pos[k];
+                const double om = c.omega[k];
+                if (pr >= 0 && fabs(om) >= kOmegaMin && fabs(om_ref[pr]) >= kOmegaMin) {
+                    f = om_ref[pr] / om;
+                    c.ref_inv[pr] = a;
+                }
             }
-            if (!gsync(c.bar, ctrl)) return;
+            sc[a] = f;
         }
+        if (!gsync(c.bar, ctrl)) return;
         // r = rhs, x = 0, |rhs|^2
         double acc = 0.0;
         for (int a = gt; a < ld; a += nthr) {
@@ -264,50 +277,38 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         // after an attempt that fell back, the next one gets a quarter of the cap (a system far from the cached one)
         const int cap = (__ldcg(flags + 3) != 0 ? kNcpPcgIters / 4 : kNcpPcgIters) + 2 * n_chg;
         while (!conv && it < cap) {
-            // t = X r_ref over the cached list (one warp per row; r_ref = r at the common candidates, 0 at dropped)
+            // t = X (D^-1 r)_ref over the cached list (one warp per row; 0 at dropped or unscaled candidates)
             for (int a = gw; a < ld_ref; a += nwarps) {
                 const float* Xa = c.X32 + (size_t)a * ldx;
                 double s = 0.0;
-                if (same) {
-                    for (int b = lane; b <= a; b += 32) s += (double)Xa[b] * __ldcg(r + b);
-                } else {
-                    for (int b = lane; b <= a && b < ka_ref; b += 32) {
-                        const int nb_ = __ldcg(c.ref_inv + b);
-                        if (nb_ >= 0) s += (double)Xa[b] * __ldcg(r + nb_);
-                    }
+                for (int b = lane; b <= a && b < ka_ref; b += 32) {
+                    const int nb_ = __ldcg(c.ref_inv + b);
+                    if (nb_ >= 0) s += (double)Xa[b] * (__ldcg(r + nb_) * __ldcg(sc + nb_));
                 }
                 s = wsum(s);
                 if (lane == 0) t[a] = s;
             }
             if (!gsync(c.bar, ctrl)) return;
-            // z = X^T t (one warp per row of the stored transpose), rz_new = r . z; z kept in w
-            acc = 0.0;
+            // zr = X^T t (one warp per row of the stored transpose)
             for (int b = gw; b < ld_ref; b += nwarps) {
                 const float* Xb = c.Xt32 + (size_t)b * ldx;
                 double s = 0.0;
                 for (int a = b + lane; a < ld_ref; a += 32) s += (double)Xb[a] * __ldcg(t + a);
                 s = wsum(s);
-                if (lane == 0) {
-                    if (same) {
-                        w[b] = s;
-                        acc += __ldcg(r + b) * s;
-                    } else {
-                        zr[b] = s;
-                    }
-                }
+                if (lane == 0) zr[b] = s;
             }
-            if (!same) {  // z on the current list: the cached factor's value, or r / M_aa on a new candidate
-                if (!gsync(c.bar, ctrl)) return;
-                for (int a = gt; a < ld; a += nthr) {
-                    const double ra = __ldcg(r + a);
-                    double z = ra;
-                    if (a < ka) {
-                        const int pr = c.ref_pos[c.act[a]];
-                        z = pr >= 0 ? __ldcg(zr + pr) : (dg[a] > 0.0 ? ra / dg[a] : ra);
-                    }
-                    w[a] = z;
-                    acc += ra * z;
+            if (!gsync(c.bar, ctrl)) return;
+            // z on the current list (kept in w): D^-1 zr at the scaled candidates, r / M_aa elsewhere; rz = r . z
+            acc = 0.0;
+            for (int a = gt; a < ld; a += nthr) {
+                const double ra = __ldcg(r + a);
+                double z = ra;
+                if (a < ka) {
+                    const double f = __ldcg(sc + a);
+                    z = f != 0.0 ? __ldcg(zr + c.ref_pos[c.act[a]]) * f : (dg[a] > 0.0 ? ra / dg[a] : ra);
                 }
+                w[a] = z;
+                acc += ra * z;
             }
             cta_partial(wsum(acc), part);
             if (!gsync(c.bar, ctrl)) return;
@@ -511,10 +512,11 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             s = wsum(s);
             if (lane == 0) x[b] = s;
         }
-        // the new cached factor: its active list and the candidates' positions in it
+        // the new cached factor: its active list, the candidates' positions in it and their omega
         for (int a = gt; a < ka; a += nthr) {
             c.act_ref[a] = c.act[a];
             c.ref_pos[c.act[a]] = a;
+            c.pcg[7 * (size_t)ldx + a] = c.omega[c.act[a]];
         }
         if (gt == 0) {
             flags[0] = 1;

