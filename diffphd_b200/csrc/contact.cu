@@ -234,6 +234,7 @@ k_ncp_block_solve(ContactDev c, const double* __restrict__ q0, const int* __rest
         vcon[j] = r64 ? (T)r64[3 * node] : T(0);
         vcon[npad + j] = r64 ? (T)r64[3 * node + 1] : T(0);
         vcon[2 * (size_t)npad + j] = r64 ? (T)r64[3 * node + 2] : T(0);
+        for (int d = 0; d < 3; ++d) c.vc[3 * (size_t)k + d] = r64 ? r64[3 * node + d] : 0.0;
     }
     if (ka == 0) {
         for (int k = gt; k < K; k += nthr) c.lt1[k] = c.lt2[k] = 0.0;
@@ -495,9 +496,15 @@ k_ncp_block_solve(ContactDev c, const double* __restrict__ q0, const int* __rest
             const int node = c.cand[k], j = iperm[node];
             const double r0 = r64 ? r64[3 * node] : 0.0, r1 = r64 ? r64[3 * node + 1] : 0.0,
                          r2 = r64 ? r64[3 * node + 2] : 0.0;
-            vcon[j] = (T)(r0 + fn * n0 + t1v * c.t1[0] + t2v * c.t2[0]);
-            vcon[npad + j] = (T)(r1 + fn * n1 + t1v * c.t1[1] + t2v * c.t2[1]);
-            vcon[2 * (size_t)npad + j] = (T)(r2 + fn * n2 + t1v * c.t1[2] + t2v * c.t2[2]);
+            const double w0 = r0 + fn * n0 + t1v * c.t1[0] + t2v * c.t2[0];
+            const double w1 = r1 + fn * n1 + t1v * c.t1[1] + t2v * c.t2[1];
+            const double w2 = r2 + fn * n2 + t1v * c.t1[2] + t2v * c.t2[2];
+            vcon[j] = (T)w0;
+            vcon[npad + j] = (T)w1;
+            vcon[2 * (size_t)npad + j] = (T)w2;
+            c.vc[3 * (size_t)k] = w0;
+            c.vc[3 * (size_t)k + 1] = w1;
+            c.vc[3 * (size_t)k + 2] = w2;
         }
     }
 }
@@ -575,42 +582,72 @@ template void launch_ncp_iteration<float>(const ContactDev&, const double*, cons
                                           const double*, const int*, float*, const double*, Ctrl*, cudaStream_t);
 
 namespace {
-__global__ void k_permute_r64(int n, const double* __restrict__ r64, const int* __restrict__ iperm,
-                              double* __restrict__ v, int npad, const Ctrl* ctrl) {
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(256) k_path_apply(ContactDev c, const double* __restrict__ vsrc, int from_nodes,
+                                                    const TI* yin, TO* yout, int npad, const Ctrl* ctrl) {
     if (ctrl->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const int j = iperm[i];
-        v[j] = r64[3 * i];
-        v[npad + j] = r64[3 * i + 1];
-        v[2 * (size_t)npad + j] = r64[3 * i + 2];
-    } else if (i < npad) {  // padding rows of the permuted vector
-        v[i] = 0.0;
-        v[npad + i] = 0.0;
-        v[2 * (size_t)npad + i] = 0.0;
+    const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (u >= c.nU) return;
+    const int row = c.tp_row[u];
+    const int64_t e0 = c.tp_ptr[u], e1 = c.tp_ptr[u + 1];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        const int k = c.tp_k[e];
+        const double v = c.tp_val[e];
+        const double* src = vsrc + 3 * (size_t)(from_nodes ? c.cand[k] : k);
+        s0 += v * src[0];
+        s1 += v * src[1];
+        s2 += v * src[2];
+    }
+    s0 = warp_sum_d(s0);
+    s1 = warp_sum_d(s1);
+    s2 = warp_sum_d(s2);
+    if (lane == 0) {
+        const double a0 = (double)yin[row], a1 = (double)yin[npad + row], a2 = (double)yin[2 * (size_t)npad + row];
+        yout[row] = (TO)(a0 + s0);
+        yout[npad + row] = (TO)(a1 + s1);
+        yout[2 * (size_t)npad + row] = (TO)(a2 + s2);
     }
 }
 
-__global__ void k_cand_to_f32(ContactDev c, const int* __restrict__ iperm, const double* __restrict__ v64,
-                              float* __restrict__ v32, int npad, const Ctrl* ctrl) {
+__global__ void k_cand_zero(ContactDev c, const int* __restrict__ iperm, float* __restrict__ v, int npad,
+                            const Ctrl* ctrl) {
     if (ctrl->done) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= c.K) return;
     const int j = iperm[c.cand[k]];
-    v32[j] = (float)v64[j];
-    v32[npad + j] = (float)v64[npad + j];
-    v32[2 * (size_t)npad + j] = (float)v64[2 * (size_t)npad + j];
+    v[j] = 0.0f;
+    v[npad + j] = 0.0f;
+    v[2 * (size_t)npad + j] = 0.0f;
+}
+
+__global__ void k_path_gather_vals(long long E, const int64_t* __restrict__ src_e, const double* __restrict__ pval,
+                                   double* __restrict__ tp_val) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < E) tp_val[i] = pval[src_e[i]];
 }
 }  // namespace
 
-void launch_permute_r64(int n, const double* r64, const int* iperm, double* vperm64, int npad, const Ctrl* ctrl,
-                        cudaStream_t st) {
-    k_permute_r64<<<(npad + 255) / 256, 256, 0, st>>>(n, r64, iperm, vperm64, npad, ctrl);
+template <typename TI, typename TO>
+void launch_path_apply(const ContactDev& c, const double* v_src, int from_nodes, const TI* y_in, TO* y_out, int npad,
+                       const Ctrl* ctrl, cudaStream_t st) {
+    if (c.nU <= 0) return;
+    k_path_apply<TI, TO><<<(unsigned)(((long long)c.nU * 32 + 255) / 256), 256, 0, st>>>(c, v_src, from_nodes, y_in,
+                                                                                        y_out, npad, ctrl);
+}
+template void launch_path_apply<double, double>(const ContactDev&, const double*, int, const double*, double*, int,
+                                                const Ctrl*, cudaStream_t);
+template void launch_path_apply<float, double>(const ContactDev&, const double*, int, const float*, double*, int,
+                                               const Ctrl*, cudaStream_t);
+template void launch_path_apply<float, float>(const ContactDev&, const double*, int, const float*, float*, int,
+                                              const Ctrl*, cudaStream_t);
+
+void launch_cand_zero(const ContactDev& c, const int* iperm, float* v, int npad, const Ctrl* ctrl, cudaStream_t st) {
+    if (c.K > 0) k_cand_zero<<<(c.K + 255) / 256, 256, 0, st>>>(c, iperm, v, npad, ctrl);
 }
 
-void launch_cand_to_f32(const ContactDev& c, const int* iperm, const double* vcon64, float* vperm32, int npad,
-                        const Ctrl* ctrl, cudaStream_t st) {
-    if (c.K > 0) k_cand_to_f32<<<(c.K + 255) / 256, 256, 0, st>>>(c, iperm, vcon64, vperm32, npad, ctrl);
+void launch_path_gather_vals(long long E, const int64_t* src_e, const double* pval, double* tp_val, cudaStream_t st) {
+    if (E > 0) k_path_gather_vals<<<(unsigned)((E + 255) / 256), 256, 0, st>>>(E, src_e, pval, tp_val);
 }
 
 void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,

@@ -8,7 +8,7 @@
 // is block diagonal over the three directions, each block the node block G of A^-1 restricted to that
 // direction's nodes; their inverse factors X_b = L_b^-1 (G_b = L_b L_b^T) are formed once per adjoint step.
 // Per CG iteration:  y = S r;  u_b = d_b . (A^-1 r) at the constrained nodes (dots of their S column paths with y);
-// lam_b = X_b^T X_b u_b;  y -= S J^T lam (an S pass over the sparse right-hand side);  z = S^T y.
+// lam_b = X_b^T X_b u_b;  y -= S J^T lam (by the constrained candidates' S column paths);  z = S^T y.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -105,11 +105,11 @@ __global__ void k_wbp_transpose(int n, const double* __restrict__ X, double* __r
     }
 }
 
-// The S-pass input -J^T lam at the constrained nodes (the vector is zero elsewhere).
-template <typename T>
+// The S-pass input -J^T lam at the constrained candidates (zero at the others), per candidate: S (-J^T lam) is
+// then applied by the candidates' S column paths.
 __global__ void k_wbp_scatter(const int* __restrict__ count, const int* __restrict__ wcand, const int* __restrict__ wpos,
-                              ContactDev c, WbpDirs dirs, int cap, const double* __restrict__ lam,
-                              const int* __restrict__ iperm, T* __restrict__ vjac, int npad, const Ctrl* ctrl) {
+                              WbpDirs dirs, int cap, const double* __restrict__ lam, double* __restrict__ vk,
+                              const Ctrl* ctrl) {
     if (ctrl->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *count) return;
@@ -120,10 +120,10 @@ __global__ void k_wbp_scatter(const int* __restrict__ count, const int* __restri
         const double l = lam[(size_t)b * cap + pos];
         for (int d = 0; d < 3; ++d) v[d] -= l * dirs.d[b][d];
     }
-    const int j = iperm[c.cand[wcand[i]]];
-    vjac[j] = (T)v[0];
-    vjac[npad + j] = (T)v[1];
-    vjac[2 * (size_t)npad + j] = (T)v[2];
+    double* o = vk + 3 * (size_t)wcand[i];
+    o[0] = v[0];
+    o[1] = v[1];
+    o[2] = v[2];
 }
 
 // G_b (the direction's constrained candidates, identity-padded to n_pad) and X_b = I before the factorisation.
@@ -141,27 +141,23 @@ __global__ void k_wbp_gather_g(int n, int n_pad, const int* __restrict__ idx, co
 template <typename T>
 void launch_wbp_precond_parts(int stage, int cap, const int* count, const int* wcand, const int* wpos, const int* nb,
                               const ContactDev& c, const WbpDirs& dirs, const T* y, int npad, const double* X, int ld,
-                              double* u, double* w, double* lam, const int* iperm, T* vjac, const Ctrl* ctrl,
-                              cudaStream_t st) {
+                              double* u, double* w, double* lam, double* vk, const Ctrl* ctrl, cudaStream_t st) {
     if (cap <= 0) return;
     if (stage == 0) {  // u = J A^-1 r, lam = (J A^-1 J^T)^-1 u (X: three blocks, then their three transposes)
         const double* Xt = X + (size_t)3 * ld * ld;
         k_wbp_jdot<T><<<(cap * 32 + 255) / 256, 256, 0, st>>>(count, wcand, wpos, c, y, npad, dirs, cap, u, ctrl);
         k_wbp_trmv<<<(unsigned)(((long long)3 * cap * 32 + 255) / 256), 256, 0, st>>>(nb, X, ld, u, w, cap, ctrl);
         k_wbp_trmvt<<<(unsigned)(((long long)3 * cap * 32 + 255) / 256), 256, 0, st>>>(nb, Xt, ld, w, lam, cap, ctrl);
-    } else {  // the S-pass input -J^T lam
-        k_wbp_scatter<T><<<(cap + 255) / 256, 256, 0, st>>>(count, wcand, wpos, c, dirs, cap, lam, iperm, vjac, npad,
-                                                             ctrl);
+    } else {  // the S-pass input -J^T lam, per candidate
+        k_wbp_scatter<<<(cap + 255) / 256, 256, 0, st>>>(count, wcand, wpos, dirs, cap, lam, vk, ctrl);
     }
 }
 template void launch_wbp_precond_parts<double>(int, int, const int*, const int*, const int*, const int*,
                                                const ContactDev&, const WbpDirs&, const double*, int, const double*,
-                                               int, double*, double*, double*, const int*, double*, const Ctrl*,
-                                               cudaStream_t);
+                                               int, double*, double*, double*, double*, const Ctrl*, cudaStream_t);
 template void launch_wbp_precond_parts<float>(int, int, const int*, const int*, const int*, const int*,
                                               const ContactDev&, const WbpDirs&, const float*, int, const double*,
-                                              int, double*, double*, double*, const int*, float*, const Ctrl*,
-                                              cudaStream_t);
+                                              int, double*, double*, double*, double*, const Ctrl*, cudaStream_t);
 
 void launch_wbp_transpose(int n, const double* X, double* Xt, int ld, cudaStream_t st) {
     if (n <= 0) return;

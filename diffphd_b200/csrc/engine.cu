@@ -73,7 +73,6 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.fp32_projection = (int)get("fp32_projection", -1);
     o.ws_lambda = (int)get("ws_lambda", 0);
     o.ncp_solver = (int)get("ncp_solver", 1);
-    o.ncp_input_fp64 = (int)get("ncp_input_fp64", 0);
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -654,6 +653,7 @@ void Engine::build_device(int threads) {
 void Engine::build_contact(double dt) {
     has_contact_ = M.has_plane && !M.contact_nodes.empty();
     contact_ = ContactDev();
+    ++contact_gen_;  // G is rebuilt: factors cached from the old one are stale
     if (!has_contact_) return;
     const int K = (int)M.contact_nodes.size();
     DPHD_CHECK((double)K * K * 8 * 2 < 64e9, "too many contact candidates for the dense Delassus block");
@@ -689,6 +689,46 @@ void Engine::build_contact(double dt) {
         device_path_vals(K, dc_off.as<int64_t>(), dc_prow.as<int>(), dc_cand.as<int>(), d_iperm.as<int>(),
                          d_vals64.as<double>(), d_row_off.as<int64_t>(), d_row_a.as<int>(), dc_pval.as<double>(), 0);
         CUDA_OK(cudaDeviceSynchronize());
+    }
+    // The same entries by row: S v for v supported on the candidates is sum_k v_k S[:, j_k], and column j_k of
+    // S = L~^-1 P is nonzero only on the etree path of j_k, so the rows of U (the union of the paths) take it in
+    // O(path entries) instead of a full S pass.  Entries of a row in candidate order (a fixed summation order).
+    {
+        const int64_t E = P.off[K];
+        std::vector<int> cnt(M.n, 0);
+        for (int64_t e = 0; e < E; ++e) cnt[P.row[e]]++;
+        std::vector<int> urow;
+        std::vector<int64_t> uptr(1, 0), rpos(M.n, -1);
+        for (int r = 0; r < M.n; ++r)
+            if (cnt[r]) {
+                rpos[r] = uptr.back();
+                urow.push_back(r);
+                uptr.push_back(uptr.back() + cnt[r]);
+            }
+        std::vector<int> tk(E);
+        std::vector<int64_t> te(E);
+        for (int k = 0; k < K; ++k)
+            for (int64_t e = P.off[k]; e < P.off[k + 1]; ++e) {
+                const int64_t q = rpos[P.row[e]]++;
+                tk[q] = k;
+                te[q] = e;
+            }
+        dc_tprow.upload(urow);
+        dc_tpptr.upload(uptr);
+        dc_tpk.upload(tk);
+        DeviceBuffer src;
+        src.upload(te);
+        dc_tpval.alloc(std::max<size_t>(1, (size_t)E) * sizeof(double));
+        launch_path_gather_vals((long long)E, src.as<int64_t>(), dc_pval.as<double>(), dc_tpval.as<double>(), 0);
+        CUDA_OK(cudaDeviceSynchronize());
+        c.nU = (int)urow.size();
+        c.tp_row = dc_tprow.as<int>();
+        c.tp_ptr = dc_tpptr.as<int64_t>();
+        c.tp_k = dc_tpk.as<int>();
+        c.tp_val = dc_tpval.as<double>();
+        dc_vc.alloc((size_t)3 * K * sizeof(double));
+        CUDA_OK(cudaMemset(dc_vc.p, 0, dc_vc.bytes));
+        c.vc = dc_vc.as<double>();
     }
     dc_G.alloc((size_t)K * K * sizeof(double));
     launch_delassus(K, dc_off.as<int64_t>(), dc_prow.as<int>(), dc_pval.as<double>(), dc_G.as<double>(), 0);
@@ -823,23 +863,20 @@ void Engine::enqueue_contact_iteration(cudaStream_t st, bool f32) {
                                  d_qt.as<double>(), inv_h2m, d_fixed_node.as<unsigned char>(), d_iperm.as<int>(),
                                  d_vperm32.as<float>(), npad_, d_prev_pd.as<double>(), d_part_gate.as<double>(),
                                  gather_blocks_, Acsr_, d_x.as<double>(), 1, c, st, d_r64.as<double>());
-        if (ncp64in_) {
-            // the NCP's input A^-1 b = x + S^T-path(S r) from an FP64 S pass: r is not small at the candidates
-            // (it carries -J^T f there), so its FP32 image would leave rounding noise in the contact gaps
-            launch_permute_r64(n, d_r64.as<double>(), d_iperm.as<int>(), d_vperm64.as<double>(), npad_, c, st);
-            launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
-            launch_ncp_iteration<double>(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, d_x.as<double>(),
-                                         d_q0.as<double>(), d_iperm.as<int>(), d_vcon.as<double>(),
-                                         d_r64.as<double>(), c, st);
-            launch_cand_to_f32(contact_, d_iperm.as<int>(), d_vcon.as<double>(), d_vperm32.as<float>(), npad_, c,
-                               st);
-        } else {
-            launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
-            launch_ncp_iteration<float>(contact_, d_x.as<double>(), d_y32.as<float>(), npad_, d_x.as<double>(),
-                                        d_q0.as<double>(), d_iperm.as<int>(), d_vperm32.as<float>(),
-                                        d_r64.as<double>(), c, st);
-        }
-        launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);
+        // One S pass on the residual away from the candidates (small near the fixed point), the candidates' part
+        // by their S column paths in FP64: r carries -J^T f there, so its FP32 image would put rounding noise
+        // into the contact gaps, and after the NCP step the S input there becomes r + J^T f (small again).
+        launch_cand_zero(contact_, d_iperm.as<int>(), d_vperm32.as<float>(), npad_, c, st);
+        launch_s_only<float>(plan32_, d_vperm32.as<float>(), d_y32.as<float>(), c, st);  // y = S r_nc
+        // S r at the rows of U, for A^-1 b = x + S^T-path(S r) at the candidates
+        launch_path_apply<float, double>(contact_, d_r64.as<double>(), 1, d_y32.as<float>(), d_y64.as<double>(), npad_,
+                                         c, st);
+        launch_ncp_iteration<double>(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, d_x.as<double>(),
+                                     d_q0.as<double>(), d_iperm.as<int>(), d_vcon.as<double>(), d_r64.as<double>(),
+                                     c, st);
+        // y = S (r + J^T f): the candidates' inputs r + J^T f (FP64, from the NCP step) by their paths
+        launch_path_apply<float, float>(contact_, contact_.vc, 0, d_y32.as<float>(), d_y32.as<float>(), npad_, c,
+                                        st);
         SpmvPlan<float> ref = plan32_;
         ref.x_base = d_x.as<double>();
         launch_st_only<float>(ref, d_y32.as<float>(), d_xraw.as<double>(), c, st);
@@ -869,9 +906,8 @@ void Engine::enqueue_contact_iteration64(cudaStream_t st) {
     launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
     launch_ncp_iteration<double>(contact_, d_x.as<double>(), d_y64.as<double>(), npad_, nullptr,
                                  d_q0.as<double>(), d_iperm.as<int>(), d_vcon.as<double>(), nullptr, c, st);
-    SpmvPlan<double> acc = plan64_;
-    acc.y_accumulate = 1;
-    launch_s_only<double>(acc, d_vcon.as<double>(), d_y64.as<double>(), c, st);
+    // y += S J^T f by the candidates' S column paths (J^T f lives on the candidates only)
+    launch_path_apply<double, double>(contact_, contact_.vc, 0, d_y64.as<double>(), d_y64.as<double>(), npad_, c, st);
     launch_st_only<double>(plan64_, d_y64.as<double>(), d_xraw.as<double>(), c, st);
 }
 
@@ -976,10 +1012,10 @@ void Engine::enqueue_contact_precond(bool f32, bool woodbury, cudaStream_t st) {
             launch_wbp_precond_parts<float>(stage, K, d_wb_count.as<int>(), d_wbp_cand.as<int>(), d_wbp_pos.as<int>(),
                                             d_wbp_nb.as<int>(), contact_, wbp_dirs_, d_y32.as<float>(), npad_,
                                             d_wbp_X.as<double>(), ld, d_wbp_u.as<double>(), d_wbp_w.as<double>(),
-                                            d_wbp_lam.as<double>(), d_iperm.as<int>(), d_vjac32.as<float>(), c, st);
-        SpmvPlan<float> acc = plan32_;
-        acc.y_accumulate = 1;
-        launch_s_only<float>(acc, d_vjac32.as<float>(), d_y32.as<float>(), c, st);
+                                            d_wbp_lam.as<double>(), d_wbp_vk.as<double>(), c, st);
+        // y -= S J^T lam by the constrained candidates' S column paths (FP64 sums)
+        launch_path_apply<float, float>(contact_, d_wbp_vk.as<double>(), 0, d_y32.as<float>(), d_y32.as<float>(),
+                                        npad_, c, st);
         launch_st_only<float>(plan32_, d_y32.as<float>(), d_xraw.as<double>(), c, st);
     } else {
         launch_s_only<double>(plan64_, d_vperm64.as<double>(), d_y64.as<double>(), c, st);
@@ -988,10 +1024,9 @@ void Engine::enqueue_contact_precond(bool f32, bool woodbury, cudaStream_t st) {
                                              d_wbp_pos.as<int>(), d_wbp_nb.as<int>(), contact_, wbp_dirs_,
                                              d_y64.as<double>(), npad_, d_wbp_X.as<double>(), ld,
                                              d_wbp_u.as<double>(), d_wbp_w.as<double>(), d_wbp_lam.as<double>(),
-                                             d_iperm.as<int>(), d_vjac64.as<double>(), c, st);
-        SpmvPlan<double> acc = plan64_;
-        acc.y_accumulate = 1;
-        launch_s_only<double>(acc, d_vjac64.as<double>(), d_y64.as<double>(), c, st);
+                                             d_wbp_vk.as<double>(), c, st);
+        launch_path_apply<double, double>(contact_, d_wbp_vk.as<double>(), 0, d_y64.as<double>(),
+                                          d_y64.as<double>(), npad_, c, st);
         launch_st_only<double>(plan64_, d_y64.as<double>(), d_xraw.as<double>(), c, st);
     }
 }
@@ -1187,13 +1222,6 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
                 cudaGraphExecDestroy(graphs_[md]);
                 graphs_[md] = nullptr;
             }
-    }
-    if (has_contact_ && (o.ncp_input_fp64 != 0) != ncp64in_) {  // captured in the mixed contact graph
-        ncp64in_ = o.ncp_input_fp64 != 0;
-        if (graphs_[8]) {
-            cudaGraphExecDestroy(graphs_[8]);
-            graphs_[8] = nullptr;
-        }
     }
     if (has_contact_) {
         contact_.mu = o.friction_mu;
@@ -1657,9 +1685,8 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
         d_wbp_X.alloc(6 * ld * ld * sizeof(double));  // the three X_b, then their transposes
         d_wbp_M.alloc(ld * ld * sizeof(double));
         for (DeviceBuffer* b : {&d_wbp_u, &d_wbp_w, &d_wbp_lam}) b->alloc((size_t)3 * K * sizeof(double));
-        DeviceBuffer& vj = f32 ? d_vjac32 : d_vjac64;
-        vj.alloc((size_t)npad_ * 3 * (f32 ? sizeof(float) : sizeof(double)));
-        CUDA_OK(cudaMemsetAsync(vj.p, 0, vj.bytes, st));
+        d_wbp_vk.alloc((size_t)3 * K * sizeof(double));  // zero at the candidates without a constraint
+        CUDA_OK(cudaMemsetAsync(d_wbp_vk.p, 0, d_wbp_vk.bytes, st));
         CUDA_OK(cudaMemcpyAsync(d_wbp_cand.p, wcand.data(), wcand.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemcpyAsync(d_wbp_pos.p, wpos.data(), wpos.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         int nb[3] = {(int)idx[0].size(), (int)idx[1].size(), (int)idx[2].size()};
@@ -1667,6 +1694,11 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
         for (int b = 0; b < 3; ++b) {
             for (int d = 0; d < 3; ++d) wbp_dirs_.d[b][d] = dirs3[b][d];
             if (nb[b] == 0) continue;
+            // G_b depends only on A and the direction's constrained candidates: a reverse sweep whose consecutive
+            // steps constrain the same candidates keeps the factor of the previous step
+            if (wbp_gen_[b] == contact_gen_ && wbp_idx_prev_[b] == idx[b]) continue;
+            wbp_gen_[b] = contact_gen_;
+            wbp_idx_prev_[b] = idx[b];
             int* db_idx = d_wbp_idx.as<int>() + (size_t)b * K;
             CUDA_OK(cudaMemcpyAsync(db_idx, idx[b].data(), nb[b] * sizeof(int), cudaMemcpyHostToDevice, st));
             const int npd = (nb[b] + 63) / 64 * 64;
@@ -1674,8 +1706,8 @@ void Engine::contact_adjoint(const Options& o, const TapeFrame& fr, cudaStream_t
             launch_wbp_gather_g(nb[b], npd, db_idx, dc_G.as<double>(), K, d_wbp_M.as<double>(), Xb, (int)ld, st);
             dense_chol_solve(d_wbp_M.as<double>(), npd, Xb, (int)ld, npd, st);  // X_b = L_b^-1
             launch_wbp_transpose(nb[b], Xb, d_wbp_X.as<double>() + (size_t)(3 + b) * ld * ld, (int)ld, st);
+            launches_ += 3;  // gather, cooperative Cholesky, transpose
         }
-        launches_ += 4;
     }
     Ctrl* c = d_ctrl.as<Ctrl>();
     init_ctrl(h_ctrl_, 1, o, o.max_pd_iter, o.bwd_clip);

@@ -51,8 +51,6 @@ struct Options {
                                  // slower on the 64^3 contact rollout, so off by default)
     int fp32_projection = -1;    // mixed precision: 1 FP32 local projections, 0 FP64 projections with FP32 S
                                  // passes, -1 automatic (FP32 without a contact set, FP64 with one)
-    int ncp_input_fp64 = 0;      // mixed precision with contact: 1 computes the NCP's A^-1 b at the candidates
-                                 // with an FP64 S pass (the other S / S^T passes of the iteration stay FP32)
     int fp32_stall_window = 40;  // mixed precision: iterations without the gate ratio halving before the rest of
                                  // the frame continues in FP64 (0: never)
     static Options parse(const std::map<std::string, double>& m);
@@ -214,8 +212,7 @@ private:
     DeviceBuffer d_z1;  // constraint correction z - mu of the last contact-aware adjoint of a reverse sweep
     // constrained-inverse preconditioner: per constrained node its candidate and its position in each direction's
     // block, the block sizes, the blocks' inverse Cholesky factors, work vectors and the sparse S-pass input
-    DeviceBuffer d_wbp_cand, d_wbp_pos, d_wbp_nb, d_wbp_idx, d_wbp_X, d_wbp_M, d_wbp_u, d_wbp_w, d_wbp_lam;
-    DeviceBuffer d_vjac64, d_vjac32;
+    DeviceBuffer d_wbp_cand, d_wbp_pos, d_wbp_nb, d_wbp_idx, d_wbp_X, d_wbp_M, d_wbp_u, d_wbp_w, d_wbp_lam, d_wbp_vk;
     WbpDirs wbp_dirs_ = {};
     int z_hist_ = 0;
     double* h_cmp_ = nullptr;
@@ -233,7 +230,10 @@ private:
     int factor_mode_ = 0, small_subtree_max_ = 512;
     int st_chunk_rows_ = kChunkRows, st_rows_ = 4;
     bool proj32_ = true;  // precision of the projections captured in the mixed-precision iteration graphs
-    bool ncp64in_ = false;  // FP64 NCP input captured in the mixed-precision contact graph
+    // the contact-adjoint preconditioner's direction factors X_b: the G they were built from (generation of the
+    // contact set-up) and their constrained candidates, reused while both are unchanged
+    long long contact_gen_ = 0, wbp_gen_[3] = {-1, -1, -1};
+    std::vector<int> wbp_idx_prev_[3];
     bool factor_on_device_ = false;
     std::unique_ptr<SBuildPlan> sb_plan_;   // device build: plan and the permuted upper triangle of A, kept from
     std::unique_ptr<PermUpper> sb_upper_;   // the symbolic step until build_device runs the numeric one
@@ -294,7 +294,8 @@ private:
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0, dc_Xinv, dc_Xt, dc_pcg,
-        dc_actref, dc_flags, dc_stats, dc_X32, dc_Xt32, dc_refpos, dc_refinv;
+        dc_actref, dc_flags, dc_stats, dc_X32, dc_Xt32, dc_refpos, dc_refinv, dc_tprow, dc_tpptr, dc_tpk, dc_tpval,
+        dc_vc;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

@@ -124,7 +124,8 @@ struct SpmvPlan {
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
-constexpr int kChunkRows = 64;       // rows per S^T chunk CTA (default of the schedule)
+constexpr int kChunkRows = 512;      // rows per S^T chunk CTA (default of the schedule; measured on the 64^3
+                                     // contact block: 64 -> 512 rows took the FP32 pair from 4.05 to 3.60 ms)
 constexpr int kStChunkMax = 512;     // largest S^T chunk (its row descriptors are staged in shared memory)
 constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 constexpr int kGatherMaxThreads = 512;  // block-size bound of the node gathers
@@ -254,6 +255,14 @@ struct ContactDev {
     int* ncp_flags = nullptr;
     unsigned long long* ncp_stats = nullptr;
     int cached = 1;                  // 1: the cached-factor solve, 0: a fresh factorisation every PD iteration
+    // S v for v supported on the candidates, row by row: the rows of U (the union of the candidates' column
+    // paths), each with its (candidate, S value) entries in candidate order
+    int nU = 0;
+    const int* tp_row = nullptr;     // nU: row of S
+    const int64_t* tp_ptr = nullptr; // nU + 1
+    const int* tp_k = nullptr;       // entries: candidate
+    const double* tp_val = nullptr;  // entries: S[row, column of the candidate]
+    double* vc = nullptr;            // 3 K: the S-pass input at the candidates after the NCP step (FP64)
 };
 template <typename T>
 void launch_ncp_cached_solve(const ContactDev& c, const double* q0, const int* iperm, T* vcon, int npad,
@@ -267,8 +276,7 @@ struct WbpDirs {
 template <typename T>
 void launch_wbp_precond_parts(int stage, int cap, const int* count, const int* wcand, const int* wpos, const int* nb,
                               const ContactDev& c, const WbpDirs& dirs, const T* y, int npad, const double* X, int ld,
-                              double* u, double* w, double* lam, const int* iperm, T* vjac, const Ctrl* ctrl,
-                              cudaStream_t st);
+                              double* u, double* w, double* lam, double* vk, const Ctrl* ctrl, cudaStream_t st);
 void launch_wbp_gather_g(int n, int n_pad, const int* idx, const double* G, int K, double* M, double* X, int ldx,
                          cudaStream_t st);
 // Xt = transpose of the lower triangle of X (n x n, leading dimension ld)
@@ -287,12 +295,15 @@ template <typename T>
 void launch_ncp_iteration(const ContactDev& c, const double* x, const T* y, int npad, const double* x_base,
                           const double* q0, const int* iperm, T* vcon, const double* r64, Ctrl* ctrl,
                           cudaStream_t st);
-// Mixed precision with an FP64 NCP input: r (node order, FP64) into the permuted FP64 S-pass input, and the
-// candidates' FP64 S-pass inputs r + J^T f (written by the FP64 NCP step) into the FP32 S-pass input.
-void launch_permute_r64(int n, const double* r64, const int* iperm, double* vperm64, int npad, const Ctrl* ctrl,
-                        cudaStream_t st);
-void launch_cand_to_f32(const ContactDev& c, const int* iperm, const double* vcon64, float* vperm32, int npad,
-                        const Ctrl* ctrl, cudaStream_t st);
+// y_out = y_in + S v at the rows of U, v supported on the candidates (one warp per row, FP64 sums):
+// v_k = v_src[3 cand[k] + d] (node order, from_nodes) or v_src[3 k + d].  y_in may alias y_out.
+template <typename TI, typename TO>
+void launch_path_apply(const ContactDev& c, const double* v_src, int from_nodes, const TI* y_in, TO* y_out, int npad,
+                       const Ctrl* ctrl, cudaStream_t st);
+// zero the candidates' entries of a permuted S-pass input
+void launch_cand_zero(const ContactDev& c, const int* iperm, float* v, int npad, const Ctrl* ctrl, cudaStream_t st);
+// the values of the row-wise path entries from the column paths (set-up)
+void launch_path_gather_vals(long long E, const int64_t* src_e, const double* pval, double* tp_val, cudaStream_t st);
 void launch_restitution(const ContactDev& c, double* q, const double* q0, const double* v0, double h, double e,
                         double slop, cudaStream_t st);
 // y (+)= S v only (first half of the pair), and x = S^T y only (second half).

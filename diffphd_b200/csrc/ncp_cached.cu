@@ -166,6 +166,7 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         vcon[j] = r64 ? (T)r64[3 * node] : T(0);
         vcon[npad + j] = r64 ? (T)r64[3 * node + 1] : T(0);
         vcon[2 * (size_t)npad + j] = r64 ? (T)r64[3 * node + 2] : T(0);
+        for (int d = 0; d < 3; ++d) c.vc[3 * (size_t)k + d] = r64 ? r64[3 * node + d] : 0.0;
     }
     if (ka == 0) {
         for (int k = gt; k < K; k += nthr) c.lt1[k] = c.lt2[k] = 0.0;
@@ -581,9 +582,15 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             const int node = c.cand[k], j = iperm[node];
             const double r0 = r64 ? r64[3 * node] : 0.0, r1 = r64 ? r64[3 * node + 1] : 0.0,
                          r2 = r64 ? r64[3 * node + 2] : 0.0;
-            vcon[j] = (T)(r0 + fn * n0 + t1v * c.t1[0] + t2v * c.t2[0]);
-            vcon[npad + j] = (T)(r1 + fn * n1 + t1v * c.t1[1] + t2v * c.t2[1]);
-            vcon[2 * (size_t)npad + j] = (T)(r2 + fn * n2 + t1v * c.t1[2] + t2v * c.t2[2]);
+            const double w0 = r0 + fn * n0 + t1v * c.t1[0] + t2v * c.t2[0];
+            const double w1 = r1 + fn * n1 + t1v * c.t1[1] + t2v * c.t2[1];
+            const double w2 = r2 + fn * n2 + t1v * c.t1[2] + t2v * c.t2[2];
+            vcon[j] = (T)w0;
+            vcon[npad + j] = (T)w1;
+            vcon[2 * (size_t)npad + j] = (T)w2;
+            c.vc[3 * (size_t)k] = w0;
+            c.vc[3 * (size_t)k + 1] = w1;
+            c.vc[3 * (size_t)k + 2] = w2;
         }
     }
 }

@@ -52,16 +52,20 @@ def test_tet_block_bench_options_match_the_fp64_oracle(oracle_lib):
         positions within 1e-6;
       * the bench's path (FP32 bulk, learned start, adjoint warm start) at the 1e-6 gate against the converged
         trajectory (the FP64 path at the 1e-10 gate): no further from it than the oracle at the 1e-6 gate;
-      * the bench's adjoint around its own forward states against the oracle's FP64 adjoint around the same
-        states: relative gradient error <= 1e-4."""
+      * the bench's adjoint (PCG, mixed precision, warm-started) over the last 3 steps of the reverse sweep,
+        around its own forward states, against the oracle's FP64 adjoint around the same states at a 1e-9 gate:
+        relative gradient error <= 1e-4.  (The reference's adjoint fixed point with its default 500-iteration
+        cap is not converged on this block: 210% from its 1e-10 solution after 3 steps, 3.5e-4 with 5000
+        iterations, measured here on the CPU -- hence the converged oracle as the yardstick.)"""
     import torch
     from diffphd_b200.warmstart import WarmStartMLP, fit, generate_dataset
     dev = torch.device("cuda:0")
-    steps, tight_steps = 20, 2
+    steps, tight_steps, bwd_steps = 20, 2, 3
     sc = scenes.nh_tet_block(steps=steps)  # 32 x 16 x 16 cells, 9,537 nodes
     base = dict(sc.options, thread_ct=16)
     mixed = dict(base, fp32_bulk=1, alg_phd_bwd_solver=1, alg_phd_bwd_warm_start=3)
     tight = dict(base, rel_tol=1e-10, abs_tol=1e-14, max_pd_iter=20000)
+    tight_bwd = dict(base, rel_tol=1e-9, abs_tol=1e-14, max_pd_iter=20000)
     # a briefly trained warm-start network (held-out material seeds), attached as in the bench
     X, Y = generate_dataset(lambda s: scenes.nh_tet_block(seed=s), [1, 2], 8, dev, options=base)
     mlp = WarmStartMLP(dev, seed=0)
@@ -77,7 +81,7 @@ def test_tet_block_bench_options_match_the_fp64_oracle(oracle_lib):
     gq, gv = _T(r, dev), torch.zeros_like(qs[0])
     gpar = np.zeros(d.NumOfPdParams())
     dpar = torch.empty(d.NumOfPdParams(), dtype=torch.float64, device=dev)
-    for i in reversed(range(steps)):
+    for i in reversed(range(steps - bwd_steps, steps)):
         dq, dv, df = torch.empty_like(gq), torch.empty_like(gq), torch.empty_like(gq)
         d.backward_device(METHOD, qs[i + 1], gq, gv, sc.dt, mixed, dq, dv, df, dl_dparams=dpar)
         gpar += dpar.cpu().numpy()
@@ -98,16 +102,17 @@ def test_tet_block_bench_options_match_the_fp64_oracle(oracle_lib):
           f"from the converged trajectory: oracle at the 1e-6 gate {err_ref_gate:.2e}, bench path {err_bench:.2e}")
     assert err_fp64 <= 1e-6
     assert err_bench <= max(err_ref_gate, 1e-6)
-    # the adjoint: the oracle's FP64 reverse sweep around the bench path's forward states
+    # the adjoint: the oracle's FP64 reverse sweep around the bench path's forward states, over the last steps,
+    # converged (a 1e-9 gate)
     qn = [x.cpu().numpy() for x in qs]
     vn = [x.cpu().numpy() for x in vs]
     g, g_v = r.copy(), np.zeros(sc.dofs)
     opar = np.zeros(d.NumOfPdParams())
-    for i in reversed(range(steps)):
-        out = o.backward(qn[i], vn[i], sc.f_ext, sc.dt, qn[i + 1], g, g_v, base)
+    for i in reversed(range(steps - bwd_steps, steps)):
+        out = o.backward(qn[i], vn[i], sc.f_ext, sc.dt, qn[i + 1], g, g_v, tight_bwd)
         opar += np.concatenate(out["dl_dparams"])
         g, g_v = out["dl_dq"], out["dl_dv"]
-    for name, a, b in (("dl_dq0", gq.cpu().numpy(), g), ("dl_dv0", gv.cpu().numpy(), g_v), ("dl_dparams", gpar, opar)):
+    for name, a, b in (("dl_dq", gq.cpu().numpy(), g), ("dl_dv", gv.cpu().numpy(), g_v), ("dl_dparams", gpar, opar)):
         err = np.linalg.norm(a - b) / np.linalg.norm(b)
         print(f"  {name}: relative error {err:.2e}")
         assert err <= 1e-4, (name, err)
