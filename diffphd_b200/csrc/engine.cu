@@ -73,6 +73,8 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.fp32_projection = (int)get("fp32_projection", -1);
     o.ws_lambda = (int)get("ws_lambda", 0);
     o.ncp_solver = (int)get("ncp_solver", 1);
+    o.ncp_cg_tol = get("ncp_cg_tol", 1e-10);
+    DPHD_CHECK(o.ncp_cg_tol > 0.0 && o.ncp_cg_tol < 1.0, "ncp_cg_tol must lie in (0, 1)");
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
     DPHD_CHECK(o.max_pd_iter > 0, "max_pd_iter must be positive.");
@@ -1235,13 +1237,15 @@ void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, c
         }
         CUDA_OK(cudaMemsetAsync(dc_lt1.p, 0, dc_lt1.bytes, st));
         CUDA_OK(cudaMemsetAsync(dc_lt2.p, 0, dc_lt2.bytes, st));
-        if (graph_mu_ != o.friction_mu)  // the friction coefficient is captured in the contact iteration graphs
+        // the friction coefficient and the NCP's CG tolerance are captured in the contact iteration graphs
+        if (graph_mu_ != o.friction_mu || contact_.cg_tol != o.ncp_cg_tol)
             for (int md : {5, 8})
                 if (graphs_[md]) {
                     cudaGraphExecDestroy(graphs_[md]);
                     graphs_[md] = nullptr;
                 }
         graph_mu_ = o.friction_mu;
+        contact_.cg_tol = o.ncp_cg_tol;
         CUDA_OK(cudaMemsetAsync(dc_bar.p, 0, dc_bar.bytes, st));  // clears an abort left by an earlier solve
         // every frame starts without a cached NCP factor, so that a frame's result depends on its inputs (and the
         // multipliers' warm start) alone: a recomputed frame repeats the original bit for bit

@@ -46,6 +46,8 @@ struct Options {
     int ws_tcgen05 = 1;          // warm-start inference on tcgen05 MMAs with TMEM accumulators (0: mma.sync)
     int ncp_solver = 1;          // NCP dense solve: 1 CG preconditioned by a cached factor (refactored when the
                                  // active list changes or CG stalls), 0 a fresh Cholesky every PD iteration
+    double ncp_cg_tol = 1e-10;   // relative residual of the cached-factor CG (the semismooth Newton step it solves
+                                 // only has to be accurate well below the PD gate)
     int ws_lambda = 0;           // with a warm-start network and contact: 1 starts each frame's NCP from the
                                  // network's predicted multipliers instead of the previous frame's (measured
                                  // slower on the 64^3 contact rollout, so off by default)

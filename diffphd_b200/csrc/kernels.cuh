@@ -255,6 +255,7 @@ struct ContactDev {
     int* ncp_flags = nullptr;
     unsigned long long* ncp_stats = nullptr;
     int cached = 1;                  // 1: the cached-factor solve, 0: a fresh factorisation every PD iteration
+    double cg_tol = 1e-10;           // relative residual of the cached-factor CG
     // S v for v supported on the candidates, row by row: the rows of U (the union of the candidates' column
     // paths), each with its (candidate, S value) entries in candidate order
     int nU = 0;

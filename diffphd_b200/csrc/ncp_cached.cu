@@ -4,18 +4,20 @@
 //   A  assembles M (full rows, identity-padded to a multiple of 64) and the right-hand side, and counts the active
 //      candidates that are not in the list act_ref the cached factor was built for;
 //   B  when a cached factor X = L_ref^-1 of an earlier M_ref of this frame exists and the two lists differ in at
-//      most kNcpMaxListChange candidates: conjugate gradients on M to |r| <= 1e-13 |rhs|, preconditioned by
-//      P = (X^T X restricted to the candidates in both lists) (+) diag(M)^-1 on the new ones.  X^T X restricted to a
-//      subset of its list is the inverse of a Schur complement of M_ref, so P M differs from I by the change of
-//      Omega and E between the PD iterations plus a term of rank <= (dropped + 2 x new candidates); near the fixed
-//      point a few iterations suffice.  X is applied from FP32 copies (the preconditioner only has to be
-//      symmetric positive definite; the residual and the iterate are FP64);
+//      most kNcpMaxListChange candidates: conjugate gradients on M to |r| <= tol |rhs| (option ncp_cg_tol,
+//      1e-10 by default: the semismooth Newton step only has to be accurate well below the PD gate),
+//      preconditioned by D^-1 X^T X D^-1 on the candidates in both lists (D = Omega Omega_ref^-1, see phase B)
+//      and diag(M)^-1 on the others.  X^T X restricted to a subset of its list is the inverse of a Schur
+//      complement of M_ref, so P M differs from I by the change of E between the PD iterations plus a term of
+//      rank <= (dropped + 2 x new candidates); near the fixed point a few iterations suffice.  X is applied from
+//      FP32 copies (the preconditioner only has to be symmetric positive definite; the residual and the iterate
+//      are FP64);
 //   C  otherwise (no factor, a large change of the list, or CG not converged): the blocked Cholesky of M with the
 //      triangular solve of the identity folded in (X = L^-1, only the lower blocks, kept as the new cached factor),
 //      then dlambda = X^T (X rhs);
 //   D  clamp, Coulomb cone and the contact right-hand side, as k_ncp_block_solve.
-// Both paths solve the same system to rounding (the CG tolerance is 1e-13), so the iterates match the
-// refactor-every-iteration solve (option ncp_solver = 0) to that level.
+// Both paths solve the same system (to the CG tolerance), so the iterates match the refactor-every-iteration
+// solve (option ncp_solver = 0) to that level.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -30,7 +32,6 @@ constexpr int kThr = 256;
 constexpr int kNcpPcgIters = 40;       // CG iteration cap for an unchanged list; + 2 per changed candidate
 constexpr int kNcpMaxListChange = 32;  // larger changes of the active list refactor at once
 constexpr double kOmegaMin = 1e-6;     // |omega| below this: the candidate's row is decoupled (E only)
-constexpr double kNcpPcgTol = 1e-13;
 constexpr long long kSpins = 1ll << 24;
 
 __device__ __forceinline__ double wsum(double v) {
@@ -345,7 +346,7 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             if (!gsync(c.bar, ctrl)) return;
             const double rr = grid_total(part);
             ++it;
-            conv = pw > 0.0 && rr <= kNcpPcgTol * kNcpPcgTol * rhs2;
+            conv = pw > 0.0 && rr <= c.cg_tol * c.cg_tol * rhs2;
             if (!gsync(c.bar, ctrl)) return;
         }
         solved = conv;

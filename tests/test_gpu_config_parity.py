@@ -5,7 +5,8 @@
     a 1e-10 gate (relative position error <= 1e-6), the bench's path no further from the converged trajectory
     than the oracle at the 1e-6 gate, and its reverse sweep against the oracle's (gradient error <= 1e-4);
   * the 16x4x4 cantilever (425 nodes) for 100 steps: gradients w.r.t. q0, v0 and the per-element Young's moduli
-    (through the Lame chain of the per-element energy parameters) against central differences with eps 1e-7;
+    (through the Lame chain of the per-element energy parameters) against central differences (eps chosen
+    above the loss's convergence noise, see the test);
   * the 24^3 contact drop (rotated block, Coulomb mu 0.5, every node a candidate) for 24 steps in FP64: the same
     contact set as the oracle at every step (the oracle on an exactly prefiltered candidate set);
   * the reference's own backward (mean stiffness inside K_pd, deformable_projective_dynamics_backward.cpp:37-44,
@@ -127,11 +128,20 @@ def _cantilever_loss(sim, sc, q0, v0, params, steps):
 
 
 def test_cantilever_100_steps_gradients_match_central_differences():
+    """Gradients of r . q_100 through 100 steps of the heterogeneous cantilever w.r.t. v0, q0 and the per-element
+    Young's moduli, against central differences of the same GPU rollout.
+
+    The forward runs to a 1e-12 gate: the loss then moves by 2.5e-9 between the 1e-11 and 1e-12 gates (the
+    oracle, measured here on the CPU; 3,000-15,000 PD iterations per frame), so its noise is ~1e-10 and a
+    central difference resolves 1e-4 only where 2 eps |dL| is above ~1e-6.  Implicit Euler damps a random
+    velocity field's high modes within the 100 steps (dL/dv0 along one is ~3e-5), so the directions are the
+    cantilever's first bending shape for v0 and q0 and a random relative field for E, with eps 1e-2 (a 1 cm/s
+    tip velocity, a 10 um tip offset: both in the linear regime of a sag of centimetres) and 1e-3 for E."""
     import torch
     from diffphd_b200.autograd import DiffSim
     dev = torch.device("cuda:0")
     sc = scenes.cantilever(steps=100, heterogeneous=True)  # 16 x 4 x 4 hex cells, per-element E
-    opts = dict(sc.options, rel_tol=1e-12, abs_tol=1e-14, max_pd_iter=5000, alg_phd_bwd_solver=1)
+    opts = dict(sc.options, rel_tol=1e-12, abs_tol=1e-14, max_pd_iter=30000, alg_phd_bwd_solver=1)
     sim = DiffSim(sc, opts)
     q0 = _T(sc.q0, dev).requires_grad_(True)
     v0 = _T(sc.v0, dev).requires_grad_(True)
@@ -141,18 +151,21 @@ def test_cantilever_100_steps_gradients_match_central_differences():
     gq0, gv0, gp = q0.grad.cpu().numpy(), v0.grad.cpu().numpy(), p0.grad.cpu().numpy()
     sizes = sim.sizes
     dE, _ = scenes.chain_material_grad(sc, np.split(gp, np.cumsum(sizes)[:-1]))
-    rng = np.random.default_rng(3)
     free = np.ones(sc.dofs, bool)
     free[sc.dirichlet_dofs] = False
-    eps = 1e-7
+    x = sc.verts[:, 0] - sc.verts[:, 0].min()
+    bend = np.zeros((sc.n, 3))
+    bend[:, 2] = x / x.max()  # first bending shape: vertical, growing from the clamped face
+    bend = bend.ravel() * free
+    rng = np.random.default_rng(3)
     with torch.no_grad():
         def loss(q0n=sc.q0, v0n=sc.v0, E=sc.youngs):
             params = np.concatenate([np.atleast_1d(p) for _, p, _ in scenes.energy_params_from_material(sc, E)])
             return float(_cantilever_loss(sim, sc, _T(q0n, dev), _T(v0n, dev), _T(params, dev), sc.steps))
-        for name, grad, direction, fn in (
-                ("v0", gv0, rng.standard_normal(sc.dofs) * free, lambda t, dv: loss(v0n=sc.v0 + t * dv)),
-                ("q0", gq0, rng.standard_normal(sc.dofs) * free * 1e-3, lambda t, dq: loss(q0n=sc.q0 + t * dq)),
-                ("E", dE, rng.standard_normal(sc.m) * sc.youngs, lambda t, de: loss(E=sc.youngs + t * de))):
+        for name, grad, direction, eps, fn in (
+                ("v0", gv0, bend, 1e-2, lambda t, dv: loss(v0n=sc.v0 + t * dv)),
+                ("q0", gq0, bend * 1e-3, 1e-2, lambda t, dq: loss(q0n=sc.q0 + t * dq)),
+                ("E", dE, rng.standard_normal(sc.m) * sc.youngs, 1e-3, lambda t, de: loss(E=sc.youngs + t * de))):
             fd = (fn(eps, direction) - fn(-eps, direction)) / (2 * eps)
             an = float(grad @ direction)
             print(f"cantilever 100 steps, d/d{name}: adjoint {an:.9e}  FD {fd:.9e}")
