@@ -460,6 +460,7 @@ def run_ours(args, rank, world, local_rank):
                    "contact_candidates": d.num_contact_candidates(), "active_contacts_at_start": active,
                    "drop_height_m": DROP_HEIGHT if args.workload == "contact64" else None,
                    "nnz_S": nnz, "factor_build_s": round(t_build, 2),
+                   "contact_path_entries_rows_depth": list(d.contact_path_stats()),
                    "factor_built_on": "device" if d.factor_built_on_device() else "host",
                    "precision": "fp32 bulk (projection, S/S^T) + fp64 residual/gate/AA/NCP",
                    "pd_start": "learned warm start (per-node MLP, BF16 tensor cores)" if mlp is not None else "q",

@@ -77,6 +77,8 @@ def load_library():
     L.dphd_kernel_launches.restype = C.c_longlong
     L.dphd_device.argtypes = [C.c_void_p]
     L.dphd_debug_set_st_schedule.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.dphd_contact_path_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int)]
     L.dphd_debug_set_mma_wait_polls.argtypes = [C.c_longlong]
     L.dphd_fp64_escalations.argtypes = [C.c_void_p]
     L.dphd_ncp_solve_stats.argtypes = [C.c_void_p] + [C.POINTER(C.c_longlong)] * 4
@@ -345,6 +347,12 @@ class Deformable:
         """0 automatic, 1 host, 2 device construction of the sparse-inverse factor (next build); in device mode the
         etree subtrees of at most `small_subtree_max` nodes (512 when 0) are still built on the host."""
         self._check(self._L.dphd_debug_set_factor_build(self._h, int(mode), int(small_subtree_max)))
+
+    def contact_path_stats(self):
+        """(entries, rows of their union, longest path) of the contact candidates' S column paths."""
+        e, r, m = C.c_longlong(0), C.c_int(0), C.c_int(0)
+        self._check(self._L.dphd_contact_path_stats(self._h, C.byref(e), C.byref(r), C.byref(m)))
+        return e.value, r.value, m.value
 
     def set_st_schedule(self, chunk_rows, rows_in_flight):
         """Schedule of the S^T pass (rows per chunk CTA, rows in flight per warp: 4 or 8) for the next factor build."""

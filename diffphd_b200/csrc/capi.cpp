@@ -386,6 +386,12 @@ int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_
 int dphd_debug_set_st_schedule(dphd_deformable* h, int chunk_rows, int rows_in_flight) {
     return guard([&] { E(h).set_st_schedule(chunk_rows, rows_in_flight); });
 }
+int dphd_contact_path_stats(dphd_deformable* h, long long* entries, int* rows, int* max_depth) {
+    return guard([&] {
+        DPHD_CHECK(entries && rows && max_depth, "contact path stats: null pointer");
+        E(h).contact_path_stats(entries, rows, max_depth);
+    });
+}
 int dphd_factor_built_on_device(const dphd_deformable* h) {
     return h && h->eng ? h->eng->factor_built_on_device() : -1;
 }

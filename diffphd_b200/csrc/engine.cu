@@ -72,8 +72,9 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.fp32_stall_window = std::max(0, (int)get("fp32_stall_window", 40));
     o.fp32_projection = (int)get("fp32_projection", -1);
     o.ws_lambda = (int)get("ws_lambda", 0);
+    o.ws_contact_start = (int)get("ws_contact_start", 0);
     o.ncp_solver = (int)get("ncp_solver", 1);
-    o.ncp_cg_tol = get("ncp_cg_tol", 1e-10);
+    o.ncp_cg_tol = get("ncp_cg_tol", 1e-13);
     DPHD_CHECK(o.ncp_cg_tol > 0.0 && o.ncp_cg_tol < 1.0, "ncp_cg_tol must lie in (0, 1)");
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
@@ -724,6 +725,8 @@ void Engine::build_contact(double dt) {
         launch_path_gather_vals((long long)E, src.as<int64_t>(), dc_pval.as<double>(), dc_tpval.as<double>(), 0);
         CUDA_OK(cudaDeviceSynchronize());
         c.nU = (int)urow.size();
+        path_entries_ = (long long)E;
+        path_max_depth_ = P.max_depth;
         c.tp_row = dc_tprow.as<int>();
         c.tp_ptr = dc_tpptr.as<int64_t>();
         c.tp_k = dc_tpk.as<int>();
@@ -1290,6 +1293,7 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     const double h2m = dt * dt / M.mass();
     const bool learned = !d_init && ws_net_;
     ws_lambda_ = o.ws_lambda != 0;
+    ws_contact_start_ = o.ws_contact_start != 0;
     if (learned) d_init = ws_predict(dq, dv, df, dt, o.ws_tcgen05 != 0, st);
     // new-rollout detection of the contact tape (forward_gpu.cpp:437-449): the input must continue the last
     // frame; the comparison is read after the solve's own synchronisation
@@ -1405,6 +1409,11 @@ const double* Engine::ws_predict(const double* dq, const double* dv, const doubl
     }
     ws_apply(dt, base, d_ws_out.as<float>(), d_ws_qinit.as<double>(), st);
     launches_ += 1;
+    if (has_contact_ && ws_contact_start_) {
+        launch_ws_contact_start(contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), contact_.n, contact_.offset,
+                                d_fixed_dof.as<unsigned char>(), dq, d_ws_qinit.as<double>(), st);
+        launches_ += 1;
+    }
     if (has_contact_ && ws_lambda_) {  // the predicted initial contact multipliers replace the previous frame's
         launch_mlp_lambda_apply(contact_.K, dc_cand.as<int>(), d_ws_out.as<float>(), 1.0 / ws_lambda_scale(dt),
                                 dc_lam.as<double>(), st);

@@ -46,8 +46,11 @@ struct Options {
     int ws_tcgen05 = 1;          // warm-start inference on tcgen05 MMAs with TMEM accumulators (0: mma.sync)
     int ncp_solver = 1;          // NCP dense solve: 1 CG preconditioned by a cached factor (refactored when the
                                  // active list changes or CG stalls), 0 a fresh Cholesky every PD iteration
-    double ncp_cg_tol = 1e-10;   // relative residual of the cached-factor CG (the semismooth Newton step it solves
-                                 // only has to be accurate well below the PD gate)
+    double ncp_cg_tol = 1e-13;   // relative residual of the cached-factor CG (1e-10 measured slower on the 64^3
+                                 // contact rollout: inexact steps leave multipliers just above 0, and the active
+                                 // list, hence the cached factor, changes more often)
+    int ws_contact_start = 0;    // with a warm-start network and contact: 1 keeps the previous gap of the
+                                 // candidates in contact and lifts predicted penetrations to the plane
     int ws_lambda = 0;           // with a warm-start network and contact: 1 starts each frame's NCP from the
                                  // network's predicted multipliers instead of the previous frame's (measured
                                  // slower on the 64^3 contact rollout, so off by default)
@@ -165,6 +168,12 @@ public:
     // the S^T pass's schedule: rows per chunk CTA and rows in flight per warp (4 or 8); takes effect at the next
     // factor build
     void set_st_schedule(int chunk_rows, int rows_in_flight);
+    // the candidates' S column paths: total entries, rows of their union, longest path (0 without contact)
+    void contact_path_stats(long long* entries, int* rows, int* max_depth) const {
+        *entries = has_contact_ ? path_entries_ : 0;
+        *rows = has_contact_ ? contact_.nU : 0;
+        *max_depth = has_contact_ ? path_max_depth_ : 0;
+    }
     int factor_built_on_device() const { return factor_on_device_ ? 1 : 0; }
     static constexpr long long kDeviceBuildNnz = 32ll << 20;
     // CUDA device that holds this handle's GPU state (-1 until the first call that builds it); every later
@@ -235,6 +244,8 @@ private:
     // the contact-adjoint preconditioner's direction factors X_b: the G they were built from (generation of the
     // contact set-up) and their constrained candidates, reused while both are unchanged
     long long contact_gen_ = 0, wbp_gen_[3] = {-1, -1, -1};
+    long long path_entries_ = 0;  // entries of the candidates' S column paths; their longest path
+    int path_max_depth_ = 0;
     std::vector<int> wbp_idx_prev_[3];
     bool factor_on_device_ = false;
     std::unique_ptr<SBuildPlan> sb_plan_;   // device build: plan and the permuted upper triangle of A, kept from
@@ -293,6 +304,7 @@ private:
     DeviceBuffer d_ws_lamnode;   // node-indexed contact multipliers (the lambda feature)
     DeviceBuffer d_ws_lamprev;   // the multipliers at the last features call (the training target's baseline)
     bool ws_lambda_ = true;
+    bool ws_contact_start_ = false;
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0, dc_Xinv, dc_Xt, dc_pcg,

@@ -255,7 +255,7 @@ struct ContactDev {
     int* ncp_flags = nullptr;
     unsigned long long* ncp_stats = nullptr;
     int cached = 1;                  // 1: the cached-factor solve, 0: a fresh factorisation every PD iteration
-    double cg_tol = 1e-10;           // relative residual of the cached-factor CG
+    double cg_tol = 1e-13;           // relative residual of the cached-factor CG
     // S v for v supported on the candidates, row by row: the rows of U (the union of the candidates' column
     // paths), each with its (candidate, S value) entries in candidate order
     int nU = 0;
@@ -375,6 +375,8 @@ void launch_mlp_lambda_apply(int K, const int* cand, const float* out, double in
 void launch_mlp_apply(int n3, const double* base, const float* out, double dx, const unsigned char* fixed_dof,
                       const double* fval, double* q_init, cudaStream_t st);
 void launch_mlp_target(int n3, const double* q_next, const double* base, double inv_dx, float* Y, cudaStream_t st);
+void launch_ws_contact_start(int K, const int* cand, const double* lam, const double* n, double off,
+                             const unsigned char* fixed_dof, const double* q_prev, double* q_init, cudaStream_t st);
 
 // Device-side adjoint routing (backward_gpu.cpp:881-917) and parameter-gradient reductions.
 // g_bar = dl_dq_next + dl_dv_next / h;  dl_dq = -dl_dv_next / h;  |g_bar| into norm_out[0].

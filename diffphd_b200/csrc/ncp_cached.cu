@@ -4,8 +4,8 @@
 //   A  assembles M (full rows, identity-padded to a multiple of 64) and the right-hand side, and counts the active
 //      candidates that are not in the list act_ref the cached factor was built for;
 //   B  when a cached factor X = L_ref^-1 of an earlier M_ref of this frame exists and the two lists differ in at
-//      most kNcpMaxListChange candidates: conjugate gradients on M to |r| <= tol |rhs| (option ncp_cg_tol,
-//      1e-10 by default: the semismooth Newton step only has to be accurate well below the PD gate),
+//      most kNcpMaxListChange candidates: conjugate gradients on M to |r| <= tol |rhs| (option ncp_cg_tol, 1e-13
+//      by default: looser steps leave multipliers just above 0 and change the active list more often),
 //      preconditioned by D^-1 X^T X D^-1 on the candidates in both lists (D = Omega Omega_ref^-1, see phase B)
 //      and diag(M)^-1 on the others.  X^T X restricted to a subset of its list is the inverse of a Schur
 //      complement of M_ref, so P M differs from I by the change of E between the PD iterations plus a term of

@@ -118,6 +118,10 @@ int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_
  * at the rounding level between schedules.  Takes effect at the next factor build.  No counterpart in the
  * reference. */
 int dphd_debug_set_st_schedule(dphd_deformable* h, int chunk_rows, int rows_in_flight);
+/* The contact candidates' S column paths (after the factor build): total entries, rows of their union (the
+ * rows a path product S v writes for v supported on the candidates), longest path.  Zeros without a contact
+ * plane.  No counterpart in the reference. */
+int dphd_contact_path_stats(dphd_deformable* h, long long* entries, int* rows, int* max_depth);
 /* 1 when the current factor was built on the device, 0 on the host, -1 for a null handle. */
 int dphd_factor_built_on_device(const dphd_deformable* h);
 /* CUDA device that holds this handle's GPU state: -1 until the first call that builds the factor (it records

@@ -8,7 +8,8 @@
     (through the Lame chain of the per-element energy parameters) against central differences (eps chosen
     above the loss's convergence noise, see the test);
   * the 24^3 contact drop (rotated block, Coulomb mu 0.5, every node a candidate) for 24 steps in FP64: the same
-    contact set as the oracle at every step (the oracle on an exactly prefiltered candidate set);
+    contact set as the oracle at every step (the oracle on an exactly prefiltered candidate set) and positions
+    within the gate's accuracy;
   * the reference's own backward (mean stiffness inside K_pd, deformable_projective_dynamics_backward.cpp:37-44,
     option bwd_mean_stiffness) against the oracle in the same mode.
 """
@@ -174,16 +175,18 @@ def test_cantilever_100_steps_gradients_match_central_differences():
 
 def test_contact_drop_24_cubed_has_the_oracles_contact_sets(oracle_lib):
     """The 24^3 drop with every node a candidate runs on the GPU; the oracle, whose Delassus block is dense over its
-    candidates (a 15,625^2 block of A^-1 columns per step), runs the same rollout on the nodes that start within
-    3 cells of the lowest one.  That prefilter is exact for this rollout -- asserted: every node the GPU ever puts
-    in contact is among them, and the GPU rollout on the prefiltered set equals the full one.  Two frames of
-    this rollout reach the 500-iteration cap in both implementations (the reference's coupled PD / NCP iteration
-    does not settle there); their iterates still agree."""
+    candidates (a 15,625^2 block of A^-1 columns per step), runs the same rollout on the 628 nodes that start
+    within 6 cells of the lowest one (the GPU puts nodes up to 3.34 cells above it in contact).  That prefilter
+    is exact for this rollout -- asserted: every node the GPU ever puts in contact is among them, and the GPU
+    rollout on the prefiltered set has the full one's contact sets and positions (to the summation-order
+    rounding of the longer candidate list).  Frames of this rollout can reach the 500-iteration cap (the
+    reference's coupled PD / NCP iteration does not settle there at the 1e-6 gate), so positions are compared
+    at the gate's accuracy (1e-4 of the displacement); the contact sets exactly."""
     import copy
     sc = scenes.contact_drop(height=0.002, steps=24)  # 24^3 hex block, seeded rotation, Coulomb mu 0.5
     opts = dict(sc.options, thread_ct=16)
     z0 = sc.q0.reshape(-1, 3)[:, 2]
-    sub = np.nonzero(z0 <= z0.min() + 3.0 * 0.01)[0]
+    sub = np.nonzero(z0 <= z0.min() + 6.0 * 0.01)[0]
     sc_sub = copy.copy(sc)
     sc_sub.plane = (sc.plane[0], sub)
 
@@ -206,13 +209,13 @@ def test_contact_drop_24_cubed_has_the_oracles_contact_sets(oracle_lib):
     assert set().union(*a_all) <= set(sub.tolist())     # the prefilter loses no contact
     assert a_all == a_sub
     for a, b in zip(q_all, q_sub):
-        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
     o = oracle_lib.OracleDeformable.from_scene(sc_sub)
     qo, vo = sc.q0.copy(), sc.v0.copy()
     for t in range(sc.steps):
         qo, vo, act_o = o.forward(qo, vo, sc.f_ext, sc.dt, opts)
         assert a_sub[t] == set(act_o.tolist()), (t, len(a_sub[t]), len(act_o))
-        assert np.linalg.norm(q_sub[t] - qo) / np.linalg.norm(qo) <= 1e-6
+        assert np.abs(q_sub[t] - qo).max() <= 1e-4 * np.abs(qo - sc.q0).max()
 
 
 def test_reference_mean_stiffness_backward_matches_the_oracle(oracle_lib):
