@@ -75,7 +75,6 @@ Options Options::parse(const std::map<std::string, double>& m) {
     o.ws_contact_start = (int)get("ws_contact_start", 0);
     o.ncp_solver = (int)get("ncp_solver", 1);
     o.ncp_cg_tol = get("ncp_cg_tol", 1e-13);
-    o.bf16_factor = (int)get("bf16_factor", 0);
     DPHD_CHECK(o.ncp_cg_tol > 0.0 && o.ncp_cg_tol < 1.0, "ncp_cg_tol must lie in (0, 1)");
     DPHD_CHECK(o.aa_window >= 0 && o.aa_window <= kMaxWindow,
                "aa_window must be in [0, " + std::to_string(kMaxWindow) + "]");
@@ -280,7 +279,6 @@ void Engine::ensure_built(double dt, int threads) {
 
 void Engine::build_device(int threads) {
     (void)threads;
-    d_vals16.release();  // a BF16 copy of an earlier factor is stale; made again on first use
     if (device_ < 0) CUDA_OK(cudaGetDevice(&device_));
     if (!stream_) CUDA_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     if (!h_ctrl_) CUDA_OK(cudaMallocHost(&h_ctrl_, sizeof(Ctrl)));
@@ -1207,25 +1205,9 @@ void Engine::check_status(const char* where) {
         throw Error(std::string(where) + ": the contact solve's grid barrier timed out (CTAs not co-resident)");
 }
 
-// The FP32 passes read the FP32 factor or its BF16 copy (option bf16_factor; made on first use).  Every graph
-// captures the plan by value, so a change drops them.
-void Engine::apply_factor_precision(const Options& o) {
-    const bool want = o.bf16_factor != 0;
-    if (want == (plan32_.vals16 != nullptr)) return;
-    if (want && !d_vals16.p) {
-        d_vals16.alloc(d_vals64.bytes / sizeof(double) * sizeof(uint16_t));
-        device_round_bf16(d_vals64.as<double>(), d_vals16.as<uint16_t>(), (long long)(d_vals64.bytes / sizeof(double)),
-                          stream_);
-        CUDA_OK(cudaStreamSynchronize(stream_));
-    }
-    drop_graphs();
-    plan32_.vals16 = want ? d_vals16.as<uint16_t>() : nullptr;
-}
-
 void Engine::run_forward_loop(const double* dq_in, double h, const Options& o, cudaStream_t st,
                               const double* d_init) {
     const int n3 = 3 * M.n;
-    apply_factor_precision(o);
     Ctrl* c = d_ctrl.as<Ctrl>();
     CUDA_OK(cudaMemcpyAsync(d_x.p, d_init ? d_init : dq_in, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CUDA_OK(cudaMemsetAsync(d_prev_pd.p, 0, n3 * sizeof(double), st));
@@ -1804,7 +1786,6 @@ void Engine::backward_core(const double* d_q_next, const double* d_gq, const dou
                            double* d_dparams, double* d_dstate_p, cudaStream_t st, const double* d_q,
                            const double* d_v, const double* d_f) {
     ensure_built(dt, o.thread_ct);
-    apply_factor_precision(o);
     const int n3 = 3 * M.n, m = M.m;
     // the contact frame of this step (tape, or a replayed forward step), before anything below uses d_x
     std::unique_ptr<TapeFrame> frame;

@@ -56,8 +56,6 @@ struct Options {
                                  // slower on the 64^3 contact rollout, so off by default)
     int fp32_projection = -1;    // mixed precision: 1 FP32 local projections, 0 FP64 projections with FP32 S
                                  // passes, -1 automatic (FP32 without a contact set, FP64 with one)
-    int bf16_factor = 0;         // mixed precision: 1 the FP32 S / S^T passes read a BF16 copy of the factor (half
-                                 // the bytes; refinement form and FP64 residuals keep the fixed points)
     int fp32_stall_window = 40;  // mixed precision: iterations without the gate ratio halving before the rest of
                                  // the frame continues in FP64 (0: never)
     static Options parse(const std::map<std::string, double>& m);
@@ -170,7 +168,6 @@ public:
     // the S^T pass's schedule: rows per chunk CTA and rows in flight per warp (4 or 8); takes effect at the next
     // factor build
     void set_st_schedule(int chunk_rows, int rows_in_flight);
-    void apply_factor_precision(const Options& o);
     // the candidates' S column paths: total entries, rows of their union, longest path (0 without contact)
     void contact_path_stats(long long* entries, int* rows, int* max_depth) const {
         *entries = has_contact_ ? path_entries_ : 0;
@@ -312,7 +309,7 @@ private:
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0, dc_Xinv, dc_Xt, dc_pcg,
         dc_actref, dc_flags, dc_stats, dc_X32, dc_Xt32, dc_refpos, dc_refinv, dc_tprow, dc_tpptr, dc_tpk, dc_tpval,
-        dc_vc, d_vals16;
+        dc_vc;
     Ctrl* h_ctrl_ = nullptr;  // pinned mirror
 };
 

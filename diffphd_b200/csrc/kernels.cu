@@ -326,24 +326,6 @@ template <> struct Vec4<float> {
         else load_stream(p);
     }
 };
-// Four S values into FP32 registers: from the FP32 factor, or from its BF16 copy (the upper 16 bits of the FP32
-// value, rounded to nearest even; widening is a shift).  Rows start at multiples of 4 values, so a BF16 group
-// of 4 is an aligned 8-byte load.
-__device__ __forceinline__ void load_s4(const float* p, int keep, Vec4<float>& o) { o.load_s(p, keep); }
-__device__ __forceinline__ void load_s4(const uint16_t* p, int keep, Vec4<float>& o) {
-    const uint2 x = keep ? __ldg(reinterpret_cast<const uint2*>(p)) : __ldcs(reinterpret_cast<const uint2*>(p));
-    o.v[0] = __uint_as_float(x.x << 16);
-    o.v[1] = __uint_as_float(x.x & 0xffff0000u);
-    o.v[2] = __uint_as_float(x.y << 16);
-    o.v[3] = __uint_as_float(x.y & 0xffff0000u);
-}
-template <typename V>
-__device__ __forceinline__ const V* s_values(const SpmvPlan<float>& p);
-template <>
-__device__ __forceinline__ const float* s_values<float>(const SpmvPlan<float>& p) { return p.vals; }
-template <>
-__device__ __forceinline__ const uint16_t* s_values<uint16_t>(const SpmvPlan<float>& p) { return p.vals16; }
-
 template <> struct Vec4<double> {
     double v[4];
     __device__ __forceinline__ void load(const double* p) {
@@ -454,7 +436,6 @@ __global__ void __launch_bounds__(256) k_spmv_S_items(SpmvPlan<T> p, const T* __
 // of S of every row of the unit, so v is read once per unit instead of once per row, and every lane keeps up to
 // kUnitRows + 3 independent 16-byte loads in flight.  Rows shorter than the unit's widest row are masked per
 // float4 (row lengths and segment starts are multiples of 4).  Partial sums go to the rows' item slots.
-template <typename V>
 __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const float* __restrict__ v,
                                                       const Ctrl* ctrl) {
     pdl_enter();
@@ -464,16 +445,15 @@ __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const f
     const int4 ud = __ldg(p.unit_desc + u);
     if (done) return;
     const int first = ud.x, nr = ud.y, a = ud.z, ncmax = ud.w;
-    const V* vals = s_values<V>(p);
-    const V* sp[kUnitRows];
+    const float* sp[kUnitRows];
     int nc[kUnitRows];
 #pragma unroll
     for (int r = 0; r < kUnitRows; ++r) {
-        sp[r] = vals;
+        sp[r] = p.vals;
         nc[r] = 0;
         if (r < nr) {
             const int4 d = __ldg(p.unit_item_desc + first + r);
-            sp[r] = vals + ((int64_t)(uint32_t)d.x | ((int64_t)d.y << 32));
+            sp[r] = p.vals + ((int64_t)(uint32_t)d.x | ((int64_t)d.y << 32));
             nc[r] = d.w;
         }
     }
@@ -491,7 +471,7 @@ __global__ void __launch_bounds__(256) k_spmv_S_units(SpmvPlan<float> p, const f
         x2.load(v2 + c);
 #pragma unroll
         for (int r = 0; r < kUnitRows; ++r) {
-            if (c < nc[r]) load_s4(sp[r] + c, p.keep_in_l2, sv[r]);
+            if (c < nc[r]) sv[r].load_s(sp[r] + c, p.keep_in_l2);
             else sv[r].v[0] = sv[r].v[1] = sv[r].v[2] = sv[r].v[3] = 0.f;
         }
 #pragma unroll
@@ -559,7 +539,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_S_fin(SpmvPlan<T> p, T* __res
 // not wait on a descriptor load each -- then each warp takes every 8th row and keeps kStRows rows in flight.
 // FROM_ITEMS: y_r is summed here from the S pass's row-contiguous item partials (in slot order, as the S fix-up
 // kernel would), so the pair needs no separate fix-up launch.
-template <typename T, bool FROM_ITEMS, int kStRows, typename V = T>
+template <typename T, bool FROM_ITEMS, int kStRows>
 __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __restrict__ y, int ch, const Ctrl* ctrl) {
     __shared__ T red[8][3][kTileCols];
     __shared__ int2 s_cl[kStChunkMax];        // per row of the chunk: first column, length of its padded segment
@@ -610,9 +590,6 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
         s_y[2][t] = y2;
     }
     __syncthreads();
-    const V* vals;
-    if constexpr (std::is_same<V, T>::value) vals = p.vals;
-    else vals = p.vals16;
     for (int b = wid; b < cnt; b += 8 * kStRows) {
         Vec4<T> sv[kStRows];
         bool in[kStRows];
@@ -623,10 +600,7 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
             if (t < cnt) {
                 const int2 cl = s_cl[t];
                 in[u] = cl.y > 0 && c >= cl.x && c + 4 <= cl.x + cl.y;
-                if (in[u]) {
-                    if constexpr (std::is_same<V, T>::value) sv[u].load_s(vals + s_off[t] + (c - cl.x), p.keep_in_l2);
-                    else load_s4(vals + s_off[t] + (c - cl.x), p.keep_in_l2, sv[u]);
-                }
+                if (in[u]) sv[u].load_s(p.vals + s_off[t] + (c - cl.x), p.keep_in_l2);
             }
         }
 #pragma unroll
@@ -657,10 +631,10 @@ __device__ __forceinline__ void st_part_body(const SpmvPlan<T>& p, const T* __re
     __syncthreads();  // `red` is reused by the next chunk of a persistent CTA
 }
 
-template <typename T, bool FROM_ITEMS, int kStRows, typename V = T>
+template <typename T, bool FROM_ITEMS, int kStRows>
 __global__ void __launch_bounds__(256) k_spmv_ST_part(SpmvPlan<T> p, const T* __restrict__ y, const Ctrl* ctrl) {
     pdl_enter();
-    st_part_body<T, FROM_ITEMS, kStRows, V>(p, y, blockIdx.x, ctrl);
+    st_part_body<T, FROM_ITEMS, kStRows>(p, y, blockIdx.x, ctrl);
 }
 
 // x = S^T y, stage 2: per tile column, sum the chunk partials in order and scatter to node-major x.
@@ -1737,13 +1711,6 @@ void launch_gather_fwd(int n, const int* node_ptr, const int* node_inc, const do
 // stage 1 of x = S^T y with the plan's rows in flight per warp
 template <typename T, bool FROM_ITEMS>
 static void launch_st_part(const SpmvPlan<T>& p, const T* y, const Ctrl* ctrl, cudaStream_t st) {
-    if constexpr (std::is_same<T, float>::value) {
-        if (p.vals16) {  // the BF16 copy of the factor
-            if (p.st_rows == 8) launch_k(k_spmv_ST_part<T, FROM_ITEMS, 8, uint16_t>, p.n_chunks, 256, 0, st, p, y, ctrl);
-            else launch_k(k_spmv_ST_part<T, FROM_ITEMS, 4, uint16_t>, p.n_chunks, 256, 0, st, p, y, ctrl);
-            return;
-        }
-    }
     if (p.st_rows == 8) launch_k(k_spmv_ST_part<T, FROM_ITEMS, 8>, p.n_chunks, 256, 0, st, p, y, ctrl);
     else launch_k(k_spmv_ST_part<T, FROM_ITEMS, 4>, p.n_chunks, 256, 0, st, p, y, ctrl);
 }
@@ -1752,12 +1719,8 @@ static void launch_st_part(const SpmvPlan<T>& p, const T* y, const Ctrl* ctrl, c
 template <typename T>
 static void launch_s_items(const SpmvPlan<T>& p, const T* v, const Ctrl* ctrl, cudaStream_t st) {
     if constexpr (std::is_same<T, float>::value) {
-        if (p.vals16 && p.n_units > 0) {  // the BF16 copy of the factor: always the row-group kernel
-            launch_k(k_spmv_S_units<uint16_t>, blocks_for((long long)p.n_units * 32, 256), 256, 0, st, p, v, ctrl);
-            return;
-        }
         if (p.use_units && p.n_units > 0) {
-            launch_k(k_spmv_S_units<float>, blocks_for((long long)p.n_units * 32, 256), 256, 0, st, p, v, ctrl);
+            launch_k(k_spmv_S_units, blocks_for((long long)p.n_units * 32, 256), 256, 0, st, p, v, ctrl);
             return;
         }
     }

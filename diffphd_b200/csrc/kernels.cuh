@@ -76,7 +76,6 @@ struct SpmvPlan {
     const int* row_a = nullptr;
     const int* row_len = nullptr;
     const T* vals = nullptr;
-    const uint16_t* vals16 = nullptr;  // FP32 plans: a BF16 copy of the factor, read instead of vals when set
     int keep_in_l2 = 0;  // S fits comfortably in L2: ordinary cached loads instead of evict-first streaming
     // y = S v: work items (row, first column, column count) of at most kSegCols columns, one warp each;
     // items of the same nested-dissection separator and column segment are adjacent so that the warps of
@@ -328,8 +327,6 @@ struct SBuildPlan;
 void device_build_factor(const SBuildPlan& P, const std::vector<int>& lo, const int64_t* d_ro, const int* d_ra,
                          const int* d_rl, double* d_vals, cudaStream_t st);
 void device_round_f32(const double* d_in, float* d_out, long long n, cudaStream_t st);
-// BF16 copy (the upper half of the FP32 value, rounded to nearest even)
-void device_round_bf16(const double* d_in, uint16_t* d_out, long long n, cudaStream_t st);
 void device_path_vals(int K, const int64_t* d_off, const int* d_prow, const int* d_cand, const int* d_iperm,
                       const double* d_vals, const int64_t* d_ro, const int* d_ra, double* d_pval, cudaStream_t st);
 

@@ -486,21 +486,6 @@ void dense_chol_solve(double* M, int n, double* X, int ldx, int ncols, cudaStrea
     DPHD_CHECK(!(status & kSfbNotPositive), "dense Cholesky: matrix is not positive definite");
 }
 
-namespace {
-__global__ void k_to_bf16(const double* __restrict__ in, uint16_t* __restrict__ out, long long n) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t u = __float_as_uint((float)in[i]);
-        out[i] = (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);  // round to nearest, ties to even
-    }
-}
-}  // namespace
-
-void device_round_bf16(const double* d_in, uint16_t* d_out, long long n, cudaStream_t st) {
-    if (n <= 0) return;
-    k_to_bf16<<<4 * device_sms(), 256, 0, st>>>(d_in, d_out, n);
-    CUDA_OK(cudaGetLastError());
-}
-
 void device_round_f32(const double* d_in, float* d_out, long long n, cudaStream_t st) {
     if (n <= 0) return;
     k_to_f32<<<4 * device_sms(), 256, 0, st>>>(d_in, d_out, n);

@@ -176,6 +176,11 @@ class OracleDeformable:
         return lib().orc_last_iters(self.h)
 
     @property
+    def last_converged(self):
+        """Whether the last forward step's PD loop met its gate before max_pd_iter."""
+        return bool(lib().orc_last_converged(self.h))
+
+    @property
     def last_filtered(self):
         """Samples whose Hessian the last backward eigen-filtered (option bwd_eigen_filter)."""
         return lib().orc_last_filtered(self.h)
