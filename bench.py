@@ -190,17 +190,25 @@ def train_warm_start(dev, args, workload):
     X, Y = generate_dataset(make, seeds, args.ws_steps, dev, options=options(sc0, "f64"))
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
-    mlp = WarmStartMLP(dev, seed=0)
-    hist = fit(mlp, X, Y, steps=args.ws_fit_steps, batch=65536, lr=2e-3, log_every=max(1, args.ws_fit_steps - 1))
-    torch.cuda.synchronize(dev)
-    t2 = time.perf_counter()
-    # mean loss over a fixed sample of the rows after training (the last mini-batch's loss alone is noisy)
+    # A fit from one initialisation at one learning rate sometimes stalls (mean losses after fitting ranged over
+    # 1.9e-4 .. 2.3e-3 between otherwise identical runs), so a few short fits are made and the one with the lowest
+    # loss on a fixed sample of the rows is kept (each fit takes about 1.5 s; the rollouts above take 20 s).
     g = torch.Generator(device=X.device).manual_seed(1)
     idx = torch.randint(0, X.shape[0], (min(262144, X.shape[0]),), device=X.device, generator=g)
-    eval_loss = float(mlp.gradient(X[idx].contiguous(), Y[idx].contiguous())[0])
+    Xe, Ye = X[idx].contiguous(), Y[idx].contiguous()
+    mlp, hist, eval_loss, tried = None, None, float("inf"), []
+    for init_seed, lr in ((0, 2e-3), (1, 2e-3), (2, 1e-3), (3, 1e-3)):
+        cand = WarmStartMLP(dev, seed=init_seed)
+        h = fit(cand, X, Y, steps=args.ws_fit_steps, batch=65536, lr=lr, log_every=max(1, args.ws_fit_steps - 1))
+        e = float(cand.gradient(Xe, Ye)[0])
+        tried.append({"init_seed": init_seed, "lr": lr, "loss_262k_rows": e})
+        if e < eval_loss:
+            mlp, hist, eval_loss = cand, h, e
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
     info = {"train_scene": make(seeds[0]).name + " (seeds %d..%d)" % (seeds[0], seeds[-1]),
             "rollout_steps_per_seed": args.ws_steps, "rows": int(X.shape[0]), "data_gen_s": round(t1 - t0, 2),
-            "fit_s": round(t2 - t1, 2), "fit_steps": args.ws_fit_steps, "batch": 65536,
+            "fit_s": round(t2 - t1, 2), "fit_steps": args.ws_fit_steps, "batch": 65536, "fits": tried,
             "loss_first_last_batch": [h[1] for h in hist], "loss_after_fit_262k_rows": eval_loss}
     del X, Y
     return mlp, info

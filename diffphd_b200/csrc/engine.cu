@@ -758,7 +758,7 @@ void Engine::build_contact(double dt) {
     dc_Xt.alloc(kcap * kcap * sizeof(double));
     dc_X32.alloc(kcap * kcap * sizeof(float));
     dc_Xt32.alloc(kcap * kcap * sizeof(float));
-    dc_pcg.alloc((8 * kcap + 1024) * sizeof(double));
+    dc_pcg.alloc((9 * kcap + 1024) * sizeof(double));
     dc_actref.alloc((size_t)K * sizeof(int));
     dc_refpos.alloc((size_t)K * sizeof(int));
     CUDA_OK(cudaMemset(dc_refpos.p, 0xff, dc_refpos.bytes));  // -1: no candidate is in a cached list yet

@@ -32,6 +32,7 @@ constexpr int kThr = 256;
 constexpr int kNcpPcgIters = 40;       // CG iteration cap for an unchanged list; + 2 per changed candidate
 constexpr int kNcpMaxListChange = 32;  // larger changes of the active list refactor at once
 constexpr double kOmegaMin = 1e-6;     // |omega| below this: the candidate's row is decoupled (E only)
+constexpr double kEDrift = 0.1;        // |E - (omega / omega_ref)^2 E_ref| above this fraction of M_kk: diagonal
 constexpr long long kSpins = 1ll << 24;
 
 __device__ __forceinline__ double wsum(double v) {
@@ -178,7 +179,8 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
     double* rhs = c.rhs;
     double* x = c.xsol;
     double* dg = c.pcg + 5 * (size_t)ldx;    // diag(M)
-    double* part = c.pcg + 8 * (size_t)ldx;  // per-CTA partial sums (omega_ref, kept with the factor, at 7 ldx)
+    double* part = c.pcg + 9 * (size_t)ldx;  // per-CTA partial sums (omega_ref and E_ref, kept with the factor,
+                                             // at 7 ldx and 8 ldx)
     // [0] cached factor valid, [1] its ka, [2] candidates not in its list (this launch), [3] the last CG fell back
     int* flags = c.ncp_flags;
     const bool have = flags[0] != 0;
@@ -239,7 +241,8 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         // M = Omega G Omega + E and M_ref = Omega_r G Omega_r + E_r, so with D = Omega Omega_r^-1 (diagonal)
         // M = D M_ref D + (E - D^2 E_r): the preconditioner D^-1 X^T X D^-1 follows the change of Omega between PD
         // iterations exactly and leaves only the diagonal change of E (small for resting contacts) to CG.
-        // Candidates with omega or omega_ref near 0 (decoupled rows E only) take the diagonal preconditioner.
+        // Candidates with omega or omega_ref near 0 (decoupled rows E only), or whose E moved away from D^2 E_r by
+        // more than kEDrift of their diagonal (a contact opening or closing), take the diagonal preconditioner.
         double* r = c.pcg;
         double* p = c.pcg + ldx;
         double* w = c.pcg + 2 * (size_t)ldx;
@@ -247,6 +250,7 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
         double* zr = c.pcg + 4 * (size_t)ldx;  // X^T X (D^-1 r) over the cached list
         double* sc = c.pcg + 6 * (size_t)ldx;  // omega_ref / omega at a scaled common candidate, else 0
         const double* om_ref = c.pcg + 7 * (size_t)ldx;
+        const double* e_ref = c.pcg + 8 * (size_t)ldx;
         for (int a = gt; a < ld; a += nthr) {
             double f = 0.0;
             if (a < ka) {
@@ -254,8 +258,11 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
                 const int pr = c.ref_pos[k];
                 const double om = c.omega[k];
                 if (pr >= 0 && fabs(om) >= kOmegaMin && fabs(om_ref[pr]) >= kOmegaMin) {
-                    f = om_ref[pr] / om;
-                    c.ref_inv[pr] = a;
+                    const double g = om / om_ref[pr];
+                    if (fabs(c.Ediag[k] - g * g * e_ref[pr]) <= kEDrift * dg[a]) {
+                        f = 1.0 / g;
+                        c.ref_inv[pr] = a;
+                    }
                 }
             }
             sc[a] = f;
@@ -519,6 +526,7 @@ k_ncp_cached_solve(ContactDev c, const double* __restrict__ q0, const int* __res
             c.act_ref[a] = c.act[a];
             c.ref_pos[c.act[a]] = a;
             c.pcg[7 * (size_t)ldx + a] = c.omega[c.act[a]];
+            c.pcg[8 * (size_t)ldx + a] = c.Ediag[c.act[a]];
         }
         if (gt == 0) {
             flags[0] = 1;
