@@ -188,6 +188,14 @@ def train_warm_start(dev, args, workload):
     sc0 = make(seeds[0])
     t0 = time.perf_counter()
     X, Y = generate_dataset(make, seeds, args.ws_steps, dev, options=options(sc0, "f64"))
+    dropped = generate_dataset.dropped_frames
+    # The displacement targets' rare extremes (impact frames) would dominate the squared loss: clipped at four times
+    # their 99.9th percentile (estimated on a fixed sample of a million entries).
+    gq = torch.Generator(device=Y.device).manual_seed(2)
+    samp = Y[:, :3].reshape(-1)[torch.randint(0, Y.shape[0] * 3, (1 << 20,), device=Y.device, generator=gq)]
+    clip = float(4.0 * torch.quantile(samp.abs().float(), 0.999))
+    clipped = int((Y[:, :3].abs() > clip).sum())
+    Y[:, :3].clamp_(-clip, clip)
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
     # A fit from one initialisation at one learning rate sometimes stalls (mean losses after fitting ranged over
@@ -209,6 +217,7 @@ def train_warm_start(dev, args, workload):
     info = {"train_scene": make(seeds[0]).name + " (seeds %d..%d)" % (seeds[0], seeds[-1]),
             "rollout_steps_per_seed": args.ws_steps, "rows": int(X.shape[0]), "data_gen_s": round(t1 - t0, 2),
             "fit_s": round(t2 - t1, 2), "fit_steps": args.ws_fit_steps, "batch": 65536, "fits": tried,
+            "unconverged_frames_dropped": dropped, "target_clip": clip, "target_entries_clipped": clipped,
             "loss_first_last_batch": [h[1] for h in hist], "loss_after_fit_262k_rows": eval_loss}
     del X, Y
     return mlp, info

@@ -185,11 +185,14 @@ class WarmStartStepper:
         self.q_prev = self._bufs["q_prev"]
 
 
-def generate_dataset(make_scene, seeds, steps, device, options=None, method="pd_eigen_alg_phd", stream=0):
+def generate_dataset(make_scene, seeds, steps, device, options=None, method="pd_eigen_alg_phd", stream=0,
+                     drop_unconverged=True):
     """Rollouts of the plain solver (PD loop from q) on each seeded scene; per step and node the features and the
     targets (q_next - q_tilde)/dx and the frame's contact multiplier (scaled, 0 off the contact set).  Returns X
-    (BF16 [N][16]) and Y (FP32 [N][4]) on `device`."""
+    (BF16 [N][16]) and Y (FP32 [N][4]) on `device`.  Frames whose PD loop stopped at max_pd_iter are left out
+    (drop_unconverged): their iterates are no solution to learn."""
     Xs, Ys = [], []
+    generate_dataset.dropped_frames = 0
     for seed in seeds:
         sc = make_scene(int(seed))
         d = core.from_scene(sc)
@@ -212,8 +215,11 @@ def generate_dataset(make_scene, seeds, steps, device, options=None, method="pd_
             d.forward_device(method, q, v, f, sc.dt, opts, qn, vn, stream=stream)
             Y = torch.empty(n3 // 3, N_USED, dtype=torch.float32, device=device)
             d.warmstart_target(sc.dt, qn, base, Y, stream=stream)
-            Xs.append(X)
-            Ys.append(Y)
+            if drop_unconverged and not d.frame_stats()[1][-1]:
+                generate_dataset.dropped_frames += 1
+            else:
+                Xs.append(X)
+                Ys.append(Y)
             q_prev, prev_base = q, base
             q, v = qn.clone(), vn.clone()
         del d
