@@ -1293,7 +1293,7 @@ void Engine::forward_device_init(const double* dq, const double* dv, const doubl
     const double h2m = dt * dt / M.mass();
     const bool learned = !d_init && ws_net_;
     ws_lambda_ = o.ws_lambda != 0;
-    ws_contact_start_ = o.ws_contact_start != 0;
+    ws_contact_start_ = o.ws_contact_start;
     if (learned) d_init = ws_predict(dq, dv, df, dt, o.ws_tcgen05 != 0, st);
     // new-rollout detection of the contact tape (forward_gpu.cpp:437-449): the input must continue the last
     // frame; the comparison is read after the solve's own synchronisation
@@ -1409,9 +1409,9 @@ const double* Engine::ws_predict(const double* dq, const double* dv, const doubl
     }
     ws_apply(dt, base, d_ws_out.as<float>(), d_ws_qinit.as<double>(), st);
     launches_ += 1;
-    if (has_contact_ && ws_contact_start_) {
-        launch_ws_contact_start(contact_.K, dc_cand.as<int>(), dc_lam.as<double>(), contact_.n, contact_.offset,
-                                d_fixed_dof.as<unsigned char>(), dq, d_ws_qinit.as<double>(), st);
+    if (has_contact_ && ws_contact_start_ > 0) {
+        launch_ws_contact_start(contact_.K, ws_contact_start_, dc_cand.as<int>(), dc_lam.as<double>(), contact_.n,
+                                contact_.offset, d_fixed_dof.as<unsigned char>(), dq, d_ws_qinit.as<double>(), st);
         launches_ += 1;
     }
     if (has_contact_ && ws_lambda_) {  // the predicted initial contact multipliers replace the previous frame's

@@ -50,7 +50,8 @@ struct Options {
                                  // contact rollout: inexact steps leave multipliers just above 0, and the active
                                  // list, hence the cached factor, changes more often)
     int ws_contact_start = 0;    // with a warm-start network and contact: 1 keeps the previous gap of the
-                                 // candidates in contact and lifts predicted penetrations to the plane
+                                 // candidates in contact and lifts predicted penetrations to the plane; 2 keeps
+                                 // the candidates in contact at their previous positions
     int ws_lambda = 0;           // with a warm-start network and contact: 1 starts each frame's NCP from the
                                  // network's predicted multipliers instead of the previous frame's (measured
                                  // slower on the 64^3 contact rollout, so off by default)
@@ -304,7 +305,7 @@ private:
     DeviceBuffer d_ws_lamnode;   // node-indexed contact multipliers (the lambda feature)
     DeviceBuffer d_ws_lamprev;   // the multipliers at the last features call (the training target's baseline)
     bool ws_lambda_ = true;
-    bool ws_contact_start_ = false;
+    int ws_contact_start_ = 0;
     int* h_ws_err_ = nullptr;    // pinned copy, read after the forward loop's synchronisation
     DeviceBuffer dc_cand, dc_off, dc_prow, dc_pval, dc_G, dc_rprec, dc_lam, dc_lt1, dc_lt2, dc_omega, dc_E, dc_h,
         dc_act, dc_kact, dc_ainvb, dc_rhs, dc_xsol, dc_bar, dc_M, d_vcon, d_r64, d_q0, dc_Xinv, dc_Xt, dc_pcg,

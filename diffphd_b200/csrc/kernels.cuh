@@ -375,7 +375,7 @@ void launch_mlp_lambda_apply(int K, const int* cand, const float* out, double in
 void launch_mlp_apply(int n3, const double* base, const float* out, double dx, const unsigned char* fixed_dof,
                       const double* fval, double* q_init, cudaStream_t st);
 void launch_mlp_target(int n3, const double* q_next, const double* base, double inv_dx, float* Y, cudaStream_t st);
-void launch_ws_contact_start(int K, const int* cand, const double* lam, const double* n, double off,
+void launch_ws_contact_start(int K, int mode, const int* cand, const double* lam, const double* n, double off,
                              const unsigned char* fixed_dof, const double* q_prev, double* q_init, cudaStream_t st);
 
 // Device-side adjoint routing (backward_gpu.cpp:881-917) and parameter-gradient reductions.

@@ -642,18 +642,28 @@ void launch_mlp_apply(int n3, const double* base, const float* out, double dx, c
                       const double* fval, double* q_init, cudaStream_t st) {
     k_mlp_apply<<<(n3 + 255) / 256, 256, 0, st>>>(n3, base, out, dx, fixed_dof, fval, q_init);
 }
-// The learned start at the contact candidates: a candidate in contact in the previous frame (lambda > 0) keeps its
-// previous gap (a resting contact stays at rest), the others are moved out of the half space if the prediction
-// penetrates it; the tangential components stay as predicted.
-__global__ void k_ws_contact_start(int K, const int* __restrict__ cand, const double* __restrict__ lam, double n0,
-                                   double n1, double n2, double off, const unsigned char* __restrict__ fixed_dof,
-                                   const double* __restrict__ q_prev, double* __restrict__ q_init) {
+// The learned start at the contact candidates.  Mode 1: a candidate in contact in the previous frame (lambda > 0)
+// keeps its previous gap (a resting contact stays at rest), the others are moved out of the half space if the
+// prediction penetrates it; the tangential components stay as predicted.  Mode 2: a candidate in contact keeps
+// its previous position altogether (the plain solver's start there), the others keep the prediction.
+__global__ void k_ws_contact_start(int K, int mode, const int* __restrict__ cand, const double* __restrict__ lam,
+                                   double n0, double n1, double n2, double off,
+                                   const unsigned char* __restrict__ fixed_dof, const double* __restrict__ q_prev,
+                                   double* __restrict__ q_init) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
     const int i = cand[k];
     if (fixed_dof[3 * i] || fixed_dof[3 * i + 1] || fixed_dof[3 * i + 2]) return;
     double* x = q_init + 3 * (size_t)i;
     const double* xp = q_prev + 3 * (size_t)i;
+    if (mode == 2) {
+        if (lam[k] > 0.0) {
+            x[0] = xp[0];
+            x[1] = xp[1];
+            x[2] = xp[2];
+        }
+        return;
+    }
     const double d = n0 * x[0] + n1 * x[1] + n2 * x[2] + off;
     const double dp = n0 * xp[0] + n1 * xp[1] + n2 * xp[2] + off;
     const double target = lam[k] > 0.0 ? dp : (d < 0.0 ? 0.0 : d);
@@ -663,11 +673,11 @@ __global__ void k_ws_contact_start(int K, const int* __restrict__ cand, const do
     x[2] += s * n2;
 }
 
-void launch_ws_contact_start(int K, const int* cand, const double* lam, const double* n, double off,
+void launch_ws_contact_start(int K, int mode, const int* cand, const double* lam, const double* n, double off,
                              const unsigned char* fixed_dof, const double* q_prev, double* q_init, cudaStream_t st) {
     if (K > 0)
-        k_ws_contact_start<<<(K + 255) / 256, 256, 0, st>>>(K, cand, lam, n[0], n[1], n[2], off, fixed_dof, q_prev,
-                                                             q_init);
+        k_ws_contact_start<<<(K + 255) / 256, 256, 0, st>>>(K, mode, cand, lam, n[0], n[1], n[2], off, fixed_dof,
+                                                             q_prev, q_init);
 }
 
 void launch_mlp_target(int n3, const double* q_next, const double* base, double inv_dx, float* Y, cudaStream_t st) {
