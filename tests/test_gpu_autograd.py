@@ -116,7 +116,7 @@ def test_checkpointed_rollout_with_learned_start_recomputes_exactly():
         params = sim.default_params().to("cuda").requires_grad_(True)
         L = _loss(sim, sc, T, q0, v0, params, T(sc.f_ext), r, ck)
         L.backward()
-        grads.append((float(L), v0.grad.cpu().numpy(), params.grad.cpu().numpy()))
+        grads.append((float(L.detach()), v0.grad.cpu().numpy(), params.grad.cpu().numpy()))
     for g in grads[1:]:
         assert g[0] == grads[0][0]
         assert np.array_equal(g[1], grads[0][1]) and np.array_equal(g[2], grads[0][2])
