@@ -372,13 +372,16 @@ void Engine::build_device(int threads) {
         std::vector<int> pos(r_ptr.begin(), r_ptr.end() - 1);
         for (size_t t = 0; t < it_row.size(); ++t) r_items[pos[it_row[t]]++] = (int)t;
     }
-    // x = S^T y schedule: each tile's row list in chunks of st_chunk_rows_ rows
+    // x = S^T y schedule: each tile's row list in chunks of `chunk` rows (long chunks for large factors, where
+    // they keep more bytes in flight per CTA; short ones for small factors, where they make enough CTAs)
+    const int chunk = st_chunk_rows_ > 0 ? st_chunk_rows_ : ((long long)ro[n] > kChunkLargeValues ? kChunkRows
+                                                                                                  : kChunkRowsSmall);
     std::vector<int> c_tile, c_p0, c_p1, t_cptr(ntiles_ + 1, 0);
     for (int t = 0; t < ntiles_; ++t) {
-        for (int p0 = tcnt[t]; p0 < tcnt[t + 1]; p0 += st_chunk_rows_) {
+        for (int p0 = tcnt[t]; p0 < tcnt[t + 1]; p0 += chunk) {
             c_tile.push_back(t);
             c_p0.push_back(p0);
-            c_p1.push_back(std::min(p0 + st_chunk_rows_, tcnt[t + 1]));
+            c_p1.push_back(std::min(p0 + chunk, tcnt[t + 1]));
         }
         if (tcnt[t] == tcnt[t + 1]) {  // keep every tile covered so stage 2 writes zeros
             c_tile.push_back(t);

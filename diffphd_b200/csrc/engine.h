@@ -240,7 +240,7 @@ private:
     void check_device() const;
     int device_ = -1;
     int factor_mode_ = 0, small_subtree_max_ = 512;
-    int st_chunk_rows_ = kChunkRows, st_rows_ = 4;
+    int st_chunk_rows_ = 0, st_rows_ = 4;  // chunk rows 0: by the factor's size
     bool proj32_ = true;  // precision of the projections captured in the mixed-precision iteration graphs
     // the contact-adjoint preconditioner's direction factors X_b: the G they were built from (generation of the
     // contact set-up) and their constrained candidates, reused while both are unchanged

@@ -124,8 +124,10 @@ struct SpmvPlan {
 };
 constexpr int kSegCols = 2048;       // columns per S v work item
 constexpr int kUnitRows = 8;         // rows per S v unit (the row-group cap of the item schedule)
-constexpr int kChunkRows = 512;      // rows per S^T chunk CTA (default of the schedule; measured on the 64^3
-                                     // contact block: 64 -> 512 rows took the FP32 pair from 4.05 to 3.60 ms)
+constexpr int kChunkRows = 512;      // rows per S^T chunk CTA for large factors (64^3 contact block: 64 -> 512
+                                     // rows took the FP32 pair from 4.05 to 3.60 ms)
+constexpr int kChunkRowsSmall = 64;  // for factors of at most kChunkLargeValues values (more CTAs to fill the GPU)
+constexpr long long kChunkLargeValues = 1ll << 28;
 constexpr int kStChunkMax = 512;     // largest S^T chunk (its row descriptors are staged in shared memory)
 constexpr int kGatherLanes = 8;      // lanes per node in the node gathers
 constexpr int kGatherMaxThreads = 512;  // block-size bound of the node gathers

@@ -113,7 +113,7 @@ int dphd_debug_set_mma_wait_polls(long long polls);
  * larger separator chain on the GPU from the Schur complement of its descendants).  Takes effect at the next
  * factor build.  No counterpart in the reference. */
 int dphd_debug_set_factor_build(dphd_deformable* h, int mode, int small_subtree_max);
-/* Schedule of the x = S^T y pass: rows of a column tile's row list per CTA (chunk_rows, 8..512, default 512) and
+/* Schedule of the x = S^T y pass: rows of a column tile's row list per CTA (chunk_rows, 8..512; by default 512 for factors above 2^28 values, else 64) and
  * rows each warp keeps in flight (4 or 8, default 4).  Changes the order of the partial sums, so results differ
  * at the rounding level between schedules.  Takes effect at the next factor build.  No counterpart in the
  * reference. */
